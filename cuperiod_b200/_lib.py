@@ -1,0 +1,282 @@
+"""ctypes binding of the engine library ``libbls_b200.so`` (``include/bls_b200.h``).
+
+The library is built in-tree by ``csrc/Makefile``.  There is no fallback: if it
+is missing, or no CUDA device is usable, every entry point raises
+:class:`~cuperiod_b200.errors.BackendUnavailableError`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from dataclasses import dataclass
+
+import numpy as np
+
+from .errors import BackendUnavailableError, EngineError
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbls_b200.so")
+
+BLS_OK, BLS_E_INVALID, BLS_E_CUDA, BLS_E_RESOURCE, BLS_E_NOMEM, BLS_E_DEVICE, BLS_E_STATE = range(7)
+N_FIELDS = 7
+FIELD_NAMES = ("power", "depth", "depth_err", "depth_snr", "duration", "transit_time",
+               "log_likelihood")
+
+_i32, _i64, _dbl, _vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+
+
+class BlsTune(ctypes.Structure):
+    _fields_ = [("device", _i32), ("smem_per_cta", _i32), ("max_tile", _i32), ("use_graph", _i32),
+                ("exact_sweep", _i32)]
+
+
+class BlsGrid(ctypes.Structure):
+    _fields_ = [("n_segments", _i32), ("seg_offsets", _vp), ("periods", _vp),
+                ("dur_offsets", _vp), ("durations", _vp), ("oversample", _i32),
+                ("objective", _i32)]
+
+
+class BlsCurves(ctypes.Structure):
+    _fields_ = [("n_curves", _i32), ("offsets", _vp), ("t", _vp), ("y", _vp), ("dy", _vp)]
+
+
+class BlsBatchInfo(ctypes.Structure):
+    _fields_ = [("n_curves", _i32), ("n_segments", _i32), ("n_periods", _i64),
+                ("n_items", _i64), ("n_points", _i64), ("folds", _dbl), ("boxes", _dbl),
+                ("trials", _dbl), ("h2d_bytes", _i64), ("ctas", _i32), ("smem_per_cta", _i32),
+                ("uniform_curves", _i32), ("fast_fold_segments", _i32)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_lib: ctypes.CDLL | None = None
+_lib_lock = threading.Lock()
+
+
+def load() -> ctypes.CDLL:
+    """The engine library, loaded once; raises if it was not built."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise BackendUnavailableError(
+                f"BLS engine library {LIB_PATH} is not built (run `make -C "
+                f"{os.path.join(_HERE, 'csrc')}` or __graft_entry__.build())")
+        lib = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        lib.bls_last_error.restype = ctypes.c_char_p
+        lib.bls_last_error.argtypes = []
+        lib.bls_engine_create.argtypes = [P(BlsTune), P(_vp)]
+        lib.bls_engine_destroy.argtypes = [_vp]
+        lib.bls_prepare.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp]
+        lib.bls_launch.argtypes = [_vp, _vp]
+        lib.bls_download.argtypes = [_vp, _vp, _vp]
+        lib.bls_device_output.argtypes = [_vp, P(_vp)]
+        lib.bls_download_best.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
+        lib.bls_search.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
+        lib.bls_batch_info.argtypes = [_vp, P(BlsBatchInfo)]
+        lib.bls_debug_fold_bins.argtypes = [_vp, _vp, _i64, _dbl, _dbl, _i32, _vp, _vp]
+        lib.bls_debug_prefix.argtypes = [_vp, _vp, _vp, _vp, _i64, _dbl, _vp, _i32, _i32, _vp, _vp,
+                                         _vp]
+        for name in ("bls_engine_create", "bls_engine_destroy", "bls_prepare", "bls_launch",
+                     "bls_download", "bls_device_output", "bls_download_best", "bls_search",
+                     "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix"):
+            getattr(lib, name).restype = ctypes.c_int
+        _lib = lib
+        return lib
+
+
+def _check(rc: int) -> None:
+    if rc == BLS_OK:
+        return
+    msg = (load().bls_last_error() or b"").decode(errors="replace")
+    if rc == BLS_E_INVALID:
+        raise ValueError(msg)
+    if rc == BLS_E_RESOURCE:
+        raise BackendUnavailableError(msg)
+    raise EngineError(f"BLS engine error {rc}: {msg}")
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _addr(a: np.ndarray | None) -> int | None:
+    return None if a is None else a.ctypes.data
+
+
+@dataclass
+class PackedGrid:
+    """A segmented period grid in the C ABI's layout (keeps its arrays alive)."""
+    seg_offsets: np.ndarray
+    periods: np.ndarray
+    dur_offsets: np.ndarray
+    durations: np.ndarray
+    oversample: int
+    objective: int
+
+    @classmethod
+    def from_segments(cls, segments, oversample: int, objective: int) -> "PackedGrid":
+        per = [_f64(p).ravel() for p, _ in segments]
+        dur = [_f64(d).ravel() for _, d in segments]
+        seg_off = np.zeros(len(segments) + 1, dtype=np.int64)
+        dur_off = np.zeros(len(segments) + 1, dtype=np.int64)
+        seg_off[1:] = np.cumsum([p.size for p in per]) if per else []
+        dur_off[1:] = np.cumsum([d.size for d in dur]) if dur else []
+        return cls(seg_off, _f64(np.concatenate(per)) if per else np.empty(0),
+                   dur_off, _f64(np.concatenate(dur)) if dur else np.empty(0),
+                   int(oversample), int(objective))
+
+    @property
+    def n_periods(self) -> int:
+        return int(self.seg_offsets[-1])
+
+    def struct(self) -> BlsGrid:
+        return BlsGrid(len(self.seg_offsets) - 1, _addr(self.seg_offsets), _addr(self.periods),
+                       _addr(self.dur_offsets), _addr(self.durations), self.oversample,
+                       self.objective)
+
+
+@dataclass
+class PackedCurves:
+    """Light curves concatenated in the C ABI's layout (keeps its arrays alive)."""
+    offsets: np.ndarray
+    t: np.ndarray
+    y: np.ndarray
+    dy: np.ndarray | None
+
+    @classmethod
+    def from_arrays(cls, curves) -> "PackedCurves":
+        ts, ys, dys = [], [], []
+        any_dy = any(c[2] is not None for c in curves)
+        for t, y, dy in curves:
+            t, y = _f64(t).ravel(), _f64(y).ravel()
+            if t.shape != y.shape:
+                raise ValueError("t and y must have the same length")
+            ts.append(t)
+            ys.append(y)
+            if any_dy:
+                dys.append(np.ones_like(t) if dy is None else _f64(dy).ravel())
+        off = np.zeros(len(curves) + 1, dtype=np.int64)
+        off[1:] = np.cumsum([t.size for t in ts])
+        cat = lambda xs: _f64(np.concatenate(xs)) if xs else np.empty(0)
+        return cls(off, cat(ts), cat(ys), cat(dys) if any_dy else None)
+
+    @property
+    def n_curves(self) -> int:
+        return len(self.offsets) - 1
+
+    def struct(self) -> BlsCurves:
+        return BlsCurves(self.n_curves, _addr(self.offsets), _addr(self.t), _addr(self.y),
+                         _addr(self.dy))
+
+
+class Engine:
+    """One engine = one device context, stream, buffer set and graph cache.
+
+    Not thread-safe (like the reference's per-worker engines,
+    src/cuperiod/methods/base.py:388-396): use one per thread.
+    """
+
+    def __init__(self, device: int = -1, *, smem_per_cta: int = 0, max_tile: int = 0,
+                 use_graph: bool = True, exact_sweep: bool = False) -> None:
+        self._lib = load()
+        tune = BlsTune(int(device), int(smem_per_cta), int(max_tile), int(bool(use_graph)),
+                       int(bool(exact_sweep)))
+        handle = _vp()
+        _check(self._lib.bls_engine_create(ctypes.byref(tune), ctypes.byref(handle)))
+        self._h = handle
+        self._grid: PackedGrid | None = None
+        self._curves: PackedCurves | None = None
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.bls_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self) -> None:  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def prepare(self, grid: PackedGrid, curves: PackedCurves, stream: int | None = None) -> None:
+        self._grid, self._curves = grid, curves
+        g, c = grid.struct(), curves.struct()
+        _check(self._lib.bls_prepare(self._h, ctypes.byref(g), ctypes.byref(c), stream))
+
+    def launch(self, stream: int | None = None) -> None:
+        _check(self._lib.bls_launch(self._h, stream))
+
+    def download(self, stream: int | None = None) -> np.ndarray:
+        """All fields: array of shape (7, n_curves, n_periods)."""
+        assert self._grid is not None and self._curves is not None
+        out = np.empty((N_FIELDS, self._curves.n_curves, self._grid.n_periods), dtype=np.float64)
+        _check(self._lib.bls_download(self._h, out.ctypes.data, stream))
+        return out
+
+    def download_best(self, stream: int | None = None):
+        assert self._curves is not None
+        n = self._curves.n_curves
+        idx = np.empty(n, dtype=np.int64)
+        val, mean, std = (np.empty(n, dtype=np.float64) for _ in range(3))
+        _check(self._lib.bls_download_best(self._h, idx.ctypes.data, val.ctypes.data,
+                                           mean.ctypes.data, std.ctypes.data, stream))
+        return idx, val, mean, std
+
+    def device_output(self) -> int:
+        ptr = _vp()
+        _check(self._lib.bls_device_output(self._h, ctypes.byref(ptr)))
+        return int(ptr.value or 0)
+
+    def info(self) -> dict:
+        info = BlsBatchInfo()
+        _check(self._lib.bls_batch_info(self._h, ctypes.byref(info)))
+        return info.as_dict()
+
+    def search(self, grid: PackedGrid, curves: PackedCurves, stream: int | None = None) -> np.ndarray:
+        self.prepare(grid, curves, stream)
+        self.launch(stream)
+        return self.download(stream)
+
+    def prefix_sums(self, t, y, dy, period: float, durations, oversample: int):
+        """Debug view: the device's padded cumulative sums of y*ivar and ivar over
+        the phase bins of one period (reference units)."""
+        t, y = _f64(t).ravel(), _f64(y).ravel()
+        dy = None if dy is None else _f64(dy).ravel()
+        durations = _f64(durations).ravel()
+        width = int(np.ceil(period / (durations.min() / oversample))) + oversample + 1
+        yw = np.empty(width + 1, dtype=np.float64)
+        iv = np.empty(width + 1, dtype=np.float64)
+        nb = ctypes.c_int32()
+        _check(self._lib.bls_debug_prefix(self._h, t.ctypes.data, y.ctypes.data, _addr(dy),
+                                          t.size, float(period), durations.ctypes.data,
+                                          durations.size, int(oversample), yw.ctypes.data,
+                                          iv.ctypes.data, ctypes.byref(nb)))
+        return yw[:nb.value + 1], iv[:nb.value + 1]
+
+    def fold_bins(self, t, period: float, bin_duration: float, width: int):
+        """Debug view: the device's phase bin of every point at one period."""
+        t = _f64(t).ravel()
+        bins = np.empty(t.size, dtype=np.int32)
+        fast = np.empty(t.size, dtype=np.int32)
+        _check(self._lib.bls_debug_fold_bins(self._h, t.ctypes.data, t.size, float(period),
+                                             float(bin_duration), int(width), bins.ctypes.data,
+                                             fast.ctypes.data))
+        return bins, fast.astype(bool)
+
+
+_local = threading.local()
+
+
+def default_engine() -> Engine:
+    """This thread's engine on the current CUDA device (created on first use)."""
+    eng = getattr(_local, "engine", None)
+    if eng is None:
+        eng = Engine()
+        _local.engine = eng
+    return eng

@@ -1,0 +1,103 @@
+// Device-side data layout of the B200 box-least-squares engine.
+//
+// One launch searches a batch of light curves over one segmented trial-period
+// grid.  The host packs every curve once (time origin removed in FP64, flux
+// centred and quantised to exact fixed point) and splits the work into items of
+// (curve, segment, tile of consecutive periods); a persistent grid of CTAs pulls
+// items from a global counter.
+#pragma once
+#include <stdint.h>
+
+namespace blsb200 {
+
+// Accumulation modes.  Every sum is an exact integer built from native 32-bit
+// shared atomics: a point's quantised value v (|v| <= 2^24) is added as its
+// unsigned low 13 bits to one word and its signed high part to another, so a
+// bin's sum is (signed) B * 2^13 + A with no carry lost for up to 2^17 points.
+//  UNIFORM: every point has the same inverse variance w: r_q (the quantised
+//           centred flux * weight) and a count per bin (three atomics).
+//  GENERAL: per-point weights.  Their dynamic range can span many decades, so
+//           the two sums (centred flux*weight and weight, both scaled by powers
+//           of two) stay FP64, like the reference's, with FP64 shared atomics.
+enum : int { MODE_UNIFORM = 0, MODE_GENERAL = 1 };
+
+constexpr int kFields = 7;          // power, depth, depth_err, depth_snr, duration, t0, loglike
+constexpr int kMaxDur = 32;         // deduplicated box widths per segment
+constexpr int kMaxTile = 16;        // periods per work item
+constexpr int kHalfBits = 13;       // bits per atomic half-word
+constexpr int kCountShift = 18;     // packed prefix: R * 2^18 + count
+constexpr int kMaxPoints = (1 << 17) - 1;  // per curve: 32-bit prefix words stay exact
+
+// One CTA folds points in chunks of kChunkThreads x kChunkPts.  The host stores
+// every full chunk lane-interleaved: memory slot chunk*2048 + r*256 + lane holds
+// the point of time index chunk*2048 + lane*8 + r, so a lane's kChunkPts points
+// are consecutive in time (equal bins merge in registers) and the lanes of a
+// warp are 8 points apart (distinct bins, few atomic conflicts), while loads
+// stay coalesced.
+constexpr int kChunkThreads = 256;
+constexpr int kChunkPts = 8;
+constexpr int kChunk = kChunkThreads * kChunkPts;
+
+struct SegmentDesc {
+    int64_t period_off;     // first period of this segment in the grid arrays
+    int32_t n_periods;
+    int32_t width;          // the reference's width: ceil(max P / bin) + oversample + 1
+    double bin_duration;
+    int32_t dur_off;        // into dur_bins
+    int32_t n_dur;
+    int32_t oversample;
+    int32_t frac_bits;      // fast fold: fraction bits of the scaled phase
+    uint32_t margin_u;      // fast fold: bin-edge margin, units of 2^-frac_bits bins
+    uint32_t margin_phi;    // fast fold: cycle-edge margin, units of 2^-32 cycles
+    int32_t fast_fold;      // 1: the fast fold's error bound holds for the batch
+    int32_t hist_len;       // bins held per period: max n_bins + 1 over the segment
+};
+
+struct CurveDesc {
+    int64_t point_off;      // first point in the packed point arrays
+    int64_t out_off;        // offset of this curve's spectrum in each output field
+    int32_t n_points;
+    int32_t mode;           // MODE_UNIFORM / MODE_GENERAL
+    int32_t exact_all;      // 1: every admissible box is evaluated in FP64
+    int32_t skip;           // 1: nothing admissible (e.g. zero total weight)
+    double t_min;           // time origin removed from tau (added back to t0)
+    double sum_y;           // sum of y*ivar (reference units)
+    double sum_ivar;        // sum of ivar
+    double ivar_floor;      // admissibility floor of either side of a box
+    double ybar;            // sum_y / sum_ivar
+    double w_uniform;       // UNIFORM: the common ivar
+    double i_total;         // GENERAL: sum of the scaled weights
+    int32_t e_r;            // r (reference units) = stored r * 2^-e_r
+    int32_t e_i;            // GENERAL: ivar (reference units) = stored weight * 2^-e_i
+};
+
+struct WorkItem {
+    int32_t curve;
+    int32_t segment;
+    int32_t p_begin;        // first period of the tile, within the segment
+    int32_t p_count;        // periods in the tile (<= kMaxTile)
+};
+
+struct BatchArgs {
+    const CurveDesc* curves;
+    const SegmentDesc* segments;
+    const WorkItem* items;
+    const double* tau;          // per point: t - t_min (FP64)
+    const uint32_t* pay_r;      // per point: r_q as low 13 bits | signed high part << 16
+    const double* r64;          // GENERAL: (y*ivar - ybar*ivar) * 2^e_r per point
+    const double* iv64;         // GENERAL: ivar * 2^e_i per point
+    const double* period;       // per grid period
+    const double* freq;         // RN(1/P)
+    const uint32_t* scale;      // round(P/bin * 2^frac_bits)
+    const int32_t* nbins;       // n_bins of the reference
+    const int32_t* dur_bins;    // per segment, box widths in bins (first-seen order)
+    double* out;                // kFields x out_stride, field-major
+    int64_t out_stride;
+    int32_t* work_counter;      // persistent scheduler: next unclaimed item
+    int32_t* error_flag;        // set by a CTA that met an impossible descriptor
+    double* debug_prefix;       // test hook: prefix sums of one period (NULL in searches)
+    int32_t n_items;
+    int32_t obj_flag;           // 0 snr, 1 log-likelihood
+};
+
+}  // namespace blsb200

@@ -1,0 +1,975 @@
+// Host side of the B200 BLS engine: the C ABI of include/bls_b200.h.
+//
+// bls_prepare packs a batch on all host cores into pinned staging (the
+// reference's host steps: time origin, median centring, inverse variances --
+// cuPeriod src/cuperiod/methods/_bls_core.py:1043-1058, 709-738 -- then this
+// engine's exact fixed-point encoding), derives each segment's binning exactly
+// as _search_spec / _duration_bins do (_bls_core.py:134-149, 697-706), builds
+// the work list and uploads everything in a few large copies.  bls_launch runs
+// the persistent search kernels (replayed from a CUDA graph when enabled);
+// bls_download / bls_download_best bring results back.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/bls_b200.h"
+#include "bls_device.h"
+#include "bls_launch.h"
+
+using namespace blsb200;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? BLS_E_NOMEM : BLS_E_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+}
+
+#define CUDA_TRY(expr, what)                          \
+    do {                                              \
+        cudaError_t e_ = (expr);                      \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return BLS_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+        cap = want;
+        return BLS_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Grow-only pinned host buffer.
+struct HostBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return BLS_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        if (e != cudaSuccess) return cuda_fail(e, "pinned host allocation");
+        cap = want;
+        return BLS_OK;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// numpy's pairwise summation of a contiguous float64 array (the algorithm of
+// numpy's pairwise_sum: 8 partial sums over blocks of at most 128 elements,
+// halves split on a multiple of 8), so sum_y and sum_ivar equal the reference's
+// yw.sum() / ivar.sum() bit for bit.
+double pairwise_sum(const double* a, int64_t n) {
+    if (n < 8) {
+        double res = 0.0;
+        for (int64_t i = 0; i < n; ++i) res += a[i];
+        return res;
+    }
+    if (n <= 128) {
+        double r[8];
+        for (int k = 0; k < 8; ++k) r[k] = a[k];
+        int64_t i;
+        for (i = 8; i < n - (n % 8); i += 8)
+            for (int k = 0; k < 8; ++k) r[k] += a[i + k];
+        double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+        for (; i < n; ++i) res += a[i];
+        return res;
+    }
+    int64_t n2 = n / 2;
+    n2 -= n2 % 8;
+    return pairwise_sum(a, n2) + pairwise_sum(a + n2, n - n2);
+}
+
+// Fast-fold parameters of one segment (see the kernel's fold_fast): the
+// fraction bits of the scaled phase and the margins that make its result
+// provably the reference's.  q_max bounds tau * (1/P) over the batch, tau_max
+// the largest time offset.
+struct FoldParams {
+    int fb = 0;
+    uint32_t mu = 0, mphi = 0;
+    bool fast = false;
+};
+
+FoldParams fold_params(int64_t width, double bin, double tau_max, double f_max, double s_max) {
+    FoldParams fp;
+    if (width < 2 || width > (1 << 20) || !(bin > 0.0)) return fp;
+    const double q_max = tau_max * f_max;
+    if (!(q_max < 262144.0)) return fp;                      // q must stay below 2^18
+    int lw = 0;
+    while ((int64_t(1) << (lw + 1)) <= width) ++lw;          // floor(log2(width))
+    fp.fb = 31 - lw;                                         // width * 2^fb < 2^32
+    const double two32 = 4294967296.0;
+    // our phase error (cycles): RN(x*RN(1/P)) and the 2^-32 grid
+    const double e_phi = q_max * std::ldexp(1.0, -52) * 1.01 + std::ldexp(1.0, -33);
+    // the reference's floor(RN(x/P)) is exact unless the phase is this close to a cycle edge
+    const double e_phi_ref = q_max * std::ldexp(1.0, -53);
+    const double mphi = std::ceil((e_phi + e_phi_ref) * two32) + 2.0;
+    // the reference's w/bin error (bins): x - P*floor rounds at ulp(x), the division at 2^-53
+    int ex = 0;
+    if (tau_max > 0.0) std::frexp(tau_max, &ex);            // tau_max < 2^ex
+    const double e_ref = 2.0 * std::ldexp(1.0, ex - 52) / bin + (double)width * std::ldexp(1.0, -52);
+    const double scale = std::ldexp(1.0, fp.fb);
+    const double e_u = e_phi * s_max * scale + 2.0;          // + S rounding and the floor
+    const double mu = std::ceil(e_u + e_ref * scale) + 2.0;
+    if (!(mphi < 1e6) || !(mu * 4.0 < scale)) return fp;
+    fp.mu = (uint32_t)mu;
+    fp.mphi = (uint32_t)mphi;
+    fp.fast = true;
+    return fp;
+}
+
+struct PeriodConst {
+    double f;
+    uint32_t S;
+    int32_t nb;
+};
+
+// The reference's n_bins of one period (_bls_core.py:358-360 / 525-526).
+inline int64_t period_bins(double P, double bin, int oversample, int64_t width) {
+    int64_t nb = (int64_t)std::ceil(P / bin) + oversample;
+    return nb > width - 1 ? width - 1 : nb;
+}
+
+struct SegmentHost {
+    SegmentDesc d;
+    std::vector<int32_t> dur;
+    bool empty_periods = false;
+};
+
+struct CurveHost {
+    CurveDesc d;
+    double tau_max = 0.0;
+    int status = BLS_OK;
+    std::string err;
+};
+
+}  // namespace
+
+struct BlsEngine {
+    int device = 0;
+    int n_sm = 0;
+    size_t smem_optin = 0;
+    cudaStream_t stream = nullptr;
+    BlsTune tune{};
+
+    // device buffers
+    DevBuf d_tau, d_pay_r, d_r64, d_iv64, d_period, d_freq, d_scale, d_nbins, d_dur, d_curves,
+        d_segments, d_items, d_out, d_ctl, d_best;
+    // pinned staging
+    HostBuf h_tau, h_pay_r, h_r64, h_iv64, h_grid, h_meta, h_ctl, h_best;
+
+    // the prepared batch
+    bool prepared = false;
+    int n_curves = 0;
+    int64_t n_periods = 0;
+    int n_items_mode[2] = {0, 0};
+    int ctas_mode[2] = {0, 0};
+    size_t smem = 0;
+    BatchArgs args[2]{};
+    BlsBatchInfo info{};
+
+    // CUDA graph of one launch
+    cudaGraphExec_t graph = nullptr;
+    bool graph_valid = false;
+
+    ~BlsEngine() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (DevBuf* b : {&d_tau, &d_pay_r, &d_r64, &d_iv64, &d_period, &d_freq, &d_scale, &d_nbins,
+                          &d_dur, &d_curves, &d_segments, &d_items, &d_out, &d_ctl, &d_best})
+            b->release();
+        for (HostBuf* b : {&h_tau, &h_pay_r, &h_r64, &h_iv64, &h_grid, &h_meta, &h_ctl, &h_best})
+            b->release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+cudaStream_t pick(BlsEngine* e, void* s) {
+    return s ? static_cast<cudaStream_t>(s) : e->stream;
+}
+
+// One quantised value (|v| <= 2^24) as the kernel adds it: the unsigned low 13
+// bits in the low half-word, the signed high part in the high half-word.
+inline uint32_t split_word(long long v) {
+    const uint32_t lo = (uint32_t)(v & ((1 << kHalfBits) - 1));
+    const int32_t hi = (int32_t)(v >> kHalfBits);              // arithmetic shift
+    return lo | ((uint32_t)(uint16_t)(int16_t)hi << 16);
+}
+
+// Memory slot of the point with time index j in a curve of n points: every full
+// chunk of kChunk points is stored lane-interleaved (see kChunk in bls_device.h),
+// the tail in time order.
+inline int64_t point_slot(int64_t j, int64_t n) {
+    const int64_t full = (n / kChunk) * kChunk;
+    if (j >= full) return j;
+    const int64_t c = j / kChunk, w = j % kChunk;
+    return c * kChunk + (w % kChunkPts) * kChunkThreads + w / kChunkPts;
+}
+
+// Pack one curve: the reference's host inputs, then the fixed-point words.
+void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* pay_r,
+                double* r64, double* iv64, CurveHost& ch, std::vector<double>& scratch) {
+    const int64_t b = cv->offsets[c], e = cv->offsets[c + 1];
+    const int64_t n = e - b;
+    CurveDesc& d = ch.d;
+    std::memset(&d, 0, sizeof(d));
+    d.point_off = off;
+    d.n_points = (int32_t)n;
+    if (n < 1) {
+        ch.status = BLS_E_INVALID;
+        ch.err = "light curve " + std::to_string(c) + " has no points";
+        return;
+    }
+    if (n > kMaxPoints) {
+        ch.status = BLS_E_INVALID;
+        ch.err = "light curve " + std::to_string(c) + " has more than " +
+                 std::to_string(kMaxPoints) + " points";
+        return;
+    }
+    const double* t = cv->t + b;
+    const double* y = cv->y + b;
+    const double* dy = cv->dy ? cv->dy + b : nullptr;
+    double t_min = t[0];
+    for (int64_t j = 0; j < n; ++j) {
+        if (!std::isfinite(t[j]) || !std::isfinite(y[j]) ||
+            (dy && !(std::isfinite(dy[j]) && dy[j] > 0.0))) {
+            ch.status = BLS_E_INVALID;
+            ch.err = "light curve " + std::to_string(c) +
+                     ": times, fluxes and errors must be finite (errors > 0)";
+            return;
+        }
+        t_min = std::min(t_min, t[j]);
+    }
+    // y - median(y) (np.median: the mean of the two middle values for even n)
+    scratch.assign(y, y + n);
+    const int64_t mid = n / 2;
+    std::nth_element(scratch.begin(), scratch.begin() + mid, scratch.end());
+    double med = scratch[mid];
+    if (n % 2 == 0) {
+        const double lo = *std::max_element(scratch.begin(), scratch.begin() + mid);
+        med = (lo + med) / 2.0;
+    }
+    // yw, ivar (reference units); sums with numpy's pairwise order
+    scratch.resize(3 * (size_t)n);
+    double* yw = scratch.data();
+    double* iv = yw + n;
+    double* r = iv + n;
+    double tau_max = 0.0;
+    bool uniform = true;
+    for (int64_t j = 0; j < n; ++j) {
+        const double tj = t[j] - t_min;
+        tau[point_slot(j, n)] = tj;
+        tau_max = std::max(tau_max, tj);
+        iv[j] = dy ? 1.0 / (dy[j] * dy[j]) : 1.0;
+        yw[j] = (y[j] - med) * iv[j];
+        uniform = uniform && iv[j] == iv[0];
+    }
+    const double sum_y = pairwise_sum(yw, n);
+    const double sum_ivar = pairwise_sum(iv, n);
+    double sum_abs = 0.0;
+    for (int64_t j = 0; j < n; ++j) sum_abs += std::fabs(yw[j]);
+    const double ybar = sum_ivar > 0.0 ? sum_y / sum_ivar : 0.0;
+    double max_r = 0.0, max_i = 0.0;
+    for (int64_t j = 0; j < n; ++j) {
+        r[j] = yw[j] - ybar * iv[j];
+        max_r = std::max(max_r, std::fabs(r[j]));
+        max_i = std::max(max_i, iv[j]);
+    }
+    int k = 0;
+    int e_r = 0;
+    if (max_r > 0.0 && std::isfinite(max_r)) {
+        std::frexp(max_r, &k);             // max_r < 2^k
+        e_r = 24 - k;                      // |r_q| <= 2^24
+    }
+    for (int64_t j = 0; j < n; ++j)
+        pay_r[point_slot(j, n)] = split_word(std::llrint(std::ldexp(r[j], e_r)));
+    int e_i = 0;
+    double i_total = 0.0;
+    if (!uniform) {
+        // per-point weights: FP64 values scaled by powers of two (exact)
+        if (max_i > 0.0 && std::isfinite(max_i)) {
+            std::frexp(max_i, &k);
+            e_i = 24 - k;
+        }
+        for (int64_t j = 0; j < n; ++j) {
+            const int64_t m = point_slot(j, n);
+            r64[m] = std::ldexp(r[j], e_r);
+            iv64[m] = std::ldexp(iv[j], e_i);
+            i_total += iv64[m];
+        }
+    }
+    const double eps = DBL_EPSILON;
+    double floor_v = 4.0 * (double)n * eps * sum_ivar;            // _ivar_floor, 75-94
+    if (!(floor_v > 0.0)) floor_v = DBL_MIN;
+    d.mode = uniform ? MODE_UNIFORM : MODE_GENERAL;
+    d.exact_all = !(sum_abs >= 1e-150 && sum_abs <= 1e150 && sum_ivar >= 1e-150 &&
+                    sum_ivar <= 1e150);
+    d.skip = !(sum_ivar > 0.0 && std::isfinite(sum_ivar));
+    d.t_min = t_min;
+    d.sum_y = sum_y;
+    d.sum_ivar = sum_ivar;
+    d.ivar_floor = floor_v;
+    d.ybar = ybar;
+    d.w_uniform = iv[0];
+    d.i_total = i_total;
+    d.e_r = e_r;
+    d.e_i = e_i;
+    ch.tau_max = tau_max;
+}
+
+template <typename F>
+void parallel_for(int n, F&& fn) {
+    int hw = (int)std::thread::hardware_concurrency();
+    int nt = std::max(1, std::min(hw, n));
+    if (nt <= 1) {
+        for (int i = 0; i < n; ++i) fn(i, 0);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> th;
+    th.reserve(nt);
+    for (int w = 0; w < nt; ++w)
+        th.emplace_back([&, w] {
+            for (;;) {
+                int i = next.fetch_add(1);
+                if (i >= n) break;
+                fn(i, w);
+            }
+        });
+    for (auto& x : th) x.join();
+}
+
+constexpr size_t kDefaultSmem = 108 * 1024;     // two CTAs per SM with the static state
+
+size_t screen_bytes(int /*mode*/, int hl) { return (size_t)hl * 8; }
+size_t period_bytes(int mode, int hl) { return period_hist_bytes(mode, hl); }
+
+int tile_cap(int mode, int hl, size_t smem, int max_tile) {
+    const size_t scr = screen_bytes(mode, hl) + 16;
+    if (smem <= scr) return 0;
+    int cap = (int)((smem - scr) / period_bytes(mode, hl));
+    cap = std::min(cap, kMaxTile);
+    if (max_tile > 0) cap = std::min(cap, max_tile);
+    return cap;
+}
+
+int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t st) {
+    if (!g || !cv) return fail(BLS_E_INVALID, "grid and curves are required");
+    if (g->n_segments < 0 || (g->n_segments > 0 && (!g->seg_offsets || !g->dur_offsets)))
+        return fail(BLS_E_INVALID, "bad segment table");
+    if (g->oversample < 1) return fail(BLS_E_INVALID, "oversample must be >= 1");
+    if (g->objective != 0 && g->objective != 1)
+        return fail(BLS_E_INVALID, "objective must be 'snr' or 'likelihood'");
+    if (cv->n_curves < 1 || !cv->offsets || !cv->t || !cv->y)
+        return fail(BLS_E_INVALID, "at least one light curve is required");
+    e->prepared = false;
+    e->graph_valid = false;
+    const int nc = cv->n_curves;
+    const int ns = g->n_segments;
+    const int o = g->oversample;
+    const int64_t P_total = ns > 0 ? g->seg_offsets[ns] - g->seg_offsets[0] : 0;
+    if (ns > 0 && g->seg_offsets[0] != 0) return fail(BLS_E_INVALID, "seg_offsets[0] must be 0");
+    const int64_t n_pts = cv->offsets[nc] - cv->offsets[0];
+    if (cv->offsets[0] != 0 || n_pts < 0) return fail(BLS_E_INVALID, "offsets[0] must be 0");
+
+    // ---- curves ---------------------------------------------------------------
+    int rc;
+    if ((rc = e->h_tau.ensure(sizeof(double) * std::max<int64_t>(n_pts, 1)))) return rc;
+    if ((rc = e->h_pay_r.ensure(sizeof(uint32_t) * std::max<int64_t>(n_pts, 1)))) return rc;
+    if ((rc = e->h_r64.ensure(sizeof(double) * std::max<int64_t>(n_pts, 1)))) return rc;
+    if ((rc = e->h_iv64.ensure(sizeof(double) * std::max<int64_t>(n_pts, 1)))) return rc;
+    std::vector<CurveHost> curves(nc);
+    int hw = std::max(1, (int)std::thread::hardware_concurrency());
+    std::vector<std::vector<double>> scratch(hw);
+    double* htau = e->h_tau.as<double>();
+    uint32_t* hpr = e->h_pay_r.as<uint32_t>();
+    double* hr64 = e->h_r64.as<double>();
+    double* hiv64 = e->h_iv64.as<double>();
+    parallel_for(nc, [&](int c, int w) {
+        const int64_t off = cv->offsets[c];
+        pack_curve(cv, c, off, htau + off, hpr + off, hr64 + off, hiv64 + off, curves[c],
+                   scratch[w]);
+        curves[c].d.out_off = (int64_t)c * P_total;
+    });
+    double tau_max = 0.0;
+    int n_uniform = 0;
+    for (int c = 0; c < nc; ++c) {
+        if (curves[c].status) return fail(curves[c].status, "%s", curves[c].err.c_str());
+        if (e->tune.exact_sweep) curves[c].d.exact_all = 1;
+        tau_max = std::max(tau_max, curves[c].tau_max);
+        n_uniform += curves[c].d.mode == MODE_UNIFORM;
+    }
+
+    // ---- segments and period constants (reference binning) ---------------------
+    std::vector<SegmentHost> segs(ns);
+    std::vector<double> per(P_total);
+    std::vector<PeriodConst> pc(P_total);
+    std::vector<int32_t> dur_all;
+    int max_hl = 2;
+    int fast_segments = 0;
+    for (int s = 0; s < ns; ++s) {
+        const int64_t p0 = g->seg_offsets[s], p1 = g->seg_offsets[s + 1];
+        const int64_t d0 = g->dur_offsets[s], d1 = g->dur_offsets[s + 1];
+        if (p1 < p0 || d1 < d0) return fail(BLS_E_INVALID, "segment %d: bad offsets", s);
+        SegmentHost& sh = segs[s];
+        SegmentDesc& sd = sh.d;
+        std::memset(&sd, 0, sizeof(sd));
+        sd.period_off = p0;
+        sd.n_periods = (int32_t)(p1 - p0);
+        sd.oversample = o;
+        sd.dur_off = (int32_t)dur_all.size();
+        if (p1 == p0) {
+            sh.empty_periods = true;
+            continue;
+        }
+        if (d1 == d0) return fail(BLS_E_INVALID, "segment %d has no durations", s);
+        double dmin = INFINITY, pmax = 0.0, fmax = 0.0;
+        for (int64_t i = d0; i < d1; ++i) {
+            const double d = g->durations[i];
+            if (!(std::isfinite(d) && d > 0.0))
+                return fail(BLS_E_INVALID, "segment %d: durations must be finite and > 0", s);
+            dmin = std::min(dmin, d);
+        }
+        for (int64_t i = p0; i < p1; ++i) {
+            const double P = g->periods[i];
+            if (!(std::isfinite(P) && P > 0.0))
+                return fail(BLS_E_INVALID,
+                            "BLS: trial periods must be finite and > 0 (segment %d)", s);
+            pmax = std::max(pmax, P);
+            per[i] = P;
+        }
+        const double bin = dmin / (double)o;                                  // _search_spec
+        for (int64_t i = d0; i < d1; ++i) {                                   // _duration_bins
+            const double kd = std::floor(g->durations[i] / bin + 0.5);
+            if (kd >= 1.0 && kd < 2147483647.0) {
+                const int32_t k = (int32_t)kd;
+                if (std::find(sh.dur.begin(), sh.dur.end(), k) == sh.dur.end()) sh.dur.push_back(k);
+            }
+        }
+        if ((int)sh.dur.size() > kMaxDur)
+            return fail(BLS_E_INVALID, "segment %d: more than %d distinct box widths", s, kMaxDur);
+        const double wmax = std::ceil(pmax / bin) + (double)o + 1.0;
+        if (!(wmax < 1073741824.0))
+            return fail(BLS_E_RESOURCE, "segment %d: %.3g phase bins per period", s, wmax);
+        const int64_t width = (int64_t)wmax;
+        int64_t hl = 2;
+        double smax = 0.0;
+        for (int64_t i = p0; i < p1; ++i) {
+            const double P = per[i];
+            const int64_t nb = period_bins(P, bin, o, width);
+            hl = std::max(hl, nb + 1);
+            fmax = std::max(fmax, 1.0 / P);
+            smax = std::max(smax, P / bin);
+        }
+        sd.width = (int32_t)width;
+        sd.bin_duration = bin;
+        sd.n_dur = (int32_t)sh.dur.size();
+        sd.hist_len = (int32_t)hl;
+        FoldParams fp = fold_params(width, bin, tau_max, fmax, smax);
+        const double scale = std::ldexp(1.0, fp.fb);
+        for (int64_t i = p0; i < p1 && fp.fast; ++i) {
+            const double P = per[i];
+            const double sc = std::nearbyint((P / bin) * scale);
+            const int64_t nb = period_bins(P, bin, o, width);
+            if (!(sc >= 1.0 && sc < 4294967296.0)) { fp.fast = false; break; }
+            const uint32_t S = (uint32_t)sc;
+            // the fast fold's largest bin, ((S - 1) >> fb) + 1, must stay inside n_bins
+            if ((int64_t)((S - 1u) >> fp.fb) + 1 > nb) { fp.fast = false; break; }
+        }
+        for (int64_t i = p0; i < p1; ++i) {
+            const double P = per[i];
+            pc[i].f = 1.0 / P;
+            pc[i].nb = (int32_t)period_bins(P, bin, o, width);
+            pc[i].S = fp.fast ? (uint32_t)std::nearbyint((P / bin) * scale) : 0u;
+        }
+        sd.fast_fold = fp.fast;
+        sd.frac_bits = fp.fast ? fp.fb : 0;
+        sd.margin_u = fp.mu;
+        sd.margin_phi = fp.mphi;
+        fast_segments += fp.fast;
+        max_hl = std::max<int>(max_hl, (int)hl);
+        dur_all.insert(dur_all.end(), sh.dur.begin(), sh.dur.end());
+    }
+
+    // ---- shared memory, tiles, work items (largest first) ----------------------
+    size_t smem = e->tune.smem_per_cta > 0 ? (size_t)e->tune.smem_per_cta : kDefaultSmem;
+    bool modes[2] = {n_uniform > 0, n_uniform < nc};
+    for (int s = 0; s < ns; ++s) {
+        if (segs[s].empty_periods) continue;
+        for (int m = 0; m < 2; ++m) {
+            if (!modes[m]) continue;
+            const size_t need = screen_bytes(m, segs[s].d.hist_len) + 16 +
+                                period_bytes(m, segs[s].d.hist_len);
+            if (need > smem) smem = need;
+        }
+    }
+    smem = (smem + 15) & ~size_t(15);
+    if (smem > e->smem_optin)
+        return fail(BLS_E_RESOURCE,
+                    "BLS: %zu bytes of shared memory per period exceed the device's %zu; "
+                    "narrow the period range (max_period_days)",
+                    smem, e->smem_optin);
+    struct ItemCost {
+        WorkItem w;
+        double cost;
+        int mode;
+    };
+    std::vector<ItemCost> items;
+    double folds = 0.0, boxes = 0.0, trials = 0.0;
+    for (int c = 0; c < nc; ++c) {
+        const int m = curves[c].d.mode;
+        for (int s = 0; s < ns; ++s) {
+            const SegmentHost& sh = segs[s];
+            if (sh.empty_periods) continue;
+            const int hl = sh.d.hist_len;
+            const int cap = tile_cap(m, hl, smem, e->tune.max_tile);
+            if (cap < 1) return fail(BLS_E_RESOURCE, "segment %d does not fit shared memory", s);
+            double box_per_period = 0.0;
+            for (int32_t k : sh.dur) box_per_period += std::max(0, hl - k);
+            for (int32_t p = 0; p < sh.d.n_periods; p += cap) {
+                ItemCost it;
+                it.w.curve = c;
+                it.w.segment = s;
+                it.w.p_begin = p;
+                it.w.p_count = std::min(cap, sh.d.n_periods - p);
+                it.mode = m;
+                it.cost = it.w.p_count * ((double)curves[c].d.n_points + 1.2 * box_per_period);
+                items.push_back(it);
+            }
+            const int64_t p0 = sh.d.period_off;
+            for (int32_t p = 0; p < sh.d.n_periods; ++p) {
+                const int nb = pc[p0 + p].nb;
+                for (int32_t k : sh.dur)
+                    if (k < nb) boxes += (double)(nb - k + 1);
+            }
+            folds += (double)curves[c].d.n_points * sh.d.n_periods;
+            trials += (double)sh.d.n_periods * sh.dur.size();
+        }
+    }
+    std::stable_sort(items.begin(), items.end(), [](const ItemCost& a, const ItemCost& b) {
+        if (a.mode != b.mode) return a.mode < b.mode;
+        return a.cost > b.cost;
+    });
+
+    // ---- stage metadata and upload ---------------------------------------------
+    const size_t n_items = items.size();
+    const size_t grid_bytes = (size_t)P_total * (8 + 8 + 4 + 4) + dur_all.size() * 4 + 64;
+    const size_t meta_bytes = sizeof(CurveDesc) * nc + sizeof(SegmentDesc) * std::max(ns, 1) +
+                              sizeof(WorkItem) * std::max<size_t>(n_items, 1) + 64;
+    if ((rc = e->h_grid.ensure(grid_bytes))) return rc;
+    if ((rc = e->h_meta.ensure(meta_bytes))) return rc;
+    char* gp = e->h_grid.as<char>();
+    double* hper = reinterpret_cast<double*>(gp);
+    double* hfreq = hper + P_total;
+    uint32_t* hscale = reinterpret_cast<uint32_t*>(hfreq + P_total);
+    int32_t* hnb = reinterpret_cast<int32_t*>(hscale + P_total);
+    int32_t* hdur = hnb + P_total;
+    for (int64_t i = 0; i < P_total; ++i) {
+        hper[i] = per[i];
+        hfreq[i] = pc[i].f;
+        hscale[i] = pc[i].S;
+        hnb[i] = pc[i].nb;
+    }
+    std::copy(dur_all.begin(), dur_all.end(), hdur);
+    char* mp = e->h_meta.as<char>();
+    CurveDesc* hcur = reinterpret_cast<CurveDesc*>(mp);
+    SegmentDesc* hseg = reinterpret_cast<SegmentDesc*>(hcur + nc);
+    WorkItem* hitem = reinterpret_cast<WorkItem*>(hseg + std::max(ns, 1));
+    for (int c = 0; c < nc; ++c) hcur[c] = curves[c].d;
+    for (int s = 0; s < ns; ++s) hseg[s] = segs[s].d;
+    e->n_items_mode[0] = e->n_items_mode[1] = 0;
+    for (size_t i = 0; i < n_items; ++i) {
+        hitem[i] = items[i].w;
+        e->n_items_mode[items[i].mode]++;
+    }
+
+    const size_t out_elems = (size_t)kFields * nc * std::max<int64_t>(P_total, 1);
+    if ((rc = e->d_tau.ensure(sizeof(double) * std::max<int64_t>(n_pts, 1)))) return rc;
+    if ((rc = e->d_pay_r.ensure(sizeof(uint32_t) * std::max<int64_t>(n_pts, 1)))) return rc;
+    if ((rc = e->d_r64.ensure(sizeof(double) * std::max<int64_t>(n_pts, 1)))) return rc;
+    if ((rc = e->d_iv64.ensure(sizeof(double) * std::max<int64_t>(n_pts, 1)))) return rc;
+    if ((rc = e->d_period.ensure(grid_bytes))) return rc;
+    if ((rc = e->d_curves.ensure(meta_bytes))) return rc;
+    if ((rc = e->d_out.ensure(sizeof(double) * out_elems))) return rc;
+    if ((rc = e->d_ctl.ensure(64))) return rc;
+    int64_t h2d = 0;
+    CUDA_TRY(cudaMemcpyAsync(e->d_tau.p, htau, sizeof(double) * n_pts, cudaMemcpyHostToDevice, st),
+             "upload times");
+    CUDA_TRY(cudaMemcpyAsync(e->d_pay_r.p, hpr, sizeof(uint32_t) * n_pts, cudaMemcpyHostToDevice,
+                             st),
+             "upload flux words");
+    h2d += (int64_t)n_pts * 12;
+    if (n_uniform < nc) {
+        CUDA_TRY(cudaMemcpyAsync(e->d_r64.p, hr64, sizeof(double) * n_pts, cudaMemcpyHostToDevice,
+                                 st),
+                 "upload flux*weight");
+        CUDA_TRY(cudaMemcpyAsync(e->d_iv64.p, hiv64, sizeof(double) * n_pts,
+                                 cudaMemcpyHostToDevice, st),
+                 "upload weights");
+        h2d += (int64_t)n_pts * 16;
+    }
+    CUDA_TRY(cudaMemcpyAsync(e->d_period.p, gp, grid_bytes, cudaMemcpyHostToDevice, st),
+             "upload grid");
+    CUDA_TRY(cudaMemcpyAsync(e->d_curves.p, mp, meta_bytes, cudaMemcpyHostToDevice, st),
+             "upload descriptors");
+    h2d += (int64_t)(grid_bytes + meta_bytes);
+    CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, 64, st), "reset control words");
+    CUDA_TRY(configure_search(smem), "shared-memory opt-in");
+
+    const char* dgp = e->d_period.as<char>();
+    const double* dper = reinterpret_cast<const double*>(dgp);
+    const double* dfreq = dper + P_total;
+    const uint32_t* dscale = reinterpret_cast<const uint32_t*>(dfreq + P_total);
+    const int32_t* dnb = reinterpret_cast<const int32_t*>(dscale + P_total);
+    const int32_t* ddur = dnb + P_total;
+    const char* dmp = e->d_curves.as<char>();
+    const CurveDesc* dcur = reinterpret_cast<const CurveDesc*>(dmp);
+    const SegmentDesc* dseg = reinterpret_cast<const SegmentDesc*>(dcur + nc);
+    const WorkItem* ditem = reinterpret_cast<const WorkItem*>(dseg + std::max(ns, 1));
+    int32_t* ctl = e->d_ctl.as<int32_t>();
+    int ctas_total = 0;
+    for (int m = 0; m < 2; ++m) {
+        BatchArgs& a = e->args[m];
+        a.curves = dcur;
+        a.segments = dseg;
+        a.items = ditem + (m == 0 ? 0 : e->n_items_mode[0]);
+        a.n_items = e->n_items_mode[m];
+        a.tau = e->d_tau.as<double>();
+        a.pay_r = e->d_pay_r.as<uint32_t>();
+        a.r64 = e->d_r64.as<double>();
+        a.iv64 = e->d_iv64.as<double>();
+        a.period = dper;
+        a.freq = dfreq;
+        a.scale = dscale;
+        a.nbins = dnb;
+        a.dur_bins = ddur;
+        a.out = e->d_out.as<double>();
+        a.out_stride = (int64_t)nc * P_total;
+        a.work_counter = ctl + m;
+        a.error_flag = ctl + 8;
+        a.debug_prefix = nullptr;
+        a.obj_flag = g->objective;
+        const int per_sm = std::max(1, max_resident_ctas(m, smem));
+        e->ctas_mode[m] = std::min(a.n_items, e->n_sm * per_sm);
+        ctas_total = std::max(ctas_total, e->ctas_mode[m]);
+    }
+    e->smem = smem;
+    e->n_curves = nc;
+    e->n_periods = P_total;
+    BlsBatchInfo& in = e->info;
+    in.n_curves = nc;
+    in.n_segments = ns;
+    in.n_periods = P_total;
+    in.n_items = (int64_t)n_items;
+    in.n_points = n_pts;
+    in.folds = folds;
+    in.boxes = boxes;
+    in.trials = trials;
+    in.h2d_bytes = h2d;
+    in.ctas = ctas_total;
+    in.smem_per_cta = (int32_t)smem;
+    in.uniform_curves = n_uniform;
+    in.fast_fold_segments = fast_segments;
+    e->prepared = true;
+    return BLS_OK;
+}
+
+// Enqueue one search (both accumulation modes) on `st`.
+int enqueue_search(BlsEngine* e, cudaStream_t st) {
+    CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, 2 * sizeof(int32_t), st), "reset work counters");
+    for (int m = 0; m < 2; ++m) {
+        if (e->args[m].n_items <= 0) continue;
+        CUDA_TRY(launch_search(e->args[m], m, e->ctas_mode[m], e->smem, st), "search launch");
+    }
+    return BLS_OK;
+}
+
+int check_device_flag(BlsEngine* e, cudaStream_t st) {
+    int rc;
+    if ((rc = e->h_ctl.ensure(64))) return rc;
+    int32_t* h = e->h_ctl.as<int32_t>();
+    CUDA_TRY(cudaMemcpyAsync(h, e->d_ctl.as<int32_t>() + 8, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             st),
+             "read error flag");
+    CUDA_TRY(cudaStreamSynchronize(st), "synchronize");
+    if (h[0] != 0) return fail(BLS_E_DEVICE, "a kernel met an impossible work descriptor");
+    return BLS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bls_last_error(void) { return g_error.c_str(); }
+
+int bls_engine_create(const BlsTune* tune, BlsEngine** engine) {
+    if (!engine) return fail(BLS_E_INVALID, "engine pointer is NULL");
+    *engine = nullptr;
+    BlsEngine* e = new BlsEngine();
+    if (tune) e->tune = *tune;
+    else {
+        e->tune.device = -1;
+        e->tune.use_graph = 1;
+    }
+    int dev = e->tune.device;
+    if (dev < 0) {
+        cudaError_t err = cudaGetDevice(&dev);
+        if (err != cudaSuccess) { delete e; return cuda_fail(err, "no CUDA device"); }
+    }
+    e->device = dev;
+    cudaError_t err = cudaSetDevice(dev);
+    if (err != cudaSuccess) { delete e; return cuda_fail(err, "cudaSetDevice"); }
+    cudaDeviceGetAttribute(&e->n_sm, cudaDevAttrMultiProcessorCount, dev);
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    e->smem_optin = (size_t)optin > 1024 ? (size_t)optin - 1024 : 0;   // static shared state
+    err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) { delete e; return cuda_fail(err, "cudaStreamCreate"); }
+    *engine = e;
+    return BLS_OK;
+}
+
+int bls_engine_destroy(BlsEngine* engine) {
+    if (!engine) return BLS_OK;
+    cudaSetDevice(engine->device);
+    cudaStreamSynchronize(engine->stream);
+    delete engine;
+    return BLS_OK;
+}
+
+int bls_prepare(BlsEngine* e, const BlsGrid* grid, const BlsCurves* curves, void* stream) {
+    if (!e) return fail(BLS_E_INVALID, "engine is NULL");
+    cudaSetDevice(e->device);
+    return do_prepare(e, grid, curves, pick(e, stream));
+}
+
+int bls_launch(BlsEngine* e, void* stream) {
+    if (!e) return fail(BLS_E_INVALID, "engine is NULL");
+    if (!e->prepared) return fail(BLS_E_STATE, "bls_launch before bls_prepare");
+    cudaSetDevice(e->device);
+    cudaStream_t st = pick(e, stream);
+    if (!e->tune.use_graph) return enqueue_search(e, st);
+    if (!e->graph_valid) {
+        if (e->graph) {
+            cudaGraphExecDestroy(e->graph);
+            e->graph = nullptr;
+        }
+        // capture on the engine's own stream, ordered after the caller's stream
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(cudaStreamSynchronize(st), "synchronize before capture");
+        CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal),
+                 "begin capture");
+        int rc = enqueue_search(e, e->stream);
+        cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return cuda_fail(ce, "end capture");
+        ce = cudaGraphInstantiate(&e->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return cuda_fail(ce, "graph instantiate");
+        e->graph_valid = true;
+    }
+    CUDA_TRY(cudaGraphLaunch(e->graph, st), "graph launch");
+    return BLS_OK;
+}
+
+int bls_download(BlsEngine* e, double* out, void* stream) {
+    if (!e || !out) return fail(BLS_E_INVALID, "engine and output are required");
+    if (!e->prepared) return fail(BLS_E_STATE, "bls_download before bls_prepare");
+    cudaSetDevice(e->device);
+    cudaStream_t st = pick(e, stream);
+    const size_t bytes = sizeof(double) * kFields * e->n_curves * e->n_periods;
+    if (bytes) CUDA_TRY(cudaMemcpyAsync(out, e->d_out.p, bytes, cudaMemcpyDeviceToHost, st),
+                        "download outputs");
+    return check_device_flag(e, st);
+}
+
+int bls_device_output(BlsEngine* e, const double** out) {
+    if (!e || !out) return fail(BLS_E_INVALID, "engine and output are required");
+    if (!e->prepared) return fail(BLS_E_STATE, "no prepared batch");
+    *out = e->d_out.as<double>();
+    return BLS_OK;
+}
+
+int bls_download_best(BlsEngine* e, int64_t* best_index, double* best_power, double* power_mean,
+                      double* power_std, void* stream) {
+    if (!e || !best_index || !best_power || !power_mean || !power_std)
+        return fail(BLS_E_INVALID, "engine and outputs are required");
+    if (!e->prepared) return fail(BLS_E_STATE, "bls_download_best before bls_prepare");
+    cudaSetDevice(e->device);
+    cudaStream_t st = pick(e, stream);
+    const int nc = e->n_curves;
+    const size_t bytes = (size_t)nc * (8 * 4);
+    int rc;
+    if ((rc = e->d_best.ensure(bytes))) return rc;
+    if ((rc = e->h_best.ensure(bytes))) return rc;
+    int64_t* di = e->d_best.as<int64_t>();
+    double* dv = reinterpret_cast<double*>(di + nc);
+    CUDA_TRY(launch_best(e->d_out.as<double>(), nc, e->n_periods, di, dv, dv + nc, dv + 2 * nc, st),
+             "best-of-spectrum launch");
+    CUDA_TRY(cudaMemcpyAsync(e->h_best.p, e->d_best.p, bytes, cudaMemcpyDeviceToHost, st),
+             "download best");
+    if ((rc = check_device_flag(e, st))) return rc;
+    const int64_t* hi = e->h_best.as<int64_t>();
+    const double* hv = reinterpret_cast<const double*>(hi + nc);
+    std::memcpy(best_index, hi, sizeof(int64_t) * nc);
+    std::memcpy(best_power, hv, sizeof(double) * nc);
+    std::memcpy(power_mean, hv + nc, sizeof(double) * nc);
+    std::memcpy(power_std, hv + 2 * nc, sizeof(double) * nc);
+    return BLS_OK;
+}
+
+int bls_search(BlsEngine* e, const BlsGrid* grid, const BlsCurves* curves, double* out,
+               void* stream) {
+    int rc;
+    if ((rc = bls_prepare(e, grid, curves, stream))) return rc;
+    if ((rc = bls_launch(e, stream))) return rc;
+    return bls_download(e, out, stream);
+}
+
+int bls_batch_info(BlsEngine* e, BlsBatchInfo* info) {
+    if (!e || !info) return fail(BLS_E_INVALID, "engine and info are required");
+    if (!e->prepared) return fail(BLS_E_STATE, "no prepared batch");
+    *info = e->info;
+    return BLS_OK;
+}
+
+int bls_debug_prefix(BlsEngine* e, const double* t, const double* y, const double* dy, int64_t n,
+                     double period, const double* durations, int32_t n_durations,
+                     int32_t oversample, double* yw_prefix, double* ivar_prefix,
+                     int32_t* n_bins) {
+    if (!e || !t || !y || !durations || !yw_prefix || !ivar_prefix || !n_bins || n < 1 ||
+        n_durations < 1)
+        return fail(BLS_E_INVALID, "bad arguments");
+    cudaSetDevice(e->device);
+    const int64_t seg_off[2] = {0, 1};
+    const int64_t dur_off[2] = {0, n_durations};
+    BlsGrid g{1, seg_off, &period, dur_off, durations, oversample, 0};
+    const int64_t offs[2] = {0, n};
+    BlsCurves c{1, offs, t, y, dy};
+    int rc;
+    if ((rc = do_prepare(e, &g, &c, e->stream))) return rc;
+    const int mode = e->args[0].n_items > 0 ? 0 : 1;
+    int32_t hl = 0;
+    CUDA_TRY(cudaStreamSynchronize(e->stream), "synchronize");
+    {
+        const char* dmp = e->d_curves.as<char>();
+        const SegmentDesc* dseg =
+            reinterpret_cast<const SegmentDesc*>(reinterpret_cast<const CurveDesc*>(dmp) + 1);
+        SegmentDesc sd;
+        CUDA_TRY(cudaMemcpy(&sd, dseg, sizeof(sd), cudaMemcpyDeviceToHost), "read segment");
+        hl = sd.hist_len;
+    }
+    DevBuf dbg;
+    if ((rc = dbg.ensure(sizeof(double) * 2 * (size_t)hl))) return rc;
+    int32_t nb = 0;
+    CUDA_TRY(cudaMemcpy(&nb, e->args[0].nbins, sizeof(int32_t), cudaMemcpyDeviceToHost),
+             "read n_bins");
+    e->args[mode].debug_prefix = dbg.as<double>();
+    rc = enqueue_search(e, e->stream);
+    e->args[mode].debug_prefix = nullptr;
+    e->graph_valid = false;
+    if (rc) { dbg.release(); return rc; }
+    cudaError_t ce = cudaMemcpyAsync(yw_prefix, dbg.p, sizeof(double) * (nb + 1),
+                                     cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(ivar_prefix, dbg.as<double>() + hl, sizeof(double) * (nb + 1),
+                             cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    dbg.release();
+    if (ce != cudaSuccess) return cuda_fail(ce, "debug prefix");
+    *n_bins = nb;
+    return check_device_flag(e, e->stream);
+}
+
+int bls_debug_fold_bins(BlsEngine* e, const double* t, int64_t n, double period,
+                        double bin_duration, int32_t width, int32_t* bins, int32_t* used_fast) {
+    if (!e || !t || !bins || !used_fast || n < 1 || n > (1 << 30))
+        return fail(BLS_E_INVALID, "bad arguments");
+    if (!(period > 0.0) || !(bin_duration > 0.0) || width < 2)
+        return fail(BLS_E_INVALID, "period, bin width and width must be positive");
+    cudaSetDevice(e->device);
+    std::vector<double> tau(n);
+    double t_min = t[0], tau_max = 0.0;
+    for (int64_t j = 0; j < n; ++j) t_min = std::min(t_min, t[j]);
+    for (int64_t j = 0; j < n; ++j) {
+        tau[j] = t[j] - t_min;
+        tau_max = std::max(tau_max, tau[j]);
+    }
+    FoldParams fp = fold_params(width, bin_duration, tau_max, 1.0 / period, period / bin_duration);
+    uint32_t S = 0;
+    if (fp.fast) {
+        const double sc = std::nearbyint((period / bin_duration) * std::ldexp(1.0, fp.fb));
+        if (sc >= 1.0 && sc < 4294967296.0) S = (uint32_t)sc;
+        else fp.fast = false;
+    }
+    DevBuf d_t, d_b, d_u;
+    int rc;
+    if ((rc = d_t.ensure(sizeof(double) * n)) || (rc = d_b.ensure(sizeof(int32_t) * n)) ||
+        (rc = d_u.ensure(sizeof(int32_t) * n))) {
+        d_t.release(); d_b.release(); d_u.release();
+        return rc;
+    }
+    cudaStream_t st = e->stream;
+    cudaError_t ce = cudaMemcpyAsync(d_t.p, tau.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess)
+        ce = launch_fold_bins(d_t.as<double>(), (int)n, period, 1.0 / period, S, bin_duration, width,
+                              fp.fb, fp.mu, fp.mphi, fp.fast ? 1 : 0, d_b.as<int32_t>(),
+                              d_u.as<int32_t>(), st);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(bins, d_b.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(used_fast, d_u.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    d_t.release(); d_b.release(); d_u.release();
+    if (ce != cudaSuccess) return cuda_fail(ce, "fold bins");
+    return BLS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,779 @@
+// B200 box-least-squares search kernels (sm_100a).
+//
+// One persistent launch processes work items of (curve, segment, tile of up to
+// kMaxTile consecutive trial periods).  Per item a CTA
+//   1. folds every point of the curve into one shared-memory histogram per
+//      period of the tile.  The phase bin is the reference's
+//      w = x - P*floor(x/P); ind = int(w/bin) + 1   (cuPeriod
+//      src/cuperiod/methods/_bls_core.py:369-376 / 536-538), computed by a fast
+//      FP64 path -- q = x * RN(1/P) rounded onto a 2^-32 grid, then one 32-bit
+//      multiply-high by P/bin -- whose result is used only when it is provably
+//      the reference's (the scaled phase is further than the combined rounding
+//      error from a cycle or bin edge); otherwise the reference's own IEEE chain
+//      runs.  With one weight for every point the bin sums are exact integers
+//      built with native 32-bit shared atomics only (64-bit and floating-point
+//      shared atomics are emulated on sm_100): each point adds the unsigned low
+//      13 bits and the signed high part of r_q (its quantised centred
+//      flux*weight) to two words and 1 to the bin's count.  With per-point
+//      weights the two sums stay FP64.  A lane holds 8 time-consecutive points
+//      and merges equal bins in registers before it touches shared memory;
+//   2. per period: applies the reference's wrap pad (_bls_core.py:377-381),
+//      turns the bins into prefix sums in place and writes an FP32 screen copy;
+//   3. sweeps every (duration, start) box.  An FP32 bound on the box objective
+//      -- maximising snr (or the log-likelihood) is maximising
+//      t^2 / (iv_in iv_out) (or t^2 / (iv_in iv_out^2)) with t = y_in - ybar iv_in
+//      -- discards every box that provably cannot be the period's best; the few
+//      that remain are evaluated with the reference's FP64 formulas
+//      (_bls_core.py:410-426) on the exact sums, and the winner is the first in
+//      (duration index, start) order among equals, as in the reference;
+//   4. writes the reference's seven per-period fields (_bls_core.py:443-460).
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "bls_device.h"
+#include "bls_launch.h"
+
+namespace blsb200 {
+namespace {
+
+constexpr int kThreads = kChunkThreads;
+constexpr int kWarps = kThreads / 32;
+constexpr int kPts = kChunkPts;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr float kRel = 1.0f / 262144.0f;    // 2^-18: relative slack of FP32 key bounds
+constexpr int kCasLimit = 1 << 16;          // retries of one FP64 shared add
+
+struct TileShared {
+    WorkItem item;
+    CurveDesc curve;
+    SegmentDesc seg;
+    double per[kMaxTile];
+    double freq[kMaxTile];
+    uint32_t scale[kMaxTile];
+    int32_t nb[kMaxTile];
+    int32_t dur[kMaxDur];
+    uint32_t tot_a[kWarps];
+    int32_t tot_b[kWarps];
+    uint32_t tot_c[kWarps];
+    double tot_rd[kWarps];
+    double tot_wd[kWarps];
+    float red_f[kWarps];
+    float red_t[kWarps];
+    double red_v[kWarps];
+    int red_di[kWarps];
+    int red_n[kWarps];
+    int next;
+};
+
+// The reference's IEEE fold (no contraction): the fallback of the fast path.
+__device__ __forceinline__ int fold_exact(double x, double P, double bin, int width) {
+    const double q = __ddiv_rn(x, P);
+    const double w = __dsub_rn(x, __dmul_rn(P, floor(q)));
+    int ind = (int)__ddiv_rn(w, bin) + 1;
+    ind = ind < 0 ? 0 : ind;
+    ind = ind > width - 1 ? width - 1 : ind;
+    return ind;
+}
+
+// Fast fold.  Returns the reference's bin when the scaled phase is provably away
+// from every edge, else -1.
+__device__ __forceinline__ int fold_fast(double x, double f, uint32_t S, int fb, uint32_t fmask,
+                                         uint32_t mu, uint32_t fr_span, uint32_t mphi,
+                                         uint32_t phi_span) {
+    const double q = __dmul_rn(x, f);
+    const double qm = __dadd_rn(q, 1572864.0);          // 1.5 * 2^20: ulp 2^-32
+    const uint32_t phi = (uint32_t)__double2loint(qm);   // round(frac(q) * 2^32)
+    const uint32_t v = __umulhi(phi, S);                 // phase * P/bin * 2^fb
+    const bool ok = ((phi - mphi) < phi_span) & (((v & fmask) - mu) < fr_span);
+    return ok ? (int)(v >> fb) + 1 : -1;
+}
+
+// FP64 add to a shared-memory word by a bounded compare-and-swap loop in the
+// shared state space.  The loop is lock-free (a failed swap means another thread
+// succeeded); the bound only guards against the impossible and sets `flag`.
+__device__ __forceinline__ void shared_add_f64(double* p, double v, int32_t* flag) {
+    if (v == 0.0) return;
+    const unsigned addr = (unsigned)__cvta_generic_to_shared(p);
+    unsigned long long old;
+    asm volatile("ld.shared.u64 %0, [%1];" : "=l"(old) : "r"(addr) : "memory");
+    for (int it = 0; it < kCasLimit; ++it) {
+        const unsigned long long want = __double_as_longlong(__longlong_as_double(old) + v);
+        unsigned long long seen;
+        asm volatile("atom.shared.cas.b64 %0, [%1], %2, %3;"
+                     : "=l"(seen) : "r"(addr), "l"(old), "l"(want) : "memory");
+        if (seen == old) return;
+        old = seen;
+    }
+    atomicExch(flag, 2);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+
+// (v, di, n) is better than (w, dj, m): larger objective, then earlier
+// (duration index, start) -- the reference's first-wins order.
+__device__ __forceinline__ bool better(double v, int di, int n, double w, int dj, int m) {
+    if (v > w) return true;
+    if (v < w || !(v == w)) return false;
+    return di < dj || (di == dj && n < m);
+}
+
+// Exact sums of one box, in the reference's units.
+struct BoxSums {
+    double y_in, iv_in;
+};
+
+// The reference's objective of one box (_bls_core.py:410-426); -inf when the box
+// is not admissible.
+__device__ __forceinline__ double box_objective(const BoxSums& s, const CurveDesc& c, int obj) {
+    const double iv_out = c.sum_ivar - s.iv_in;
+    if (!(s.iv_in >= c.ivar_floor) || !(iv_out >= c.ivar_floor)) return -CUDART_INF;
+    const double yin = s.y_in / s.iv_in;
+    const double yout = (c.sum_y - s.y_in) / iv_out;
+    if (yout < yin) return -CUDART_INF;
+    const double depth = yout - yin;
+    if (obj == 0) return depth / sqrt(1.0 / s.iv_in + 1.0 / iv_out);
+    return 0.5 * s.iv_in * depth * depth;
+}
+
+// Bins held per period, rounded so each per-period array starts 16-byte aligned.
+__device__ __host__ __forceinline__ int padded_bins(int hl) { return (hl + 3) & ~3; }
+
+// Histogram layout of one period (hlp = padded_bins(hl) bins).
+//  UNIFORM: A[hlp] (sum of the low 13 bits of r_q), B[hlp] (sum of its signed
+//           high part), C[hlp] (count) -- all 32-bit; prefix sums in place.
+//  GENERAL: R[hlp], W[hlp] -- FP64 sums of the scaled centred flux*weight and
+//           of the scaled weight; prefix sums in place.
+template <int MODE>
+__device__ __host__ __forceinline__ size_t hist_period_bytes(int hl) {
+    return (size_t)padded_bins(hl) * (MODE == MODE_UNIFORM ? 12 : 16);
+}
+
+template <int MODE>
+struct PointRegs {
+    double x[kPts];
+    uint32_t lo[MODE == MODE_UNIFORM ? kPts : 1], hi[MODE == MODE_UNIFORM ? kPts : 1];
+    double rv[MODE == MODE_GENERAL ? kPts : 1], iv[MODE == MODE_GENERAL ? kPts : 1];
+};
+
+template <int MODE, bool TAIL>
+__device__ __forceinline__ void load_points(const BatchArgs& a, const CurveDesc& c, int base,
+                                            PointRegs<MODE>& p) {
+    const int tid = threadIdx.x;
+    const double* __restrict__ tau = a.tau + c.point_off;
+#pragma unroll
+    for (int r = 0; r < kPts; ++r) {
+        const int j = base + r * kThreads + tid;
+        const bool ok = !TAIL || j < c.n_points;
+        p.x[r] = ok ? __ldg(tau + j) : -1.0;
+        if (MODE == MODE_UNIFORM) {
+            const uint32_t w = ok ? __ldg(a.pay_r + c.point_off + j) : 0u;
+            p.lo[r] = w & 0xffffu;
+            p.hi[r] = (uint32_t)((int32_t)w >> 16);    // signed high part
+        } else {
+            p.rv[r] = ok ? __ldg(a.r64 + c.point_off + j) : 0.0;
+            p.iv[r] = ok ? __ldg(a.iv64 + c.point_off + j) : 0.0;
+        }
+    }
+}
+
+template <int MODE>
+__device__ __forceinline__ void flush_run(unsigned char* hq, int hlp, int bin, uint32_t sa,
+                                          uint32_t sb, uint32_t sc, double sr, double sw,
+                                          int32_t* flag) {
+    if (MODE == MODE_UNIFORM) {
+        uint32_t* A = reinterpret_cast<uint32_t*>(hq);
+        atomicAdd(A + bin, sa);
+        atomicAdd(A + hlp + bin, sb);
+        atomicAdd(A + 2 * hlp + bin, sc);
+    } else {
+        double* R = reinterpret_cast<double*>(hq);
+        shared_add_f64(R + bin, sr, flag);
+        shared_add_f64(R + hlp + bin, sw, flag);
+    }
+}
+
+template <int MODE, bool TAIL>
+__device__ __forceinline__ void fold_points(const TileShared& s, unsigned char* hist_base,
+                                            const PointRegs<MODE>& p, int pt, int hl,
+                                            int32_t* flag) {
+    const SegmentDesc& g = s.seg;
+    const int fb = g.frac_bits;
+    const uint32_t fmask = (1u << fb) - 1u;
+    const uint32_t mu = g.margin_u;
+    const uint32_t fr_span = (1u << fb) - 2u * mu;
+    const uint32_t mphi = g.margin_phi;
+    const uint32_t phi_span = 0u - 2u * mphi;
+    const bool fast = g.fast_fold != 0;
+    const double bin = g.bin_duration;
+    const int width = g.width;
+    const int hlp = padded_bins(hl);
+    for (int q = 0; q < pt; ++q) {
+        const double f = s.freq[q];
+        const double P = s.per[q];
+        const uint32_t S = s.scale[q];
+        const int nbq = s.nb[q];
+        unsigned char* hq = hist_base + (size_t)q * hist_period_bytes<MODE>(hl);
+        // the lane's run of equal bins, flushed to shared memory when the bin changes
+        int cur = -1;
+        uint32_t sa = 0u, sb = 0u, sc = 0u;
+        double sr = 0.0, sw = 0.0;
+#pragma unroll
+        for (int r = 0; r < kPts; ++r) {
+            if (TAIL && p.x[r] < 0.0) continue;
+            int ind = fast ? fold_fast(p.x[r], f, S, fb, fmask, mu, fr_span, mphi, phi_span) : -1;
+            if (ind < 0) {
+                ind = fold_exact(p.x[r], P, bin, width);
+                if (ind > nbq) continue;     // a bin the reference never reads
+            }
+            if (ind != cur) {
+                if (cur >= 0) flush_run<MODE>(hq, hlp, cur, sa, sb, sc, sr, sw, flag);
+                cur = ind;
+                sa = sb = sc = 0u;
+                sr = sw = 0.0;
+            }
+            if (MODE == MODE_UNIFORM) {
+                sa += p.lo[r];
+                sb += p.hi[r];
+                sc += 1u;
+            } else {
+                sr += p.rv[r];
+                sw += p.iv[r];
+            }
+        }
+        if (cur >= 0) flush_run<MODE>(hq, hlp, cur, sa, sb, sc, sr, sw, flag);
+    }
+}
+
+// Exact prefix of r_q at bin i from the two 32-bit prefix words.
+__device__ __forceinline__ long long prefix_r(const uint32_t* A, const int32_t* B, int i) {
+    return (long long)B[i] * (1ll << kHalfBits) + (long long)A[i];
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ TileShared s;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s.next = atomicAdd(a.work_counter, 1);
+        __syncthreads();
+        const int it = s.next;
+        if (it >= a.n_items) break;
+        if (tid == 0) {
+            s.item = a.items[it];
+            s.curve = a.curves[s.item.curve];
+            s.seg = a.segments[s.item.segment];
+        }
+        __syncthreads();
+        const int pt = s.item.p_count;
+        const int hl = s.seg.hist_len;
+        const int n_dur = s.seg.n_dur;
+        if (pt < 1 || pt > kMaxTile || n_dur < 0 || n_dur > kMaxDur || hl < 2) {
+            if (tid == 0) atomicExch(a.error_flag, 1);
+            continue;
+        }
+        const int64_t g0 = s.seg.period_off + s.item.p_begin;
+        if (tid < pt) {
+            s.per[tid] = a.period[g0 + tid];
+            s.freq[tid] = a.freq[g0 + tid];
+            s.scale[tid] = a.scale[g0 + tid];
+            s.nb[tid] = a.nbins[g0 + tid];
+        }
+        if (tid < n_dur) s.dur[tid] = a.dur_bins[s.seg.dur_off + tid];
+        __syncthreads();
+
+        double* out = a.out + s.curve.out_off + g0;
+        const int64_t ostride = a.out_stride;
+        if (s.curve.skip || n_dur == 0) {       // nothing admissible anywhere
+            if (tid < pt) {
+                out[tid] = -CUDART_INF;
+                for (int f = 1; f < kFields; ++f) out[f * ostride + tid] = 0.0;
+            }
+            continue;
+        }
+
+        // ---- 1. fold ---------------------------------------------------------
+        const size_t pbytes = hist_period_bytes<MODE>(hl);
+        const int hlp = padded_bins(hl);
+        {
+            const int n16 = (int)((pt * pbytes) / 16);
+            uint4* z = reinterpret_cast<uint4*>(smem);
+            for (int i = tid; i < n16; i += kThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
+        }
+        __syncthreads();
+        {
+            const int n = s.curve.n_points;
+            int base = 0;
+            for (; base + kChunk <= n; base += kChunk) {
+                PointRegs<MODE> p;
+                load_points<MODE, false>(a, s.curve, base, p);
+                fold_points<MODE, false>(s, smem, p, pt, hl, a.error_flag);
+            }
+            if (base < n) {
+                PointRegs<MODE> p;
+                load_points<MODE, true>(a, s.curve, base, p);
+                fold_points<MODE, true>(s, smem, p, pt, hl, a.error_flag);
+            }
+        }
+        __syncthreads();
+
+        // ---- 2-4. per period: pad, prefix, sweep, reduce, write ----------------
+        const size_t hist_bytes = (size_t)pt * pbytes;               // multiple of 16
+        float2* scr = reinterpret_cast<float2*>(smem + hist_bytes);
+        const CurveDesc& cv = s.curve;
+        const int obj = a.obj_flag;
+        const int e_r = cv.e_r, e_i = cv.e_i;
+
+        for (int q = 0; q < pt; ++q) {
+            const int nb = s.nb[q];
+            const int L = nb + 1;
+            unsigned char* hq = smem + (size_t)q * pbytes;
+            uint32_t* A = reinterpret_cast<uint32_t*>(hq);        // UNIFORM words
+            int32_t* B = reinterpret_cast<int32_t*>(A + hlp);
+            uint32_t* C = A + 2 * hlp;
+            double* R = reinterpret_cast<double*>(hq);            // GENERAL sums
+            double* W = R + hlp;
+
+            if (tid == 0) {                     // wrap pad, sequential like the reference
+                const int o = s.seg.oversample;
+                for (int k = 0; k < o; ++k) {
+                    const int dst = nb - o + k;
+                    if (dst >= 0 && dst < s.seg.width && dst < hl && 1 + k < hl) {
+                        if (MODE == MODE_UNIFORM) {
+                            A[dst] = A[1 + k];
+                            B[dst] = B[1 + k];
+                            C[dst] = C[1 + k];
+                        } else {
+                            R[dst] = R[1 + k];
+                            W[dst] = W[1 + k];
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+
+            // prefix scan, pass 1: per-warp totals of each contiguous range
+            const int E = ((L + kWarps * 32 - 1) / (kWarps * 32)) * 32;
+            const int lo_i = warp * E;
+            const int hi_i = min(L, lo_i + E);
+            {
+                uint32_t ta = 0u, tc = 0u;
+                int32_t tb = 0;
+                double tr = 0.0, tw = 0.0;
+                for (int i = lo_i + lane; i < hi_i; i += 32) {
+                    if (MODE == MODE_UNIFORM) {
+                        ta += A[i];
+                        tb += B[i];
+                        tc += C[i];
+                    } else {
+                        tr += R[i];
+                        tw += W[i];
+                    }
+                }
+                if (MODE == MODE_UNIFORM) {
+                    ta = warp_sum(ta);
+                    tb = warp_sum(tb);
+                    tc = warp_sum(tc);
+                } else {
+                    tr = warp_sum(tr);
+                    tw = warp_sum(tw);
+                }
+                if (lane == 0) {
+                    s.tot_a[warp] = ta;
+                    s.tot_b[warp] = tb;
+                    s.tot_c[warp] = tc;
+                    s.tot_rd[warp] = tr;
+                    s.tot_wd[warp] = tw;
+                }
+            }
+            __syncthreads();
+            // pass 2: inclusive scan inside each range, prefix written in place,
+            // FP32 screen copy {t prefix, weight prefix}
+            float tmax = 0.0f;
+            {
+                uint32_t oa = 0u, oc = 0u;
+                int32_t ob = 0;
+                double orr = 0.0, ow = 0.0;
+                for (int w = 0; w < warp; ++w) {
+                    oa += s.tot_a[w];
+                    ob += s.tot_b[w];
+                    oc += s.tot_c[w];
+                    orr += s.tot_rd[w];
+                    ow += s.tot_wd[w];
+                }
+                for (int g = lo_i; g < hi_i; g += 32) {
+                    const int i = g + lane;
+                    const bool in = i < hi_i;
+                    float tf, wf;
+                    if (MODE == MODE_UNIFORM) {
+                        uint32_t va = in ? A[i] : 0u, vc = in ? C[i] : 0u;
+                        int32_t vb = in ? B[i] : 0;
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const uint32_t xa = __shfl_up_sync(kFull, va, o);
+                            const int32_t xb = __shfl_up_sync(kFull, vb, o);
+                            const uint32_t xc = __shfl_up_sync(kFull, vc, o);
+                            if (lane >= o) {
+                                va += xa;
+                                vb += xb;
+                                vc += xc;
+                            }
+                        }
+                        const uint32_t pa = oa + va, pc = oc + vc;
+                        const int32_t pb = ob + vb;
+                        if (in) {
+                            A[i] = pa;
+                            B[i] = pb;
+                            C[i] = pc;
+                        }
+                        tf = (float)((long long)pb * (1ll << kHalfBits) + (long long)pa);
+                        wf = (float)pc;
+                        oa += __shfl_sync(kFull, va, 31);
+                        ob += __shfl_sync(kFull, vb, 31);
+                        oc += __shfl_sync(kFull, vc, 31);
+                    } else {
+                        double vr = in ? R[i] : 0.0, vw = in ? W[i] : 0.0;
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const double xr = __shfl_up_sync(kFull, vr, o);
+                            const double xw = __shfl_up_sync(kFull, vw, o);
+                            if (lane >= o) {
+                                vr += xr;
+                                vw += xw;
+                            }
+                        }
+                        const double cr = orr + vr, cw = ow + vw;
+                        if (in) {
+                            R[i] = cr;
+                            W[i] = cw;
+                        }
+                        tf = (float)cr;
+                        wf = (float)cw;
+                        orr += __shfl_sync(kFull, vr, 31);
+                        ow += __shfl_sync(kFull, vw, 31);
+                    }
+                    if (in) {
+                        scr[i] = make_float2(tf, wf);
+                        tmax = fmaxf(tmax, fabsf(tf));
+                    }
+                }
+                tmax = warp_max(tmax);
+                if (lane == 0) s.red_t[warp] = tmax;
+            }
+            __syncthreads();
+            tmax = 0.0f;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) tmax = fmaxf(tmax, s.red_t[w]);
+
+            // weight prefix and flux*weight prefix at bin i, in the reference's units
+            auto iv_prefix = [&](int i) -> double {
+                return MODE == MODE_UNIFORM ? (double)C[i] * cv.w_uniform : ldexp(W[i], -e_i);
+            };
+            // exact sums of box (n, d) in the reference's units
+            auto box_sums = [&](int n, int d) -> BoxSums {
+                BoxSums b;
+                if (MODE == MODE_UNIFORM) {
+                    b.iv_in = (double)(C[n + d] - C[n]) * cv.w_uniform;
+                    b.y_in = ldexp((double)(prefix_r(A, B, n + d) - prefix_r(A, B, n)), -e_r) +
+                             cv.ybar * b.iv_in;
+                } else {
+                    b.iv_in = ldexp(W[n + d] - W[n], -e_i);
+                    b.y_in = ldexp(R[n + d] - R[n], -e_r) + cv.ybar * b.iv_in;
+                }
+                return b;
+            };
+            auto exact = [&](int n, int d) -> double {
+                return box_objective(box_sums(n, d), cv, obj);
+            };
+
+            if (a.debug_prefix != nullptr && q == 0) {   // test hook: this period's prefixes
+                for (int i = tid; i < L; i += kThreads) {
+                    const double r_i = MODE == MODE_UNIFORM ? ldexp((double)prefix_r(A, B, i), -e_r)
+                                                            : ldexp(R[i], -e_r);
+                    a.debug_prefix[i] = r_i + cv.ybar * iv_prefix(i);
+                    a.debug_prefix[hl + i] = iv_prefix(i);
+                }
+            }
+
+            // ---- sweep: durations outer, starts inner (the reference's order) ----
+            const float Et = cv.exact_all ? CUDART_INF_F : tmax * (1.0f / 2097152.0f);  // 2^-21
+            const float Wt = MODE == MODE_UNIFORM ? (float)cv.n_points : (float)cv.i_total;
+            const float Ei = MODE == MODE_UNIFORM ? 0.0f : Wt * (1.0f / 2097152.0f);
+            const float floor_q =
+                MODE == MODE_GENERAL ? (float)ldexp(cv.ivar_floor, e_i) * (1.0f + 1e-3f) : 0.0f;
+
+            bool has = false, ex_ok = false;
+            int bn = 0, bdi = 0;
+            float lb = -1.0f, hb = -1.0f;
+            double ex_v = -CUDART_INF;
+            float thr = -1.0f;
+
+            for (int di = 0; di < n_dur; ++di) {
+                const int d = s.dur[di];
+                if (d >= nb) continue;
+                const int nmax = nb - d;
+                for (int n0 = warp * 32; n0 <= nmax; n0 += kThreads) {
+                    const int n = n0 + lane;
+                    bool upd = false;
+                    if (n <= nmax) {
+                        const float2 av = scr[n];
+                        const float2 bv = scr[n + d];
+                        const float t = bv.x - av.x;
+                        const float iv = bv.y - av.y;       // count, or scaled weight
+                        const float ov = Wt - iv;
+                        float den_lo, den_hi;
+                        bool ok, sure_valid;
+                        if (MODE == MODE_UNIFORM) {
+                            den_lo = iv * ov;                // exact counts: > 0 iff valid
+                            if (obj) den_lo *= ov;
+                            den_hi = den_lo;
+                            sure_valid = true;
+                            ok = den_lo > 0.0f;
+                        } else {
+                            const float il = fmaxf(iv - Ei, 0.0f), ol = fmaxf(ov - Ei, 0.0f);
+                            const float ih = iv + Ei, oh = ov + Ei;
+                            den_lo = obj ? il * ol * ol : il * ol;
+                            den_hi = obj ? ih * oh * oh : ih * oh;
+                            sure_valid = (il >= floor_q) & (ol >= floor_q);
+                            // an empty box is exactly 0 in the FP64 prefix
+                            ok = (den_lo > 0.0f) || (W[n + d] != W[n]);
+                        }
+                        const float th = fabsf(t) + Et;
+                        if (ok && t <= Et && !(th * th < thr * den_lo)) {
+                            // ---- rare path: a box that may compete ----
+                            const float tl = fmaxf(fabsf(t) - Et, 0.0f);
+                            const float khi = den_lo > 0.0f
+                                                  ? __fdividef(th * th, den_lo) * (1.0f + kRel)
+                                                  : CUDART_INF_F;
+                            const float klo = __fdividef(tl * tl, den_hi) * (1.0f - kRel);
+                            const bool sure = (t < -Et) & sure_valid & (klo > 0.0f);
+                            if (!has) {
+                                if (sure) {
+                                    has = true; ex_ok = false; bn = n; bdi = di; lb = klo; hb = khi;
+                                    upd = true;
+                                } else {
+                                    const double v = exact(n, d);
+                                    if (v > -CUDART_INF) {
+                                        has = true; ex_ok = true; ex_v = v; bn = n; bdi = di;
+                                        lb = klo; hb = khi; upd = true;
+                                    }
+                                }
+                            } else if (sure && klo > hb) {
+                                ex_ok = false; bn = n; bdi = di; lb = klo; hb = khi; upd = true;
+                            } else if (khi >= lb) {
+                                if (!ex_ok) { ex_v = exact(bn, s.dur[bdi]); ex_ok = true; }
+                                const double v = exact(n, d);
+                                if (v > -CUDART_INF && better(v, di, n, ex_v, bdi, bn)) {
+                                    ex_v = v; bn = n; bdi = di; lb = fmaxf(klo, lb); hb = khi;
+                                    upd = true;
+                                }
+                            }
+                        }
+                    }
+                    if (__any_sync(kFull, upd))
+                        thr = warp_max(has ? lb * (1.0f - 2.0f * kRel) : -1.0f);
+                }
+            }
+
+            // ---- reduce: candidates that may hold the period's maximum ----------
+            float L_lo = warp_max(has ? lb : -1.0f);
+            if (lane == 0) s.red_f[warp] = L_lo;
+            __syncthreads();
+            L_lo = -1.0f;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) L_lo = fmaxf(L_lo, s.red_f[w]);
+            double v = -CUDART_INF;
+            int vdi = 1 << 30, vn = 1 << 30;
+            if (has && hb >= L_lo) {
+                if (!ex_ok) { ex_v = exact(bn, s.dur[bdi]); ex_ok = true; }
+                v = ex_v; vdi = bdi; vn = bn;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(kFull, v, o);
+                const int odi = __shfl_xor_sync(kFull, vdi, o);
+                const int on = __shfl_xor_sync(kFull, vn, o);
+                if (better(ov, odi, on, v, vdi, vn)) { v = ov; vdi = odi; vn = on; }
+            }
+            if (lane == 0) { s.red_v[warp] = v; s.red_di[warp] = vdi; s.red_n[warp] = vn; }
+            __syncthreads();
+            if (tid == 0) {
+                for (int w = 1; w < kWarps; ++w)
+                    if (better(s.red_v[w], s.red_di[w], s.red_n[w], v, vdi, vn)) {
+                        v = s.red_v[w]; vdi = s.red_di[w]; vn = s.red_n[w];
+                    }
+                double* o = out + q;
+                if (!(v > -CUDART_INF)) {
+                    o[0] = -CUDART_INF;
+                    for (int f = 1; f < kFields; ++f) o[f * ostride] = 0.0;
+                } else {
+                    const int d = s.dur[vdi];
+                    const BoxSums b = box_sums(vn, d);
+                    const double iv_out = cv.sum_ivar - b.iv_in;
+                    const double yin = b.y_in / b.iv_in;
+                    const double yout = (cv.sum_y - b.y_in) / iv_out;
+                    const double depth = yout - yin;
+                    const double derr = sqrt(1.0 / b.iv_in + 1.0 / iv_out);
+                    const double dsnr = depth / derr;
+                    const double ll = 0.5 * b.iv_in * depth * depth;
+                    const double bin = s.seg.bin_duration;
+                    const double dur = (double)d * bin;
+                    o[0] = obj == 0 ? dsnr : ll;
+                    o[1 * ostride] = depth;
+                    o[2 * ostride] = derr;
+                    o[3 * ostride] = dsnr;
+                    o[4 * ostride] = dur;
+                    o[5 * ostride] = fmod((double)vn * bin + 0.5 * dur, s.per[q]) + cv.t_min;
+                    o[6 * ostride] = ll;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Phase bins of every point at one period through the fast path with its
+// fallback (the tests compare them with the reference's fold bit for bit).
+__global__ void fold_bins_kernel(const double* tau, int n, double P, double f, uint32_t S,
+                                 double bin, int width, int fb, uint32_t mu, uint32_t mphi,
+                                 int fast, int32_t* out, int32_t* used_fast) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t fmask = (1u << fb) - 1u;
+    int ind = fast ? fold_fast(tau[j], f, S, fb, fmask, mu, (1u << fb) - 2u * mu, mphi,
+                               0u - 2u * mphi)
+                   : -1;
+    used_fast[j] = ind >= 0;
+    if (ind < 0) ind = fold_exact(tau[j], P, bin, width);
+    out[j] = ind;
+}
+
+// Per curve: the largest power (non-finite values count as 0, as the
+// reference's assembly does before its SDE and peak search) with its first
+// index, and the mean and population standard deviation of that power.
+__global__ void best_kernel(const double* power, int64_t n_periods, int64_t* best_index,
+                            double* best_power, double* mean_out, double* std_out) {
+    __shared__ double red_s[kWarps];
+    __shared__ double red_v[kWarps];
+    __shared__ long long red_i[kWarps];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double* p = power + (int64_t)blockIdx.x * n_periods;
+    double sum = 0.0, bv = -CUDART_INF;
+    long long bi = -1;
+    for (int64_t i = tid; i < n_periods; i += kThreads) {
+        const double v = p[i];
+        const double z = isfinite(v) ? v : 0.0;
+        sum += z;
+        if (z > bv || (z == bv && i < bi)) { bv = z; bi = i; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_xor_sync(kFull, sum, o);
+        const double ov = __shfl_xor_sync(kFull, bv, o);
+        const long long oi = __shfl_xor_sync(kFull, bi, o);
+        if (ov > bv || (ov == bv && oi >= 0 && (bi < 0 || oi < bi))) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) { red_s[warp] = sum; red_v[warp] = bv; red_i[warp] = bi; }
+    __syncthreads();
+    sum = 0.0;
+    bv = -CUDART_INF;
+    bi = -1;
+    for (int w = 0; w < kWarps; ++w) {
+        sum += red_s[w];
+        if (red_v[w] > bv || (red_v[w] == bv && red_i[w] >= 0 && (bi < 0 || red_i[w] < bi))) {
+            bv = red_v[w];
+            bi = red_i[w];
+        }
+    }
+    const double mean = n_periods > 0 ? sum / (double)n_periods : 0.0;
+    __syncthreads();
+    double ss = 0.0;
+    for (int64_t i = tid; i < n_periods; i += kThreads) {
+        const double v = p[i];
+        const double z = (isfinite(v) ? v : 0.0) - mean;
+        ss += z * z;
+    }
+    ss = warp_sum(ss);
+    if (lane == 0) red_s[warp] = ss;
+    __syncthreads();
+    if (tid == 0) {
+        ss = 0.0;
+        for (int w = 0; w < kWarps; ++w) ss += red_s[w];
+        best_index[blockIdx.x] = bi;
+        best_power[blockIdx.x] = bv;
+        mean_out[blockIdx.x] = mean;
+        std_out[blockIdx.x] = n_periods > 0 ? sqrt(ss / (double)n_periods) : 0.0;
+    }
+}
+
+}  // namespace
+
+cudaError_t configure_search(size_t smem) {
+    cudaError_t e = cudaFuncSetAttribute(bls_search_kernel<MODE_UNIFORM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(bls_search_kernel<MODE_GENERAL>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t launch_search(const BatchArgs& args, int mode, int n_ctas, size_t smem,
+                          cudaStream_t stream) {
+    if (mode == MODE_UNIFORM)
+        bls_search_kernel<MODE_UNIFORM><<<n_ctas, kThreads, smem, stream>>>(args);
+    else
+        bls_search_kernel<MODE_GENERAL><<<n_ctas, kThreads, smem, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_best(const double* power, int n_curves, int64_t n_periods, int64_t* best_index,
+                        double* best_power, double* mean, double* sd, cudaStream_t stream) {
+    if (n_curves <= 0) return cudaSuccess;
+    best_kernel<<<n_curves, kThreads, 0, stream>>>(power, n_periods, best_index, best_power, mean,
+                                                   sd);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_bins(const double* tau, int n, double P, double f, uint32_t S, double bin,
+                             int width, int fb, uint32_t mu, uint32_t mphi, int fast,
+                             int32_t* out, int32_t* used_fast, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    fold_bins_kernel<<<(n + 255) / 256, 256, 0, stream>>>(tau, n, P, f, S, bin, width, fb, mu,
+                                                          mphi, fast, out, used_fast);
+    return cudaGetLastError();
+}
+
+int search_threads() { return kThreads; }
+
+size_t period_hist_bytes(int mode, int hl) {
+    return mode == MODE_UNIFORM ? hist_period_bytes<MODE_UNIFORM>(hl)
+                                : hist_period_bytes<MODE_GENERAL>(hl);
+}
+
+int max_resident_ctas(int mode, size_t smem) {
+    int blocks = 0;
+    if (mode == MODE_UNIFORM)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, bls_search_kernel<MODE_UNIFORM>,
+                                                      kThreads, smem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, bls_search_kernel<MODE_GENERAL>,
+                                                      kThreads, smem);
+    return blocks;
+}
+
+}  // namespace blsb200

@@ -1,0 +1,162 @@
+/*
+ * C ABI of the B200 box-least-squares (BLS) engine: libbls_b200.so.
+ *
+ * Plain pointers and sizes only.  Host arrays in, host (or device) arrays out;
+ * the engine owns its device buffers, pinned staging, CUDA stream and graphs.
+ * Every function returns 0 on success or a BLS_E_* code; bls_last_error()
+ * describes the last failure of the calling thread.
+ *
+ * The entry points replace, in cuPeriod 1.3.0:
+ *   bls_engine_create / bls_engine_destroy
+ *       -- the per-worker engine hook PeriodogramMethod.make_engine
+ *          (src/cuperiod/methods/base.py:388-396), built once per batch worker
+ *          (src/cuperiod/batch/runner.py:253-277);
+ *   bls_search
+ *       -- _bls_search_cuda_specs (src/cuperiod/methods/_bls_core.py:741-840):
+ *          one upload, one launch per segment, one download.  With one curve it
+ *          is bls_power_segments (1075-1130) / bls_power (882-1028); with many
+ *          curves it is the batch runner's per-curve loop
+ *          (src/cuperiod/batch/runner.py:214-250) done in one launch;
+ *   bls_prepare / bls_launch / bls_download
+ *       -- the three phases of _bls_search_cuda_specs taken apart: the uploads
+ *          of _cuda_curve (709-738), the kernel launches (796-825) and the
+ *          stacked (7, P) download (828);
+ *   bls_download_best
+ *       -- the per-curve reduction of the spectrum that Periodogram.best_period
+ *          and the batch row need (src/cuperiod/core/result.py:369-438,
+ *          src/cuperiod/methods/bls.py:274-301 for the SDE);
+ *   bls_debug_fold_bins / bls_debug_prefix
+ *       -- the phase-bin lines of the fold (_bls_core.py:369-376 / 536-538) and
+ *          the padded cumulative sums (377-388), exported so tests can compare
+ *          the device's intermediate results with the reference's;
+ *   bls_last_error
+ *       -- the exceptions the reference raises before a launch (ValueError,
+ *          BackendUnavailableError from core/backend.py:340-384).
+ */
+#ifndef BLS_B200_H
+#define BLS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    BLS_OK = 0,
+    BLS_E_INVALID = 1,      /* bad argument or input data (the reference's ValueError) */
+    BLS_E_CUDA = 2,         /* CUDA runtime failure */
+    BLS_E_RESOURCE = 3,     /* a segment too wide for shared memory (BackendUnavailableError) */
+    BLS_E_NOMEM = 4,        /* device or pinned host allocation failed */
+    BLS_E_DEVICE = 5,       /* a kernel reported an impossible work descriptor */
+    BLS_E_STATE = 6         /* call out of order (e.g. launch before prepare) */
+};
+
+/* Output fields, in the reference's order (_OUTPUT_NAMES, _bls_core.py:675-684). */
+enum {
+    BLS_F_POWER = 0, BLS_F_DEPTH, BLS_F_DEPTH_ERR, BLS_F_DEPTH_SNR,
+    BLS_F_DURATION, BLS_F_TRANSIT_TIME, BLS_F_LOG_LIKELIHOOD, BLS_N_FIELDS
+};
+
+typedef struct BlsEngine BlsEngine;
+
+typedef struct {
+    int32_t device;          /* CUDA device ordinal; -1 = the current device */
+    int32_t smem_per_cta;    /* dynamic shared memory per CTA in bytes; 0 = automatic */
+    int32_t max_tile;        /* periods per work item, 1..16; 0 = as many as fit */
+    int32_t use_graph;       /* 1: replay bls_launch from a captured CUDA graph */
+    int32_t exact_sweep;     /* 1: evaluate every box in FP64, no FP32 screen (the
+                                reference's screen=False, _bls_core.py:468-500) */
+} BlsTune;
+
+/* One trial-period grid, split into duration-homogeneous segments (each is one
+ * _SearchSpec of the reference, _bls_core.py:687-706).  All host pointers. */
+typedef struct {
+    int32_t n_segments;
+    const int64_t* seg_offsets;   /* n_segments+1 offsets into periods */
+    const double* periods;        /* every segment's periods, concatenated */
+    const int64_t* dur_offsets;   /* n_segments+1 offsets into durations */
+    const double* durations;      /* every segment's box durations, concatenated */
+    int32_t oversample;           /* phase bins per shortest duration */
+    int32_t objective;            /* 0 = depth SNR, 1 = log-likelihood */
+} BlsGrid;
+
+/* A batch of light curves, concatenated.  All host pointers.  Times, fluxes and
+ * errors must be finite, errors > 0; dy may be NULL (unit errors). */
+typedef struct {
+    int32_t n_curves;
+    const int64_t* offsets;       /* n_curves+1 offsets into t / y / dy */
+    const double* t;
+    const double* y;              /* flux, transits as dips */
+    const double* dy;             /* 1-sigma errors, or NULL */
+} BlsCurves;
+
+/* What one prepared batch holds (sizes and the algorithmic work of one launch). */
+typedef struct {
+    int32_t n_curves;
+    int32_t n_segments;
+    int64_t n_periods;            /* periods per curve */
+    int64_t n_items;              /* work items of one launch */
+    int64_t n_points;             /* points over all curves */
+    double folds;                 /* point-period folds per launch */
+    double boxes;                 /* (duration, start) boxes per launch */
+    double trials;                /* (period, duration) trials per launch */
+    int64_t h2d_bytes;            /* bytes uploaded by bls_prepare */
+    int32_t ctas;                 /* persistent CTAs per launch */
+    int32_t smem_per_cta;
+    int32_t uniform_curves;       /* curves on the one-weight fast path */
+    int32_t fast_fold_segments;   /* segments whose fold runs the fast path */
+} BlsBatchInfo;
+
+int bls_engine_create(const BlsTune* tune, BlsEngine** engine);
+int bls_engine_destroy(BlsEngine* engine);
+const char* bls_last_error(void);
+
+/* Pack and upload a batch (host preparation runs on all host cores).  `stream`
+ * is a cudaStream_t; NULL selects the engine's own stream. */
+int bls_prepare(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* curves, void* stream);
+
+/* Run the search of the prepared batch on the device (no host transfers). */
+int bls_launch(BlsEngine* engine, void* stream);
+
+/* Copy every field of every curve, field-major: out[f][c][p] with
+ * f < BLS_N_FIELDS, c < n_curves, p < n_periods (grid order).  Waits for the
+ * stream. */
+int bls_download(BlsEngine* engine, double* out, void* stream);
+
+/* Device address of the output fields (layout as bls_download), valid until the
+ * next bls_prepare. */
+int bls_device_output(BlsEngine* engine, const double** out);
+
+/* Per curve: index (grid order) and value of the largest finite power, and the
+ * mean and standard deviation of the power with non-finite values as 0 (the
+ * reference's SDE normalisation, methods/bls.py:274-301).  Waits for the stream. */
+int bls_download_best(BlsEngine* engine, int64_t* best_index, double* best_power,
+                      double* power_mean, double* power_std, void* stream);
+
+/* prepare + launch + download in one call. */
+int bls_search(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* curves, double* out,
+               void* stream);
+
+int bls_batch_info(BlsEngine* engine, BlsBatchInfo* info);
+
+/* Phase bin of every point of one curve (times t, n points; t_min removed as the
+ * reference does) at one period of a segment whose shortest duration and
+ * oversample give the bin width, as the search kernel computes it.  used_fast[j]
+ * is 1 where the fast fold decided the bin.  Host arrays. */
+int bls_debug_fold_bins(BlsEngine* engine, const double* t, int64_t n, double period,
+                        double bin_duration, int32_t width, int32_t* bins, int32_t* used_fast);
+
+/* Prefix sums of y*ivar and ivar over the phase bins 0..n_bins of one period,
+ * after the wrap pad, as the search kernel holds them (the cumulative sums of
+ * _bls_core.py:377-388), for one curve (dy may be NULL).  yw_prefix and
+ * ivar_prefix need room for n_bins + 1 values; *n_bins receives n_bins. */
+int bls_debug_prefix(BlsEngine* engine, const double* t, const double* y, const double* dy,
+                     int64_t n, double period, const double* durations, int32_t n_durations,
+                     int32_t oversample, double* yw_prefix, double* ivar_prefix, int32_t* n_bins);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BLS_B200_H */

@@ -1,0 +1,199 @@
+/*
+ * TEST INFRASTRUCTURE ONLY -- the CPU oracle of the BLS parity tests.
+ *
+ * A plain-C restatement of cuPeriod's numba box-least-squares kernel
+ * (src/cuperiod/methods/_bls_core.py:341-462) in its exact, unscreened form
+ * (_bls_search_numba(..., screen=False), _bls_core.py:468-500).  Every
+ * operation keeps the reference's order and IEEE rounding: the translation unit
+ * is built with -ffp-contract=off (no fused multiply-add) and without fast-math,
+ * like numba's fastmath=False, so the phase fold, the bin sums, the cumulative
+ * sums and the box objective round exactly as the reference's do.
+ *
+ * Only the tests, the smoke check and the benchmark's CPU-baseline leg load
+ * this library, and only as the checker or the timed CPU baseline.  The
+ * product path (cuperiod_b200) never calls it.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+#include <stdatomic.h>
+
+/* Output fields, field-major (7 x n_periods), in the reference's order
+ * (_OUTPUT_NAMES, _bls_core.py:675-684). */
+enum { O_POWER, O_DEPTH, O_DEPTH_ERR, O_DEPTH_SNR, O_DURATION, O_TT, O_LL, O_NFIELDS };
+
+/* Phase bin of one point, as the numba kernel computes it
+ * (_bls_core.py:369-376): w = x - P*floor(x/P); ind = int(w/bin) + 1, clipped. */
+static inline int64_t fold_bin(double x, double period, double bin_duration, int64_t width)
+{
+    double w = x - period * floor(x / period);
+    int64_t ind = (int64_t)(w / bin_duration) + 1;
+    if (ind < 0) ind = 0;
+    else if (ind > width - 1) ind = width - 1;
+    return ind;
+}
+
+/* Per-period bin count, _bls_core.py:358-360. */
+static inline int64_t period_bins(double period, double bin_duration, int64_t oversample,
+                                  int64_t width)
+{
+    int64_t n_bins = (int64_t)ceil(period / bin_duration) + oversample;
+    if (n_bins > width - 1) n_bins = width - 1;
+    return n_bins;
+}
+
+/* The phase bins of every point at one period (debug view used by the tests to
+ * check the device's bit-exact bin assignment). */
+int bls_oracle_fold_bins(const double* tau, int64_t n_points, double period,
+                         double bin_duration, int64_t width, int32_t* out)
+{
+    for (int64_t j = 0; j < n_points; ++j)
+        out[j] = (int32_t)fold_bin(tau[j], period, bin_duration, width);
+    return 0;
+}
+
+/* Arguments shared by the worker threads of one search. */
+typedef struct {
+    const double *tau, *yw, *wv, *periods;
+    const int64_t* dur_bins;
+    int64_t n_points, n_periods, n_dur, oversample, width;
+    double bin_duration, sum_y, sum_ivar, t_min, ivar_floor;
+    int obj_flag;
+    double* out;
+    atomic_long next;       /* next unclaimed period block */
+    atomic_int failed;
+} search_args;
+
+#define PERIOD_BLOCK 16
+
+/* One trial period: _bls_core.py:357-460 with screen=False. */
+static void search_period(const search_args* a, int64_t pidx, double* my, double* mi)
+{
+    const int64_t n_periods = a->n_periods, width = a->width, oversample = a->oversample;
+    const double bin_duration = a->bin_duration, sum_y = a->sum_y, sum_ivar = a->sum_ivar;
+    const double ivar_floor = a->ivar_floor;
+    double* o_power = a->out + (size_t)O_POWER * n_periods;
+    double* o_depth = a->out + (size_t)O_DEPTH * n_periods;
+    double* o_derr = a->out + (size_t)O_DEPTH_ERR * n_periods;
+    double* o_dsnr = a->out + (size_t)O_DEPTH_SNR * n_periods;
+    double* o_dur = a->out + (size_t)O_DURATION * n_periods;
+    double* o_tt = a->out + (size_t)O_TT * n_periods;
+    double* o_ll = a->out + (size_t)O_LL * n_periods;
+
+    const double period = a->periods[pidx];
+    const int64_t n_bins = period_bins(period, bin_duration, oversample, width);
+    for (int64_t i = 0; i <= n_bins; ++i) { my[i] = 0.0; mi[i] = 0.0; }
+    for (int64_t j = 0; j < a->n_points; ++j) {          /* fold, 365-376 */
+        const int64_t ind = fold_bin(a->tau[j], period, bin_duration, width);
+        my[ind] += a->yw[j];
+        mi[ind] += a->wv[j];
+    }
+    for (int64_t k = 0; k < oversample; ++k) {           /* wrap pad, 377-381 */
+        const int64_t dst = n_bins - oversample + k;
+        if (0 <= dst && dst < width) { my[dst] = my[1 + k]; mi[dst] = mi[1 + k]; }
+    }
+    double ay = 0.0, ai = 0.0;                            /* cumulative sums, 382-388 */
+    for (int64_t i = 0; i <= n_bins; ++i) {
+        ay += my[i]; my[i] = ay;
+        ai += mi[i]; mi[i] = ai;
+    }
+    double loc = -INFINITY;
+    int64_t ln = 0, ld = 0;
+    for (int64_t di = 0; di < a->n_dur; ++di) {           /* exact sweep, 395-440 */
+        const int64_t d = a->dur_bins[di];
+        if (d < 1 || d >= n_bins) continue;
+        const int64_t m = n_bins - d + 1;
+        for (int64_t n = 0; n < m; ++n) {
+            const double y_in = my[n + d] - my[n];
+            const double iv_in = mi[n + d] - mi[n];
+            const double iv_out = sum_ivar - iv_in;
+            if (iv_in < ivar_floor || iv_out < ivar_floor) continue;
+            const double yin = y_in / iv_in;
+            const double yout = (sum_y - y_in) / iv_out;
+            if (yout < yin) continue;
+            const double depth = yout - yin;
+            double obj;
+            if (a->obj_flag == 0) obj = depth / sqrt(1.0 / iv_in + 1.0 / iv_out);
+            else obj = 0.5 * iv_in * depth * depth;
+            if (obj > loc) { loc = obj; ln = n; ld = d; }
+        }
+    }
+    if (!(loc > -INFINITY)) {                             /* no admissible box, 441-442 */
+        o_power[pidx] = -INFINITY;
+        o_depth[pidx] = 0.0; o_derr[pidx] = 0.0; o_dsnr[pidx] = 0.0;
+        o_dur[pidx] = 0.0; o_tt[pidx] = 0.0; o_ll[pidx] = 0.0;
+        return;
+    }
+    const double y_in = my[ln + ld] - my[ln];             /* epilogue, 443-460 */
+    const double iv_in = mi[ln + ld] - mi[ln];
+    const double iv_out = sum_ivar - iv_in;
+    const double yin = y_in / iv_in;
+    const double yout = (sum_y - y_in) / iv_out;
+    const double depth = yout - yin;
+    const double derr = sqrt(1.0 / iv_in + 1.0 / iv_out);
+    const double dsnr = depth / derr;
+    const double ll = 0.5 * iv_in * depth * depth;
+    const double dur = (double)ld * bin_duration;
+    o_power[pidx] = a->obj_flag == 0 ? dsnr : ll;
+    o_depth[pidx] = depth;
+    o_derr[pidx] = derr;
+    o_dsnr[pidx] = dsnr;
+    o_dur[pidx] = dur;
+    o_tt[pidx] = fmod((double)ln * bin_duration + 0.5 * dur, period) + a->t_min;
+    o_ll[pidx] = ll;
+}
+
+static void* search_worker(void* arg)
+{
+    search_args* a = (search_args*)arg;
+    double* my = (double*)malloc(sizeof(double) * (size_t)a->width);
+    double* mi = (double*)malloc(sizeof(double) * (size_t)a->width);
+    if (!my || !mi) {
+        atomic_store(&a->failed, 1);
+    } else {
+        for (;;) {
+            const int64_t p0 = atomic_fetch_add(&a->next, PERIOD_BLOCK);
+            if (p0 >= a->n_periods) break;
+            const int64_t p1 = p0 + PERIOD_BLOCK < a->n_periods ? p0 + PERIOD_BLOCK : a->n_periods;
+            for (int64_t p = p0; p < p1; ++p) search_period(a, p, my, mi);
+        }
+    }
+    free(my);
+    free(mi);
+    return NULL;
+}
+
+/* The box search over every period (the numba kernel's prange loop, 356). The
+ * periods are independent, so n_threads workers share them; the result does
+ * not depend on the thread count. */
+int bls_oracle_search(const double* tau, const double* yw, const double* wv, int64_t n_points,
+                      const double* periods, int64_t n_periods,
+                      const int64_t* dur_bins, int64_t n_dur,
+                      double bin_duration, int64_t oversample, int64_t width,
+                      double sum_y, double sum_ivar, double t_min, int obj_flag,
+                      double ivar_floor, double* out, int n_threads)
+{
+    if (width < 2 || n_periods < 0 || n_points < 0) return 1;
+    search_args a = {
+        .tau = tau, .yw = yw, .wv = wv, .periods = periods, .dur_bins = dur_bins,
+        .n_points = n_points, .n_periods = n_periods, .n_dur = n_dur,
+        .oversample = oversample, .width = width, .bin_duration = bin_duration,
+        .sum_y = sum_y, .sum_ivar = sum_ivar, .t_min = t_min, .ivar_floor = ivar_floor,
+        .obj_flag = obj_flag, .out = out,
+    };
+    atomic_init(&a.next, 0);
+    atomic_init(&a.failed, 0);
+    if (n_threads < 1) n_threads = 1;
+    if (n_threads > 512) n_threads = 512;
+    pthread_t th[512];
+    int started = 0;
+    for (int i = 1; i < n_threads; ++i) {
+        if (pthread_create(&th[started], NULL, search_worker, &a) != 0) break;
+        ++started;
+    }
+    search_worker(&a);
+    for (int i = 0; i < started; ++i) pthread_join(th[i], NULL);
+    return atomic_load(&a.failed) ? 2 : 0;
+}

@@ -1,0 +1,328 @@
+"""TEST INFRASTRUCTURE ONLY -- the CPU oracle of the BLS parity tests.
+
+A restatement of cuPeriod's BLS path on the CPU: the host-side steps in numpy
+(each function cites the reference file:line it follows) and the per-period box
+search in plain C (``bls_oracle.c``, the numba kernel of
+``src/cuperiod/methods/_bls_core.py:341-462`` evaluated without its screen).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+may import this module, and only as the checker or the timed CPU baseline.  The
+product package ``cuperiod_b200`` never imports it.
+
+It is pinned against golden vectors produced by the reference's own numba
+backend (``tests/golden/make_golden.py``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle_bls.so")
+_lib: ctypes.CDLL | None = None
+
+F64_EPS = float(np.finfo(np.float64).eps)
+OUTPUT_NAMES = ("power", "depth", "depth_err", "depth_snr", "duration",
+                "transit_time", "log_likelihood")
+SEGMENT_FIELDS = ("period", "power", "depth", "depth_snr", "duration", "transit_time")
+
+
+def build() -> str:
+    """Compile the C oracle with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def _load() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        lib = ctypes.CDLL(_LIB_PATH)
+        d, i64, i32 = ctypes.c_double, ctypes.c_int64, ctypes.c_int
+        p = ctypes.c_void_p
+        lib.bls_oracle_search.argtypes = [p, p, p, i64, p, i64, p, i64, d, i64, i64,
+                                          d, d, d, i32, d, p, i32]
+        lib.bls_oracle_search.restype = i32
+        lib.bls_oracle_fold_bins.argtypes = [p, i64, d, d, i64, p]
+        lib.bls_oracle_fold_bins.restype = i32
+        _lib = lib
+    return _lib
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+# --- kernel-level host steps ---------------------------------------------------
+
+def ivar_floor(n_points: int, sum_ivar: float) -> float:
+    """``_ivar_floor`` (float64 path), ``_bls_core.py:75-94``."""
+    floor = 4.0 * n_points * F64_EPS * sum_ivar
+    if not floor > 0.0:
+        return float(np.finfo(np.float64).tiny)
+    return floor
+
+
+def duration_bins(durations, bin_duration: float) -> list[int]:
+    """``_duration_bins``, ``_bls_core.py:134-149``: round half away, dedupe in order."""
+    seen: set[int] = set()
+    out: list[int] = []
+    for d in np.asarray(durations, dtype=np.float64).tolist():
+        kd = math.floor(d / bin_duration + 0.5)
+        if kd >= 1 and kd not in seen:
+            seen.add(kd)
+            out.append(kd)
+    return out
+
+
+@dataclass
+class Spec:
+    periods: np.ndarray
+    bin_duration: float
+    dur_bins: list[int]
+    width: int
+
+
+def search_spec(periods, durations, oversample: int) -> Spec:
+    """``_search_spec``, ``_bls_core.py:697-706``."""
+    p = np.ascontiguousarray(periods, dtype=np.float64)
+    d = np.ascontiguousarray(durations, dtype=np.float64)
+    bin_duration = float(d.min()) / oversample
+    dur = duration_bins(d, bin_duration)
+    max_n_bins = int(np.ceil(float(p.max()) / bin_duration)) + oversample
+    return Spec(p, bin_duration, dur, max_n_bins + 1)
+
+
+def host_inputs(t, y, dy):
+    """``_host_inputs``, ``_bls_core.py:1043-1058``."""
+    t_host = np.ascontiguousarray(t, dtype=np.float64)
+    y_host = np.ascontiguousarray(y, dtype=np.float64)
+    if y_host.size:
+        y_host = y_host - float(np.median(y_host))
+    ivar_host = 1.0 / (np.ascontiguousarray(dy, dtype=np.float64) ** 2)
+    return t_host, y_host, ivar_host
+
+
+def objective_flag(objective: str) -> int:
+    """``_objective_flag``, ``_bls_core.py:1031-1035``."""
+    if objective not in ("snr", "likelihood"):
+        raise ValueError("objective must be 'snr' or 'likelihood'")
+    return 0 if objective == "snr" else 1
+
+
+def search(t, y, ivar, periods, *, bin_duration, dur_bins, oversample, width,
+           obj_flag, n_threads: int | None = None) -> dict[str, np.ndarray]:
+    """``_bls_search_numba(..., screen=False)``, ``_bls_core.py:468-500``."""
+    lib = _load()
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    ivar = np.ascontiguousarray(ivar, dtype=np.float64)
+    yw = np.ascontiguousarray(np.asarray(y, dtype=np.float64) * ivar, dtype=np.float64)
+    t_min = float(t.min())
+    tau = np.ascontiguousarray(t - t_min, dtype=np.float64)
+    db = np.ascontiguousarray(dur_bins, dtype=np.int64)
+    sum_y = float(yw.sum())
+    sum_ivar = float(ivar.sum())
+    per = np.ascontiguousarray(periods, dtype=np.float64)
+    out = np.empty((7, per.size), dtype=np.float64)
+    if n_threads is None:
+        n_threads = os.cpu_count() or 1
+    rc = lib.bls_oracle_search(
+        _ptr(tau), _ptr(yw), _ptr(ivar), tau.size, _ptr(per), per.size, _ptr(db), db.size,
+        float(bin_duration), int(oversample), int(width), sum_y, sum_ivar, t_min,
+        int(obj_flag), ivar_floor(int(tau.size), sum_ivar), _ptr(out), int(n_threads))
+    if rc != 0:
+        raise RuntimeError(f"oracle search failed ({rc})")
+    return dict(zip(OUTPUT_NAMES, out))
+
+
+def fold_bins(t, period: float, bin_duration: float, width: int) -> np.ndarray:
+    """Phase bin of every point at one period (the numba fold, ``_bls_core.py:365-376``)."""
+    lib = _load()
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    tau = np.ascontiguousarray(t - float(t.min()), dtype=np.float64)
+    out = np.empty(tau.size, dtype=np.int32)
+    lib.bls_oracle_fold_bins(_ptr(tau), tau.size, float(period), float(bin_duration),
+                             int(width), _ptr(out))
+    return out
+
+
+def padded_cumsums(t, y, dy, period: float, durations, oversample: int):
+    """The cumulative sums of y*ivar and ivar over bins 0..n_bins of one period
+    after the wrap pad (``_bls_core.py:357-388``), accumulated in point order."""
+    spec = search_spec([period], durations, oversample)
+    th, yh, ih = host_inputs(t, y, dy)
+    yw = yh * ih
+    bins = fold_bins(th, period, spec.bin_duration, spec.width)
+    nb = min(int(np.ceil(period / spec.bin_duration)) + oversample, spec.width - 1)
+    my = np.zeros(spec.width)
+    mi = np.zeros(spec.width)
+    np.add.at(my, bins, yw)
+    np.add.at(mi, bins, ih)
+    for k in range(oversample):
+        dst = nb - oversample + k
+        if 0 <= dst < spec.width:
+            my[dst] = my[1 + k]
+            mi[dst] = mi[1 + k]
+    return np.cumsum(my[:nb + 1]), np.cumsum(mi[:nb + 1])
+
+
+def bls_power(t, y, dy, periods, durations, oversample: int, *, objective: str = "snr",
+              n_threads: int | None = None) -> dict[str, np.ndarray]:
+    """``bls_power(..., backend="numba")``, ``_bls_core.py:882-1028``."""
+    obj_flag = objective_flag(objective)
+    periods_host = np.ascontiguousarray(periods, dtype=np.float64)
+    if periods_host.size == 0:
+        out = {name: np.empty(0) for name in OUTPUT_NAMES}
+        out["period"] = periods_host
+        return out
+    spec = search_spec(periods_host, durations, oversample)
+    th, yh, ih = host_inputs(t, y, dy)
+    out = search(th, yh, ih, periods_host, bin_duration=spec.bin_duration,
+                 dur_bins=spec.dur_bins, oversample=oversample, width=spec.width,
+                 obj_flag=obj_flag, n_threads=n_threads)
+    out["period"] = periods_host
+    return out
+
+
+# --- grid and segments (methods/bls.py) ------------------------------------------
+
+@dataclass
+class Settings:
+    """The ``BLSSettings`` fields the BLS path reads (``core/config.py:218-302``)."""
+    min_period_days: float = 0.2
+    max_period_days: float = 100.0
+    min_transits: int = 2
+    duration_min_frac: float = 0.01
+    duration_max_frac: float = 0.12
+    n_durations: int = 8
+    min_duration_days: float = 0.01
+    segment_factor: float = 2.0
+    grid_duration_frac: float = 0.05
+    grid_oversample: int = 2
+    bins_per_duration: int = 10
+    objective: str = "snr"
+    min_detections: int = 20
+    extra: dict = field(default_factory=dict)
+
+
+def segment_durations(p_lo: float, s: Settings) -> np.ndarray:
+    """``_segment_durations``, ``bls.py:39-49``."""
+    d_hi = s.duration_max_frac * p_lo
+    d_lo = max(s.duration_min_frac * p_lo, s.min_duration_days)
+    if d_lo >= d_hi:
+        return np.asarray([d_hi], dtype=np.float64)
+    return np.asarray(np.geomspace(d_lo, d_hi, s.n_durations), dtype=np.float64)
+
+
+def segment_periods(baseline: float, s: Settings) -> list[tuple[float, np.ndarray]]:
+    """``_max_period`` + ``_segment_bounds`` + ``_segment_periods``, ``bls.py:52-105``
+    (without the size guard)."""
+    max_period = min(s.max_period_days, baseline / s.min_transits)
+    bounds = []
+    p_lo = s.min_period_days
+    while p_lo < max_period:
+        p_hi = min(p_lo * s.segment_factor, max_period)
+        bounds.append((p_lo, p_hi))
+        p_lo = p_hi
+    if not bounds:
+        return []
+    df = s.grid_duration_frac / (s.grid_oversample * baseline)
+    parts = []
+    for p_lo, p_hi in bounds:
+        freq = np.arange(1.0 / p_hi, 1.0 / p_lo, df)
+        freq = freq[freq < 1.0 / p_lo]
+        if freq.size:
+            parts.append((p_lo, np.asarray(1.0 / freq[::-1], dtype=np.float64)))
+    return parts
+
+
+def default_grid(baseline: float, s: Settings):
+    """``BLSMethod.default_grid``, ``bls.py:327-359``: ``(periods, meta)``."""
+    parts = segment_periods(baseline, s)
+    periods = np.concatenate([p for _, p in parts]) if parts else np.empty(0)
+    meta = {"segmented": True,
+            "segment_starts": tuple(float(p_lo) for p_lo, _ in parts),
+            "segment_sizes": tuple(int(p.size) for _, p in parts)}
+    return periods, meta
+
+
+def log_segments(periods: np.ndarray, s: Settings):
+    """``_log_segments``, ``bls.py:128-152``."""
+    p0 = float(periods.min())
+    with np.errstate(divide="ignore", invalid="ignore"):
+        index = np.floor(np.log(periods / p0) / math.log(s.segment_factor) + 1e-9).astype(np.int64)
+    return [(np.ascontiguousarray(periods[index == k]),
+             segment_durations(p0 * s.segment_factor ** k, s))
+            for k in np.unique(index).tolist()]
+
+
+def grid_segments(periods: np.ndarray, meta: dict | None, s: Settings):
+    """``_grid_segments``, ``bls.py:155-190``."""
+    periods = np.asarray(periods, dtype=np.float64)
+    if periods.size == 0:
+        return []
+    meta = meta or {}
+    starts, sizes = meta.get("segment_starts"), meta.get("segment_sizes")
+    if (starts is not None and sizes is not None and len(starts) == len(sizes)
+            and sum(int(v) for v in sizes) == periods.size):
+        segs, off = [], 0
+        for p_lo, size in zip(starts, sizes):
+            segs.append((periods[off:off + int(size)], segment_durations(float(p_lo), s)))
+            off += int(size)
+        return segs
+    return log_segments(periods, s)
+
+
+def method_power(t, flux, err, periods, meta, s: Settings, n_threads: int | None = None):
+    """``BLSMethod.power`` + ``_assemble`` (``bls.py:274-301``, ``361-395``) on finite
+    flux-domain input: ``(frequency, power, extras)`` sorted by ascending frequency."""
+    t = np.asarray(t, dtype=np.float64)
+    flux = np.asarray(flux, dtype=np.float64)
+    err = np.ones_like(flux) if err is None else np.asarray(err, dtype=np.float64)
+    chunks = {name: [] for name in SEGMENT_FIELDS}
+    for per, dur in grid_segments(periods, meta, s):
+        out = bls_power(t, flux, err, per, dur, s.bins_per_duration,
+                        objective=s.objective, n_threads=n_threads)
+        for name in SEGMENT_FIELDS:
+            chunks[name].append(out[name])
+    arrays = {k: np.concatenate(v) for k, v in chunks.items()}
+    power = np.nan_to_num(arrays["power"], nan=0.0, posinf=0.0, neginf=0.0)
+    mean, std = float(power.mean()), float(power.std())
+    sde = (power - mean) / std if std > 0.0 else np.zeros_like(power)
+    frequency = 1.0 / arrays["period"]
+    order = np.argsort(frequency, kind="stable")
+    extras = {"depth": arrays["depth"], "depth_snr": arrays["depth_snr"],
+              "duration": arrays["duration"], "t0": arrays["transit_time"], "sde": sde}
+    return frequency[order], power[order], {k: v[order] for k, v in extras.items()}
+
+
+def best_index(power: np.ndarray) -> int:
+    """Index of ``Periodogram.best_period`` (``core/result.py:369-438``): the highest
+    finite candidate among interior local maxima and boundary peaks."""
+    safe = np.where(np.isfinite(power), power, -np.inf)
+    n = safe.size
+    cand = []
+    if n >= 3:
+        interior = (safe[1:-1] > safe[:-2]) & (safe[1:-1] >= safe[2:])
+        cand = (np.flatnonzero(interior) + 1).tolist()
+    if n == 1:
+        cand.append(0)
+    elif n >= 2:
+        if safe[0] >= safe[1]:
+            cand.append(0)
+        if safe[-1] > safe[-2]:
+            cand.append(n - 1)
+    cand = [c for c in cand if np.isfinite(power[c])]
+    if not cand:
+        finite = np.flatnonzero(np.isfinite(power))
+        return int(finite[np.argmax(power[finite])]) if finite.size else -1
+    cand = np.asarray(cand)
+    order = np.argsort(power[cand])[::-1]
+    return int(cand[order[0]])
