@@ -1,0 +1,239 @@
+"""The BLS method plugin on the B200 engine.
+
+Mirrors cuPeriod's ``BLSMethod`` (src/cuperiod/methods/bls.py): the same
+default log-segmented period grid, the same per-segment duration sets and the
+same segmentation of custom grids, so the engine searches exactly the
+(period, duration) trials the reference searches; ``power`` runs every segment
+of a light curve in one engine launch and assembles the reference's
+``Periodogram`` (SDE, extras, ascending frequency).  ``power_many`` searches a
+whole chunk of light curves sharing one grid in one launch -- the hook the
+batch runner uses instead of a per-curve loop.
+"""
+
+from __future__ import annotations
+
+import math
+from typing import Any, ClassVar, Literal, Sequence
+
+import numpy as np
+
+from . import _lib
+from .core import BACKENDS, _objective_flag
+from .errors import InsufficientDataError
+from .grid import GridSpec, check_grid_size
+from .lightcurve import Domain, LightCurve
+from .result import Periodogram
+from .settings import BLSSettings
+
+#: Per-period fields of a segment (bls.py:33).
+SEGMENT_FIELDS = ("period", "power", "depth", "depth_snr", "duration", "transit_time")
+
+Segment = tuple[np.ndarray, np.ndarray]
+
+#: The backend name recorded in results.
+BACKEND_NAME = "b200"
+
+
+def _segment_durations(p_lo: float, settings: BLSSettings) -> np.ndarray:
+    """Box durations of the segment starting at ``p_lo`` (bls.py:39-49)."""
+    d_hi = settings.duration_max_frac * p_lo
+    d_lo = max(settings.duration_min_frac * p_lo, settings.min_duration_days)
+    if d_lo >= d_hi:
+        return np.asarray([d_hi], dtype=np.float64)
+    return np.asarray(np.geomspace(d_lo, d_hi, settings.n_durations), dtype=np.float64)
+
+
+def _max_period(baseline: float, settings: BLSSettings) -> float:
+    """Largest searchable period (bls.py:52-54)."""
+    return min(settings.max_period_days, baseline / settings.min_transits)
+
+
+def _segment_bounds(baseline: float, settings: BLSSettings) -> list[tuple[float, float]]:
+    """``[(p_lo, p_hi), ...]`` of the default log segments (bls.py:57-68)."""
+    max_period = _max_period(baseline, settings)
+    bounds: list[tuple[float, float]] = []
+    p_lo = settings.min_period_days
+    while p_lo < max_period:
+        p_hi = min(p_lo * settings.segment_factor, max_period)
+        bounds.append((p_lo, p_hi))
+        p_lo = p_hi
+    return bounds
+
+
+def _segment_periods(baseline: float, settings: BLSSettings, *, time=None,
+                     context: str = "BLS default grid") -> list[tuple[float, np.ndarray]]:
+    """Non-empty default segments, each uniform in frequency (bls.py:71-105)."""
+    bounds = _segment_bounds(baseline, settings)
+    if not bounds:
+        return []
+    df = settings.grid_duration_frac / (settings.grid_oversample * baseline)
+    total = sum(max(0, math.ceil((1.0 / p_lo - 1.0 / p_hi) / df)) for p_lo, p_hi in bounds)
+    check_grid_size(total, automatic=True, time=time, baseline=baseline, context=context)
+    parts: list[tuple[float, np.ndarray]] = []
+    for p_lo, p_hi in bounds:
+        freq = np.arange(1.0 / p_hi, 1.0 / p_lo, df)
+        freq = freq[freq < 1.0 / p_lo]   # arange may overshoot its stop by a rounding quantum
+        if freq.size:
+            parts.append((p_lo, np.asarray(1.0 / freq[::-1], dtype=np.float64)))
+    return parts
+
+
+def _segment_grids(baseline: float, settings: BLSSettings, *, time=None,
+                   context: str = "BLS default grid") -> list[Segment]:
+    """``[(periods, durations), ...]`` of the default grid (bls.py:108-125)."""
+    return [(periods, _segment_durations(p_lo, settings))
+            for p_lo, periods in _segment_periods(baseline, settings, time=time,
+                                                  context=context)]
+
+
+def _log_segments(periods: np.ndarray, settings: BLSSettings) -> list[Segment]:
+    """Split any period grid into the default grid's log segments (bls.py:128-152)."""
+    p0 = float(periods.min())
+    with np.errstate(divide="ignore", invalid="ignore"):
+        index = np.floor(np.log(periods / p0) / math.log(settings.segment_factor)
+                         + 1e-9).astype(np.int64)
+    return [(np.ascontiguousarray(periods[index == k]),
+             _segment_durations(p0 * settings.segment_factor ** k, settings))
+            for k in np.unique(index).tolist()]
+
+
+def _grid_segments(grid: GridSpec, settings: BLSSettings) -> list[Segment]:
+    """The segments that search exactly ``grid``'s periods (bls.py:155-190)."""
+    periods = np.asarray(grid.period, dtype=np.float64)
+    if periods.size == 0:
+        return []
+    if not np.all(np.isfinite(periods)):
+        raise ValueError("BLS: trial periods must be finite; drop frequency 0 from the grid")
+    starts = grid.meta.get("segment_starts")
+    sizes = grid.meta.get("segment_sizes")
+    if (starts is not None and sizes is not None and len(starts) == len(sizes)
+            and sum(int(s) for s in sizes) == periods.size):
+        segments: list[Segment] = []
+        offset = 0
+        for p_lo, size in zip(starts, sizes):
+            stop = offset + int(size)
+            segments.append((periods[offset:stop], _segment_durations(float(p_lo), settings)))
+            offset = stop
+        return segments
+    return _log_segments(periods, settings)
+
+
+def _assemble(fields: dict[str, np.ndarray], n: int, baseline: float, meta: Any) -> Periodogram:
+    """SDE and the Periodogram of one curve's concatenated segments (bls.py:274-301)."""
+    power = np.nan_to_num(fields["power"], nan=0.0, posinf=0.0, neginf=0.0)
+    mean, std = float(power.mean()), float(power.std())
+    sde = (power - mean) / std if std > 0.0 else np.zeros_like(power)
+    extras = {"depth": fields["depth"], "depth_snr": fields["depth_snr"],
+              "duration": fields["duration"], "t0": fields["transit_time"], "sde": sde}
+    return Periodogram.from_spectrum(method="BLS", backend=BACKEND_NAME,
+                                     frequency=1.0 / fields["period"], power=power,
+                                     objective_sense="max", n_samples=n, baseline=baseline,
+                                     extras=extras, meta=meta)
+
+
+def _prepared_curve(lc: LightCurve, settings: BLSSettings):
+    """``finite()``, the reference's guards and unit errors (bls.py:369-380)."""
+    finite = lc.finite()
+    if finite.n < settings.min_detections:
+        raise InsufficientDataError(
+            f"BLS: {finite.n} finite points < min_detections {settings.min_detections}")
+    if finite.baseline <= 0.0:
+        raise InsufficientDataError("BLS: no usable time baseline")
+    err = finite.error if finite.error is not None else np.ones_like(finite.value)
+    return finite, err
+
+
+class BLSMethod:
+    """Box Least Squares on the B200 engine (the reference's ``BLSMethod``,
+    bls.py:304-417, with ``"b200"`` as its only backend)."""
+
+    name: ClassVar[str] = "BLS"
+    objective_sense: ClassVar[Literal["max", "min"]] = "max"
+    supports_multiband: ClassVar[bool] = False
+    natural_domain: ClassVar[Domain] = Domain.FLUX
+    settings_cls: ClassVar[type] = BLSSettings
+    gpu_backend: ClassVar[str] = BACKEND_NAME
+    all_backends: ClassVar[tuple[str, ...]] = (BACKEND_NAME,)
+
+    def resolve_backend(self, backend: str | None) -> str:
+        """Every GPU-ish selector resolves to this engine; CPU backends do not exist
+        here and raise (there is no CPU fallback)."""
+        b = (backend or "auto").lower()
+        if b in BACKENDS:
+            return BACKEND_NAME
+        from .errors import BackendUnavailableError
+        raise BackendUnavailableError(
+            f"BLS backend {backend!r} is not available: this engine runs on the B200 only")
+
+    def default_grid(self, lc: LightCurve, settings: BLSSettings) -> GridSpec:
+        """Log period segments up to min(max_period_days, baseline/min_transits),
+        with the segmentation recorded in ``meta`` (bls.py:327-359)."""
+        finite = lc.finite()
+        parts = _segment_periods(finite.baseline, settings, time=finite.time)
+        if not parts:
+            raise InsufficientDataError("BLS: baseline too short for the configured period range")
+        periods = np.concatenate([p for _, p in parts])
+        return GridSpec(kind="period", values=periods, uniform=False,
+                        meta={"segmented": True,
+                              "segment_starts": tuple(float(p) for p, _ in parts),
+                              "segment_sizes": tuple(int(p.size) for _, p in parts)})
+
+    def power(self, grid: GridSpec, lc: LightCurve, settings: BLSSettings,
+              backend: str = BACKEND_NAME, engine: _lib.Engine | None = None) -> Periodogram:
+        """One light curve: every segment in one launch, then the reference's
+        assembly (bls.py:361-395)."""
+        self.resolve_backend(backend)
+        finite, err = _prepared_curve(lc, settings)
+        segments = _grid_segments(grid, settings)
+        if not segments:
+            raise InsufficientDataError("BLS: empty trial grid")
+        out = self._search(segments, [(finite.time, finite.value, err)], settings, engine)
+        fields = _fields(out[:, 0, :], segments)
+        return _assemble(fields, finite.n, finite.baseline, finite.meta)
+
+    def power_many(self, grid: GridSpec, lcs: Sequence[LightCurve], settings: BLSSettings,
+                   backend: str = BACKEND_NAME, engine: _lib.Engine | None = None
+                   ) -> list[Periodogram]:
+        """Many light curves over one grid in one launch; one Periodogram each."""
+        self.resolve_backend(backend)
+        segments = _grid_segments(grid, settings)
+        if not segments:
+            raise InsufficientDataError("BLS: empty trial grid")
+        prepared = [_prepared_curve(lc, settings) for lc in lcs]
+        out = self._search(segments, [(f.time, f.value, e) for f, e in prepared], settings, engine)
+        return [_assemble(_fields(out[:, i, :], segments), f.n, f.baseline, f.meta)
+                for i, (f, _) in enumerate(prepared)]
+
+    def _search(self, segments, curves, settings, engine):
+        grid = _lib.PackedGrid.from_segments(segments, settings.bins_per_duration,
+                                             _objective_flag(settings.objective))
+        packed = _lib.PackedCurves.from_arrays(curves)
+        return (engine or _lib.default_engine()).search(grid, packed)
+
+
+def _fields(out: np.ndarray, segments: list[Segment]) -> dict[str, np.ndarray]:
+    """Engine rows (7, P) of one curve as the assembly's per-period fields."""
+    names = _lib.FIELD_NAMES
+    fields = {name: np.ascontiguousarray(out[i]) for i, name in enumerate(names)}
+    fields["period"] = np.concatenate([np.asarray(p, dtype=np.float64) for p, _ in segments])
+    return fields
+
+
+_REGISTRY: dict[str, BLSMethod] = {}
+
+
+def register(method: BLSMethod) -> None:
+    _REGISTRY[method.name.upper()] = method
+
+
+def get_method(name: str) -> BLSMethod:
+    from .errors import UnknownMethodError
+    key = "".join(ch for ch in str(name) if ch.isalnum()).upper()
+    if key not in _REGISTRY:
+        raise UnknownMethodError(f"unknown method {name!r}; this engine provides BLS")
+    return _REGISTRY[key]
+
+
+register(BLSMethod())
+
+__all__ = ["BLSMethod", "get_method", "register"]

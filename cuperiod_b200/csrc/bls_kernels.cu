@@ -43,6 +43,7 @@ constexpr int kPts = kChunkPts;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr float kRel = 1.0f / 262144.0f;    // 2^-18: relative slack of FP32 key bounds
 constexpr int kCasLimit = 1 << 16;          // retries of one FP64 shared add
+constexpr int kNoBox = 1 << 29;             // duration slot past the last real duration
 
 struct TileShared {
     WorkItem item;
@@ -52,7 +53,10 @@ struct TileShared {
     double freq[kMaxTile];
     uint32_t scale[kMaxTile];
     int32_t nb[kMaxTile];
-    int32_t dur[kMaxDur];
+    int32_t dur[kMaxDur + 4];       // padded with kNoBox for groups of four
+    double win_v[kMaxTile];         // per period of the tile: the best box
+    int32_t win_di[kMaxTile];
+    int32_t win_n[kMaxTile];
     uint32_t tot_a[kWarps];
     int32_t tot_b[kWarps];
     uint32_t tot_c[kWarps];
@@ -221,25 +225,40 @@ __device__ __forceinline__ void fold_points(const TileShared& s, unsigned char* 
     const int hlp = padded_bins(hl);
     for (int q = 0; q < pt; ++q) {
         const double f = s.freq[q];
-        const double P = s.per[q];
         const uint32_t S = s.scale[q];
-        const int nbq = s.nb[q];
         unsigned char* hq = hist_base + (size_t)q * hist_period_bytes<MODE>(hl);
-        // the lane's run of equal bins, flushed to shared memory when the bin changes
+        // 1. the fast fold of all points, straight-line (-1: near an edge, -2: skip)
+        int ind[kPts];
+        bool miss = false;
+#pragma unroll
+        for (int r = 0; r < kPts; ++r) {
+            ind[r] = fast ? fold_fast(p.x[r], f, S, fb, fmask, mu, fr_span, mphi, phi_span) : -1;
+            if (TAIL && p.x[r] < 0.0) ind[r] = -2;
+            miss |= ind[r] == -1;
+        }
+        // 2. rare: the reference's IEEE chain for points near a cycle or bin edge
+        if (miss) {
+            const double P = s.per[q];
+            const int nbq = s.nb[q];
+#pragma unroll
+            for (int r = 0; r < kPts; ++r) {
+                if (ind[r] == -1) {
+                    const int e = fold_exact(p.x[r], P, bin, width);
+                    ind[r] = e > nbq ? -2 : e;        // a bin the reference never reads
+                }
+            }
+        }
+        // 3. merge the lane's runs of equal bins, one flush per run
         int cur = -1;
         uint32_t sa = 0u, sb = 0u, sc = 0u;
         double sr = 0.0, sw = 0.0;
 #pragma unroll
         for (int r = 0; r < kPts; ++r) {
-            if (TAIL && p.x[r] < 0.0) continue;
-            int ind = fast ? fold_fast(p.x[r], f, S, fb, fmask, mu, fr_span, mphi, phi_span) : -1;
-            if (ind < 0) {
-                ind = fold_exact(p.x[r], P, bin, width);
-                if (ind > nbq) continue;     // a bin the reference never reads
-            }
-            if (ind != cur) {
+            const int bi = ind[r];
+            if (bi < 0) continue;
+            if (bi != cur) {
                 if (cur >= 0) flush_run<MODE>(hq, hlp, cur, sa, sb, sc, sr, sw, flag);
-                cur = ind;
+                cur = bi;
                 sa = sb = sc = 0u;
                 sr = sw = 0.0;
             }
@@ -259,6 +278,23 @@ __device__ __forceinline__ void fold_points(const TileShared& s, unsigned char* 
 // Exact prefix of r_q at bin i from the two 32-bit prefix words.
 __device__ __forceinline__ long long prefix_r(const uint32_t* A, const int32_t* B, int i) {
     return (long long)B[i] * (1ll << kHalfBits) + (long long)A[i];
+}
+
+// Exact sums of box (n, d) in the reference's units from one period's prefixes.
+template <int MODE>
+__device__ __forceinline__ BoxSums box_sums(const uint32_t* A, const int32_t* B, const uint32_t* C,
+                                            const double* R, const double* W,
+                                            const CurveDesc& cv, int n, int d) {
+    BoxSums b;
+    if (MODE == MODE_UNIFORM) {
+        b.iv_in = (double)(C[n + d] - C[n]) * cv.w_uniform;
+        b.y_in = ldexp((double)(prefix_r(A, B, n + d) - prefix_r(A, B, n)), -cv.e_r) +
+                 cv.ybar * b.iv_in;
+    } else {
+        b.iv_in = ldexp(W[n + d] - W[n], -cv.e_i);
+        b.y_in = ldexp(R[n + d] - R[n], -cv.e_r) + cv.ybar * b.iv_in;
+    }
+    return b;
 }
 
 template <int MODE>
@@ -295,7 +331,7 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
             s.scale[tid] = a.scale[g0 + tid];
             s.nb[tid] = a.nbins[g0 + tid];
         }
-        if (tid < n_dur) s.dur[tid] = a.dur_bins[s.seg.dur_off + tid];
+        if (tid < kMaxDur + 4) s.dur[tid] = tid < n_dur ? a.dur_bins[s.seg.dur_off + tid] : kNoBox;
         __syncthreads();
 
         double* out = a.out + s.curve.out_off + g0;
@@ -333,12 +369,13 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
         }
         __syncthreads();
 
-        // ---- 2-4. per period: pad, prefix, sweep, reduce, write ----------------
+        // ---- 2-3. per period: pad, prefix, sweep, reduce ------------------------
         const size_t hist_bytes = (size_t)pt * pbytes;               // multiple of 16
         float2* scr = reinterpret_cast<float2*>(smem + hist_bytes);
         const CurveDesc& cv = s.curve;
         const int obj = a.obj_flag;
         const int e_r = cv.e_r, e_i = cv.e_i;
+        const int o = s.seg.oversample;
 
         for (int q = 0; q < pt; ++q) {
             const int nb = s.nb[q];
@@ -349,29 +386,41 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
             uint32_t* C = A + 2 * hlp;
             double* R = reinterpret_cast<double*>(hq);            // GENERAL sums
             double* W = R + hlp;
-
-            if (tid == 0) {                     // wrap pad, sequential like the reference
-                const int o = s.seg.oversample;
-                for (int k = 0; k < o; ++k) {
-                    const int dst = nb - o + k;
-                    if (dst >= 0 && dst < s.seg.width && dst < hl && 1 + k < hl) {
-                        if (MODE == MODE_UNIFORM) {
-                            A[dst] = A[1 + k];
-                            B[dst] = B[1 + k];
-                            C[dst] = C[1 + k];
-                        } else {
-                            R[dst] = R[1 + k];
-                            W[dst] = W[1 + k];
-                        }
+            auto copy_bin = [&](int dst, int src) {
+                if (dst >= 0 && dst < s.seg.width && dst < hl && src < hl) {
+                    if (MODE == MODE_UNIFORM) {
+                        A[dst] = A[src];
+                        B[dst] = B[src];
+                        C[dst] = C[src];
+                    } else {
+                        R[dst] = R[src];
+                        W[dst] = W[src];
                     }
                 }
+            };
+
+            // wrap pad: bins 1..o copied to nb-o..nb-1 (_bls_core.py:377-381).  When
+            // the two ranges overlap one thread copies in the reference's order;
+            // otherwise the warp that owns each destination copies it in pass 1
+            // (the source bins are not written before pass 2).
+            const bool overlap = nb - o <= o;
+            if (overlap) {
+                if (tid == 0)
+                    for (int k = 0; k < o; ++k) copy_bin(nb - o + k, 1 + k);
+                __syncthreads();
             }
-            __syncthreads();
 
             // prefix scan, pass 1: per-warp totals of each contiguous range
             const int E = ((L + kWarps * 32 - 1) / (kWarps * 32)) * 32;
             const int lo_i = warp * E;
             const int hi_i = min(L, lo_i + E);
+            if (!overlap) {
+                for (int k = lane; k < o; k += 32) {
+                    const int dst = nb - o + k;
+                    if (dst >= lo_i && dst < hi_i) copy_bin(dst, 1 + k);
+                }
+                __syncwarp();
+            }
             {
                 uint32_t ta = 0u, tc = 0u;
                 int32_t tb = 0;
@@ -425,11 +474,11 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                         uint32_t va = in ? A[i] : 0u, vc = in ? C[i] : 0u;
                         int32_t vb = in ? B[i] : 0;
 #pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const uint32_t xa = __shfl_up_sync(kFull, va, o);
-                            const int32_t xb = __shfl_up_sync(kFull, vb, o);
-                            const uint32_t xc = __shfl_up_sync(kFull, vc, o);
-                            if (lane >= o) {
+                        for (int k = 1; k < 32; k <<= 1) {
+                            const uint32_t xa = __shfl_up_sync(kFull, va, k);
+                            const int32_t xb = __shfl_up_sync(kFull, vb, k);
+                            const uint32_t xc = __shfl_up_sync(kFull, vc, k);
+                            if (lane >= k) {
                                 va += xa;
                                 vb += xb;
                                 vc += xc;
@@ -450,10 +499,10 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                     } else {
                         double vr = in ? R[i] : 0.0, vw = in ? W[i] : 0.0;
 #pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const double xr = __shfl_up_sync(kFull, vr, o);
-                            const double xw = __shfl_up_sync(kFull, vw, o);
-                            if (lane >= o) {
+                        for (int k = 1; k < 32; k <<= 1) {
+                            const double xr = __shfl_up_sync(kFull, vr, k);
+                            const double xw = __shfl_up_sync(kFull, vw, k);
+                            if (lane >= k) {
                                 vr += xr;
                                 vw += xw;
                             }
@@ -481,27 +530,12 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
 #pragma unroll
             for (int w = 0; w < kWarps; ++w) tmax = fmaxf(tmax, s.red_t[w]);
 
-            // weight prefix and flux*weight prefix at bin i, in the reference's units
             auto iv_prefix = [&](int i) -> double {
                 return MODE == MODE_UNIFORM ? (double)C[i] * cv.w_uniform : ldexp(W[i], -e_i);
             };
-            // exact sums of box (n, d) in the reference's units
-            auto box_sums = [&](int n, int d) -> BoxSums {
-                BoxSums b;
-                if (MODE == MODE_UNIFORM) {
-                    b.iv_in = (double)(C[n + d] - C[n]) * cv.w_uniform;
-                    b.y_in = ldexp((double)(prefix_r(A, B, n + d) - prefix_r(A, B, n)), -e_r) +
-                             cv.ybar * b.iv_in;
-                } else {
-                    b.iv_in = ldexp(W[n + d] - W[n], -e_i);
-                    b.y_in = ldexp(R[n + d] - R[n], -e_r) + cv.ybar * b.iv_in;
-                }
-                return b;
-            };
             auto exact = [&](int n, int d) -> double {
-                return box_objective(box_sums(n, d), cv, obj);
+                return box_objective(box_sums<MODE>(A, B, C, R, W, cv, n, d), cv, obj);
             };
-
             if (a.debug_prefix != nullptr && q == 0) {   // test hook: this period's prefixes
                 for (int i = tid; i < L; i += kThreads) {
                     const double r_i = MODE == MODE_UNIFORM ? ldexp((double)prefix_r(A, B, i), -e_r)
@@ -511,12 +545,16 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                 }
             }
 
-            // ---- sweep: durations outer, starts inner (the reference's order) ----
+            // ---- sweep: each lane one start, all durations ------------------------
             const float Et = cv.exact_all ? CUDART_INF_F : tmax * (1.0f / 2097152.0f);  // 2^-21
             const float Wt = MODE == MODE_UNIFORM ? (float)cv.n_points : (float)cv.i_total;
             const float Ei = MODE == MODE_UNIFORM ? 0.0f : Wt * (1.0f / 2097152.0f);
             const float floor_q =
                 MODE == MODE_GENERAL ? (float)ldexp(cv.ivar_floor, e_i) * (1.0f + 1e-3f) : 0.0f;
+            int dmin = 1 << 29;
+            for (int k = 0; k < n_dur; ++k)
+                if (s.dur[k] < nb) dmin = min(dmin, s.dur[k]);
+            const int nmax = nb - dmin;                // largest start of any box
 
             bool has = false, ex_ok = false;
             int bn = 0, bdi = 0;
@@ -524,91 +562,107 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
             double ex_v = -CUDART_INF;
             float thr = -1.0f;
 
-            for (int di = 0; di < n_dur; ++di) {
-                const int d = s.dur[di];
-                if (d >= nb) continue;
-                const int nmax = nb - d;
-                for (int n0 = warp * 32; n0 <= nmax; n0 += kThreads) {
-                    const int n = n0 + lane;
-                    bool upd = false;
-                    if (n <= nmax) {
-                        const float2 av = scr[n];
-                        const float2 bv = scr[n + d];
-                        const float t = bv.x - av.x;
-                        const float iv = bv.y - av.y;       // count, or scaled weight
-                        const float ov = Wt - iv;
-                        float den_lo, den_hi;
-                        bool ok, sure_valid;
-                        if (MODE == MODE_UNIFORM) {
-                            den_lo = iv * ov;                // exact counts: > 0 iff valid
-                            if (obj) den_lo *= ov;
-                            den_hi = den_lo;
-                            sure_valid = true;
-                            ok = den_lo > 0.0f;
-                        } else {
-                            const float il = fmaxf(iv - Ei, 0.0f), ol = fmaxf(ov - Ei, 0.0f);
-                            const float ih = iv + Ei, oh = ov + Ei;
-                            den_lo = obj ? il * ol * ol : il * ol;
-                            den_hi = obj ? ih * oh * oh : ih * oh;
-                            sure_valid = (il >= floor_q) & (ol >= floor_q);
-                            // an empty box is exactly 0 in the FP64 prefix
-                            ok = (den_lo > 0.0f) || (W[n + d] != W[n]);
-                        }
-                        const float th = fabsf(t) + Et;
-                        if (ok && t <= Et && !(th * th < thr * den_lo)) {
-                            // ---- rare path: a box that may compete ----
-                            const float tl = fmaxf(fabsf(t) - Et, 0.0f);
-                            const float khi = den_lo > 0.0f
-                                                  ? __fdividef(th * th, den_lo) * (1.0f + kRel)
-                                                  : CUDART_INF_F;
-                            const float klo = __fdividef(tl * tl, den_hi) * (1.0f - kRel);
-                            const bool sure = (t < -Et) & sure_valid & (klo > 0.0f);
-                            if (!has) {
-                                if (sure) {
-                                    has = true; ex_ok = false; bn = n; bdi = di; lb = klo; hb = khi;
-                                    upd = true;
-                                } else {
-                                    const double v = exact(n, d);
-                                    if (v > -CUDART_INF) {
-                                        has = true; ex_ok = true; ex_v = v; bn = n; bdi = di;
-                                        lb = klo; hb = khi; upd = true;
-                                    }
-                                }
-                            } else if (sure && klo > hb) {
-                                ex_ok = false; bn = n; bdi = di; lb = klo; hb = khi; upd = true;
-                            } else if (khi >= lb) {
-                                if (!ex_ok) { ex_v = exact(bn, s.dur[bdi]); ex_ok = true; }
-                                const double v = exact(n, d);
-                                if (v > -CUDART_INF && better(v, di, n, ex_v, bdi, bn)) {
-                                    ex_v = v; bn = n; bdi = di; lb = fmaxf(klo, lb); hb = khi;
-                                    upd = true;
-                                }
+            // one box that passed the screen: keep it if it may be this lane's best
+            auto consider = [&](int n, int di, int d, float t, float den_lo, float den_hi,
+                                bool sure_valid) -> bool {
+                const float th = fabsf(t) + Et;
+                const float tl = fmaxf(fabsf(t) - Et, 0.0f);
+                const float khi =
+                    den_lo > 0.0f ? __fdividef(th * th, den_lo) * (1.0f + kRel) : CUDART_INF_F;
+                const float klo = __fdividef(tl * tl, den_hi) * (1.0f - kRel);
+                const bool sure = (t < -Et) & sure_valid & (klo > 0.0f);
+                if (!has) {
+                    if (sure) {
+                        has = true; ex_ok = false; bn = n; bdi = di; lb = klo; hb = khi;
+                        return true;
+                    }
+                    const double v = exact(n, d);
+                    if (v > -CUDART_INF) {
+                        has = true; ex_ok = true; ex_v = v; bn = n; bdi = di; lb = klo; hb = khi;
+                        return true;
+                    }
+                    return false;
+                }
+                if (sure && klo > hb) {
+                    ex_ok = false; bn = n; bdi = di; lb = klo; hb = khi;
+                    return true;
+                }
+                if (khi >= lb) {
+                    if (!ex_ok) { ex_v = exact(bn, s.dur[bdi]); ex_ok = true; }
+                    const double v = exact(n, d);
+                    if (v > -CUDART_INF && better(v, di, n, ex_v, bdi, bn)) {
+                        ex_v = v; bn = n; bdi = di; lb = fmaxf(klo, lb); hb = khi;
+                        return true;
+                    }
+                }
+                return false;
+            };
+
+            for (int n0 = warp * 32; n0 <= nmax; n0 += kThreads) {
+                const int n = n0 + lane;
+                bool upd = false;
+                if (n <= nmax) {
+                    const float2 av = scr[n];
+                    for (int di0 = 0; di0 < n_dur; di0 += 4) {
+                        float tt[4], dl[4], dh[4];
+                        bool cand[4], sv[4];
+                        int dd[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int d = s.dur[di0 + k];          // padded with kNoBox
+                            const bool inb = (d < nb) & (n + d <= nb);
+                            const float2 bv = scr[inb ? n + d : n];
+                            const float t = bv.x - av.x;
+                            const float iv = bv.y - av.y;        // count, or scaled weight
+                            const float ov = Wt - iv;
+                            float den_lo, den_hi;
+                            bool ok, sure_valid;
+                            if (MODE == MODE_UNIFORM) {
+                                den_lo = obj ? iv * ov * ov : iv * ov;   // > 0 iff valid
+                                den_hi = den_lo;
+                                sure_valid = true;
+                                ok = den_lo > 0.0f;
+                            } else {
+                                const float il = fmaxf(iv - Ei, 0.0f), ol = fmaxf(ov - Ei, 0.0f);
+                                const float ih = iv + Ei, oh = ov + Ei;
+                                den_lo = obj ? il * ol * ol : il * ol;
+                                den_hi = obj ? ih * oh * oh : ih * oh;
+                                sure_valid = (il >= floor_q) & (ol >= floor_q);
+                                // an empty box is exactly 0 in the FP64 prefix
+                                ok = (den_lo > 0.0f) || (inb && W[n + d] != W[n]);
                             }
+                            const float th = fabsf(t) + Et;
+                            cand[k] = inb & ok & (t <= Et) & !(th * th < thr * den_lo);
+                            tt[k] = t;
+                            dl[k] = den_lo;
+                            dh[k] = den_hi;
+                            sv[k] = sure_valid;
+                            dd[k] = d;
+                        }
+                        if (cand[0] | cand[1] | cand[2] | cand[3]) {
+#pragma unroll
+                            for (int k = 0; k < 4; ++k)
+                                if (cand[k]) upd |= consider(n, di0 + k, dd[k], tt[k], dl[k], dh[k], sv[k]);
                         }
                     }
-                    if (__any_sync(kFull, upd))
-                        thr = warp_max(has ? lb * (1.0f - 2.0f * kRel) : -1.0f);
                 }
+                if (__any_sync(kFull, upd))
+                    thr = warp_max(has ? lb * (1.0f - 2.0f * kRel) : -1.0f);
             }
 
-            // ---- reduce: candidates that may hold the period's maximum ----------
-            float L_lo = warp_max(has ? lb : -1.0f);
-            if (lane == 0) s.red_f[warp] = L_lo;
-            __syncthreads();
-            L_lo = -1.0f;
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) L_lo = fmaxf(L_lo, s.red_f[w]);
+            // ---- reduce: lanes whose best may be their warp's maximum -------------
+            const float Lw = warp_max(has ? lb : -1.0f);
             double v = -CUDART_INF;
             int vdi = 1 << 30, vn = 1 << 30;
-            if (has && hb >= L_lo) {
+            if (has && hb >= Lw) {
                 if (!ex_ok) { ex_v = exact(bn, s.dur[bdi]); ex_ok = true; }
                 v = ex_v; vdi = bdi; vn = bn;
             }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(kFull, v, o);
-                const int odi = __shfl_xor_sync(kFull, vdi, o);
-                const int on = __shfl_xor_sync(kFull, vn, o);
+            for (int k = 16; k > 0; k >>= 1) {
+                const double ov = __shfl_xor_sync(kFull, v, k);
+                const int odi = __shfl_xor_sync(kFull, vdi, k);
+                const int on = __shfl_xor_sync(kFull, vn, k);
                 if (better(ov, odi, on, v, vdi, vn)) { v = ov; vdi = odi; vn = on; }
             }
             if (lane == 0) { s.red_v[warp] = v; s.red_di[warp] = vdi; s.red_n[warp] = vn; }
@@ -618,32 +672,47 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                     if (better(s.red_v[w], s.red_di[w], s.red_n[w], v, vdi, vn)) {
                         v = s.red_v[w]; vdi = s.red_di[w]; vn = s.red_n[w];
                     }
-                double* o = out + q;
-                if (!(v > -CUDART_INF)) {
-                    o[0] = -CUDART_INF;
-                    for (int f = 1; f < kFields; ++f) o[f * ostride] = 0.0;
-                } else {
-                    const int d = s.dur[vdi];
-                    const BoxSums b = box_sums(vn, d);
-                    const double iv_out = cv.sum_ivar - b.iv_in;
-                    const double yin = b.y_in / b.iv_in;
-                    const double yout = (cv.sum_y - b.y_in) / iv_out;
-                    const double depth = yout - yin;
-                    const double derr = sqrt(1.0 / b.iv_in + 1.0 / iv_out);
-                    const double dsnr = depth / derr;
-                    const double ll = 0.5 * b.iv_in * depth * depth;
-                    const double bin = s.seg.bin_duration;
-                    const double dur = (double)d * bin;
-                    o[0] = obj == 0 ? dsnr : ll;
-                    o[1 * ostride] = depth;
-                    o[2 * ostride] = derr;
-                    o[3 * ostride] = dsnr;
-                    o[4 * ostride] = dur;
-                    o[5 * ostride] = fmod((double)vn * bin + 0.5 * dur, s.per[q]) + cv.t_min;
-                    o[6 * ostride] = ll;
-                }
+                s.win_v[q] = v;
+                s.win_di[q] = vdi;
+                s.win_n[q] = vn;
             }
-            __syncthreads();
+        }
+
+        // ---- 4. the tile's seven output fields, one thread per period ----------
+        __syncthreads();
+        if (tid < pt) {
+            const int q = tid;
+            unsigned char* hq = smem + (size_t)q * pbytes;
+            const uint32_t* A = reinterpret_cast<const uint32_t*>(hq);
+            const int32_t* B = reinterpret_cast<const int32_t*>(A + hlp);
+            const uint32_t* C = A + 2 * hlp;
+            const double* R = reinterpret_cast<const double*>(hq);
+            const double* W = R + hlp;
+            double* op = out + q;
+            if (!(s.win_v[q] > -CUDART_INF)) {
+                op[0] = -CUDART_INF;
+                for (int f = 1; f < kFields; ++f) op[f * ostride] = 0.0;
+            } else {
+                const int vn = s.win_n[q];
+                const int d = s.dur[s.win_di[q]];
+                const BoxSums b = box_sums<MODE>(A, B, C, R, W, cv, vn, d);
+                const double iv_out = cv.sum_ivar - b.iv_in;
+                const double yin = b.y_in / b.iv_in;
+                const double yout = (cv.sum_y - b.y_in) / iv_out;
+                const double depth = yout - yin;
+                const double derr = sqrt(1.0 / b.iv_in + 1.0 / iv_out);
+                const double dsnr = depth / derr;
+                const double ll = 0.5 * b.iv_in * depth * depth;
+                const double bin = s.seg.bin_duration;
+                const double dur = (double)d * bin;
+                op[0] = obj == 0 ? dsnr : ll;
+                op[1 * ostride] = depth;
+                op[2 * ostride] = derr;
+                op[3 * ostride] = dsnr;
+                op[4 * ostride] = dur;
+                op[5 * ostride] = fmod((double)vn * bin + 0.5 * dur, s.per[q]) + cv.t_min;
+                op[6 * ostride] = ll;
+            }
         }
     }
 }

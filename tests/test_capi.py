@@ -1,0 +1,49 @@
+"""The C ABI library loads without a GPU and exports every function the public
+header declares."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+
+def _declared():
+    text = open(os.path.join(ROOT, "include", "bls_b200.h")).read()
+    return sorted(set(re.findall(r"^(?:int|const char\*)\s+(bls_\w+)\(", text, re.M)))
+
+
+def test_header_declares_the_entry_points():
+    names = _declared()
+    for must in ("bls_engine_create", "bls_engine_destroy", "bls_last_error", "bls_prepare",
+                 "bls_launch", "bls_download", "bls_download_best", "bls_search",
+                 "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from cuperiod_b200 import _lib
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in _declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_struct_layouts_match_the_header():
+    from cuperiod_b200 import _lib
+    # BlsTune: 5 int32; BlsGrid: int32 + 4 pointers + 2 int32 (padded); BlsCurves: int32 + 4 ptrs
+    assert ctypes.sizeof(_lib.BlsTune) == 20
+    assert ctypes.sizeof(_lib.BlsGrid) == 8 + 4 * 8 + 8
+    assert ctypes.sizeof(_lib.BlsCurves) == 8 + 4 * 8
+    assert ctypes.sizeof(_lib.BlsBatchInfo) == 4 + 4 + 8 * 3 + 8 * 3 + 8 + 4 * 4
+
+
+def test_engine_creation_without_a_device_raises():
+    import pytest
+    import torch
+    from cuperiod_b200 import _lib
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises((_lib.EngineError, RuntimeError)):
+        _lib.Engine()

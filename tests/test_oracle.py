@@ -1,0 +1,45 @@
+"""The CPU oracle is pinned to the reference: bit-exact on every golden vector the
+reference's numba backend produced (tests/golden/make_golden.py)."""
+
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from _cases import FIELDS, GOLDEN, kernel_golden
+from oracle import oracle
+
+
+@pytest.mark.parametrize("meta_arrays", kernel_golden(), ids=lambda c: c[0]["name"])
+def test_oracle_bit_exact_on_golden(meta_arrays):
+    meta, a = meta_arrays
+    with np.errstate(over="ignore", divide="ignore", invalid="ignore"):
+        out = oracle.bls_power(a["t"], a["y"], a["dy"], a["periods"], a["durations"],
+                               meta["oversample"], objective=meta["objective"], n_threads=4)
+    got = np.stack([out[f] for f in FIELDS])
+    assert np.array_equal(got, a["out"], equal_nan=True)
+
+
+def _method_cases():
+    index = json.load(open(os.path.join(GOLDEN, "method_cases.json")))
+    z = np.load(os.path.join(GOLDEN, "method_cases.npz"))
+    return [(m, z) for m in index]
+
+
+@pytest.mark.parametrize("case", _method_cases(), ids=lambda c: c[0]["name"])
+def test_oracle_method_level_on_golden(case):
+    meta, z = case
+    k = meta["key"]
+    s = oracle.Settings(**meta["settings"])
+    periods = z[f"{k}_grid"]
+    freq, power, extras = oracle.method_power(z[f"{k}_t"], z[f"{k}_flux"], z[f"{k}_err"],
+                                              periods, meta["grid_meta"], s, n_threads=4)
+    np.testing.assert_array_equal(freq, z[f"{k}_frequency"])
+    np.testing.assert_array_equal(power, z[f"{k}_power"])
+    for name in ("depth", "depth_snr", "duration", "t0", "sde"):
+        np.testing.assert_array_equal(extras[name], z[f"{k}_x_{name}"])
+    i = oracle.best_index(power)
+    assert 1.0 / freq[i] == meta["best_period"]
