@@ -93,12 +93,45 @@ __device__ __forceinline__ int fold_fast(double x, double f, uint32_t S, int fb,
     return ok ? (int)(v >> fb) + 1 : -1;
 }
 
+// Shared-memory accesses by 32-bit shared-space address (the hot loops compute
+// addresses in 32-bit arithmetic instead of converting generic pointers).
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+template <int OFF>
+__device__ __forceinline__ void red_add_u32(uint32_t a, uint32_t v) {
+    asm volatile("red.shared.add.u32 [%0+%2], %1;" ::"r"(a), "r"(v), "n"(OFF) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_u32(uint32_t a) {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void st_u32(uint32_t a, uint32_t v) {
+    asm volatile("st.shared.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ double ld_f64(uint32_t a) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void st_f64(uint32_t a, double v) {
+    asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ float2 ld_f2(uint32_t a) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void st_f2(uint32_t a, float2 v) {
+    asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
+}
+
 // FP64 add to a shared-memory word by a bounded compare-and-swap loop in the
 // shared state space.  The loop is lock-free (a failed swap means another thread
 // succeeded); the bound only guards against the impossible and sets `flag`.
-__device__ __forceinline__ void shared_add_f64(double* p, double v, int32_t* flag) {
+__device__ __forceinline__ void shared_add_f64(uint32_t addr, double v, int32_t* flag) {
     if (v == 0.0) return;
-    const unsigned addr = (unsigned)__cvta_generic_to_shared(p);
     unsigned long long old;
     asm volatile("ld.shared.u64 %0, [%1];" : "=l"(old) : "r"(addr) : "memory");
     for (int it = 0; it < kCasLimit; ++it) {
@@ -151,17 +184,17 @@ __device__ __forceinline__ double box_objective(const BoxSums& s, const CurveDes
     return 0.5 * s.iv_in * depth * depth;
 }
 
-// Bins held per period, rounded so each per-period array starts 16-byte aligned.
-__device__ __host__ __forceinline__ int padded_bins(int hl) { return (hl + 3) & ~3; }
-
-// Histogram layout of one period (hlp = padded_bins(hl) bins).
-//  UNIFORM: A[hlp] (sum of the low 13 bits of r_q), B[hlp] (sum of its signed
-//           high part), C[hlp] (count) -- all 32-bit; prefix sums in place.
-//  GENERAL: R[hlp], W[hlp] -- FP64 sums of the scaled centred flux*weight and
-//           of the scaled weight; prefix sums in place.
+// Histogram layout of one period: one record per bin, prefix sums in place.
+//  UNIFORM: {A, B, C}, 12 bytes -- sum of the low 13 bits of r_q, sum of its
+//           signed high part, count (32-bit words);
+//  GENERAL: {R, W}, 16 bytes -- FP64 sums of the scaled centred flux*weight and
+//           of the scaled weight.
+// A period's region is padded to 16 bytes.
+template <int MODE>
+__device__ __host__ constexpr int bin_bytes() { return MODE == MODE_UNIFORM ? 12 : 16; }
 template <int MODE>
 __device__ __host__ __forceinline__ size_t hist_period_bytes(int hl) {
-    return (size_t)padded_bins(hl) * (MODE == MODE_UNIFORM ? 12 : 16);
+    return ((size_t)hl * bin_bytes<MODE>() + 15) & ~size_t(15);
 }
 
 template <int MODE>
@@ -192,24 +225,8 @@ __device__ __forceinline__ void load_points(const BatchArgs& a, const CurveDesc&
     }
 }
 
-template <int MODE>
-__device__ __forceinline__ void flush_run(unsigned char* hq, int hlp, int bin, uint32_t sa,
-                                          uint32_t sb, uint32_t sc, double sr, double sw,
-                                          int32_t* flag) {
-    if (MODE == MODE_UNIFORM) {
-        uint32_t* A = reinterpret_cast<uint32_t*>(hq);
-        atomicAdd(A + bin, sa);
-        atomicAdd(A + hlp + bin, sb);
-        atomicAdd(A + 2 * hlp + bin, sc);
-    } else {
-        double* R = reinterpret_cast<double*>(hq);
-        shared_add_f64(R + bin, sr, flag);
-        shared_add_f64(R + hlp + bin, sw, flag);
-    }
-}
-
 template <int MODE, bool TAIL>
-__device__ __forceinline__ void fold_points(const TileShared& s, unsigned char* hist_base,
+__device__ __forceinline__ void fold_points(const TileShared& s, uint32_t hist_s,
                                             const PointRegs<MODE>& p, int pt, int hl,
                                             int32_t* flag) {
     const SegmentDesc& g = s.seg;
@@ -222,11 +239,11 @@ __device__ __forceinline__ void fold_points(const TileShared& s, unsigned char* 
     const bool fast = g.fast_fold != 0;
     const double bin = g.bin_duration;
     const int width = g.width;
-    const int hlp = padded_bins(hl);
+    const uint32_t pbytes = (uint32_t)hist_period_bytes<MODE>(hl);
     for (int q = 0; q < pt; ++q) {
         const double f = s.freq[q];
         const uint32_t S = s.scale[q];
-        unsigned char* hq = hist_base + (size_t)q * hist_period_bytes<MODE>(hl);
+        const uint32_t hq = hist_s + (uint32_t)q * pbytes;
         // 1. the fast fold of all points, straight-line (-1: near an edge, -2: skip)
         int ind[kPts];
         bool miss = false;
@@ -248,51 +265,45 @@ __device__ __forceinline__ void fold_points(const TileShared& s, unsigned char* 
                 }
             }
         }
-        // 3. merge the lane's runs of equal bins, one flush per run
-        int cur = -1;
-        uint32_t sa = 0u, sb = 0u, sc = 0u;
-        double sr = 0.0, sw = 0.0;
+        // 3. accumulate: one record address per point feeds all its atomics
 #pragma unroll
         for (int r = 0; r < kPts; ++r) {
-            const int bi = ind[r];
-            if (bi < 0) continue;
-            if (bi != cur) {
-                if (cur >= 0) flush_run<MODE>(hq, hlp, cur, sa, sb, sc, sr, sw, flag);
-                cur = bi;
-                sa = sb = sc = 0u;
-                sr = sw = 0.0;
-            }
+            if (ind[r] < 0) continue;
+            const uint32_t rec = hq + (uint32_t)ind[r] * (uint32_t)bin_bytes<MODE>();
             if (MODE == MODE_UNIFORM) {
-                sa += p.lo[r];
-                sb += p.hi[r];
-                sc += 1u;
+                red_add_u32<0>(rec, p.lo[r]);
+                red_add_u32<4>(rec, p.hi[r]);
+                red_add_u32<8>(rec, 1u);
             } else {
-                sr += p.rv[r];
-                sw += p.iv[r];
+                shared_add_f64(rec, p.rv[r], flag);
+                shared_add_f64(rec + 8, p.iv[r], flag);
             }
         }
-        if (cur >= 0) flush_run<MODE>(hq, hlp, cur, sa, sb, sc, sr, sw, flag);
     }
 }
 
-// Exact prefix of r_q at bin i from the two 32-bit prefix words.
-__device__ __forceinline__ long long prefix_r(const uint32_t* A, const int32_t* B, int i) {
-    return (long long)B[i] * (1ll << kHalfBits) + (long long)A[i];
+// Exact prefix of r_q at bin i from a UNIFORM record's two prefix words.
+__device__ __forceinline__ long long prefix_r(uint32_t hq, int i) {
+    const uint32_t rec = hq + (uint32_t)i * 12u;
+    return (long long)(int32_t)ld_u32(rec + 4) * (1ll << kHalfBits) + (long long)ld_u32(rec);
+}
+__device__ __forceinline__ uint32_t prefix_c(uint32_t hq, int i) {
+    return ld_u32(hq + (uint32_t)i * 12u + 8u);
 }
 
-// Exact sums of box (n, d) in the reference's units from one period's prefixes.
+// Exact sums of box (n, d) in the reference's units from one period's prefixes
+// (hq: the period's region).
 template <int MODE>
-__device__ __forceinline__ BoxSums box_sums(const uint32_t* A, const int32_t* B, const uint32_t* C,
-                                            const double* R, const double* W,
-                                            const CurveDesc& cv, int n, int d) {
+__device__ __forceinline__ BoxSums box_sums(uint32_t hq, const CurveDesc& cv, int n, int d) {
     BoxSums b;
     if (MODE == MODE_UNIFORM) {
-        b.iv_in = (double)(C[n + d] - C[n]) * cv.w_uniform;
-        b.y_in = ldexp((double)(prefix_r(A, B, n + d) - prefix_r(A, B, n)), -cv.e_r) +
+        b.iv_in = (double)(prefix_c(hq, n + d) - prefix_c(hq, n)) * cv.w_uniform;
+        b.y_in = ldexp((double)(prefix_r(hq, n + d) - prefix_r(hq, n)), -cv.e_r) +
                  cv.ybar * b.iv_in;
     } else {
-        b.iv_in = ldexp(W[n + d] - W[n], -cv.e_i);
-        b.y_in = ldexp(R[n + d] - R[n], -cv.e_r) + cv.ybar * b.iv_in;
+        const uint32_t r1 = hq + (uint32_t)(n + d) * 16u, r0 = hq + (uint32_t)n * 16u;
+        b.iv_in = ldexp(ld_f64(r1 + 8) - ld_f64(r0 + 8), -cv.e_i);
+        b.y_in = ldexp(ld_f64(r1) - ld_f64(r0), -cv.e_r) + cv.ybar * b.iv_in;
     }
     return b;
 }
@@ -346,7 +357,7 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
 
         // ---- 1. fold ---------------------------------------------------------
         const size_t pbytes = hist_period_bytes<MODE>(hl);
-        const int hlp = padded_bins(hl);
+        const uint32_t smem_s = smem_addr(smem);
         {
             const int n16 = (int)((pt * pbytes) / 16);
             uint4* z = reinterpret_cast<uint4*>(smem);
@@ -359,42 +370,39 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
             for (; base + kChunk <= n; base += kChunk) {
                 PointRegs<MODE> p;
                 load_points<MODE, false>(a, s.curve, base, p);
-                fold_points<MODE, false>(s, smem, p, pt, hl, a.error_flag);
+                fold_points<MODE, false>(s, smem_s, p, pt, hl, a.error_flag);
             }
             if (base < n) {
                 PointRegs<MODE> p;
                 load_points<MODE, true>(a, s.curve, base, p);
-                fold_points<MODE, true>(s, smem, p, pt, hl, a.error_flag);
+                fold_points<MODE, true>(s, smem_s, p, pt, hl, a.error_flag);
             }
         }
         __syncthreads();
 
         // ---- 2-3. per period: pad, prefix, sweep, reduce ------------------------
         const size_t hist_bytes = (size_t)pt * pbytes;               // multiple of 16
-        float2* scr = reinterpret_cast<float2*>(smem + hist_bytes);
+        const uint32_t scr_s = smem_s + (uint32_t)hist_bytes;        // FP32 screen copy
         const CurveDesc& cv = s.curve;
         const int obj = a.obj_flag;
         const int e_r = cv.e_r, e_i = cv.e_i;
         const int o = s.seg.oversample;
+        constexpr uint32_t kRec = (uint32_t)bin_bytes<MODE>();
 
         for (int q = 0; q < pt; ++q) {
             const int nb = s.nb[q];
             const int L = nb + 1;
-            unsigned char* hq = smem + (size_t)q * pbytes;
-            uint32_t* A = reinterpret_cast<uint32_t*>(hq);        // UNIFORM words
-            int32_t* B = reinterpret_cast<int32_t*>(A + hlp);
-            uint32_t* C = A + 2 * hlp;
-            double* R = reinterpret_cast<double*>(hq);            // GENERAL sums
-            double* W = R + hlp;
+            const uint32_t hq = smem_s + (uint32_t)(q * pbytes);
             auto copy_bin = [&](int dst, int src) {
                 if (dst >= 0 && dst < s.seg.width && dst < hl && src < hl) {
+                    const uint32_t rd = hq + (uint32_t)dst * kRec, rs = hq + (uint32_t)src * kRec;
                     if (MODE == MODE_UNIFORM) {
-                        A[dst] = A[src];
-                        B[dst] = B[src];
-                        C[dst] = C[src];
+                        st_u32(rd, ld_u32(rs));
+                        st_u32(rd + 4, ld_u32(rs + 4));
+                        st_u32(rd + 8, ld_u32(rs + 8));
                     } else {
-                        R[dst] = R[src];
-                        W[dst] = W[src];
+                        st_f64(rd, ld_f64(rs));
+                        st_f64(rd + 8, ld_f64(rs + 8));
                     }
                 }
             };
@@ -426,13 +434,14 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                 int32_t tb = 0;
                 double tr = 0.0, tw = 0.0;
                 for (int i = lo_i + lane; i < hi_i; i += 32) {
+                    const uint32_t rec = hq + (uint32_t)i * kRec;
                     if (MODE == MODE_UNIFORM) {
-                        ta += A[i];
-                        tb += B[i];
-                        tc += C[i];
+                        ta += ld_u32(rec);
+                        tb += (int32_t)ld_u32(rec + 4);
+                        tc += ld_u32(rec + 8);
                     } else {
-                        tr += R[i];
-                        tw += W[i];
+                        tr += ld_f64(rec);
+                        tw += ld_f64(rec + 8);
                     }
                 }
                 if (MODE == MODE_UNIFORM) {
@@ -469,10 +478,11 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                 for (int g = lo_i; g < hi_i; g += 32) {
                     const int i = g + lane;
                     const bool in = i < hi_i;
+                    const uint32_t rec = hq + (uint32_t)(in ? i : lo_i) * kRec;
                     float tf, wf;
                     if (MODE == MODE_UNIFORM) {
-                        uint32_t va = in ? A[i] : 0u, vc = in ? C[i] : 0u;
-                        int32_t vb = in ? B[i] : 0;
+                        uint32_t va = in ? ld_u32(rec) : 0u, vc = in ? ld_u32(rec + 8) : 0u;
+                        int32_t vb = in ? (int32_t)ld_u32(rec + 4) : 0;
 #pragma unroll
                         for (int k = 1; k < 32; k <<= 1) {
                             const uint32_t xa = __shfl_up_sync(kFull, va, k);
@@ -486,10 +496,11 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                         }
                         const uint32_t pa = oa + va, pc = oc + vc;
                         const int32_t pb = ob + vb;
+                        __syncwarp();
                         if (in) {
-                            A[i] = pa;
-                            B[i] = pb;
-                            C[i] = pc;
+                            st_u32(rec, pa);
+                            st_u32(rec + 4, (uint32_t)pb);
+                            st_u32(rec + 8, pc);
                         }
                         tf = (float)((long long)pb * (1ll << kHalfBits) + (long long)pa);
                         wf = (float)pc;
@@ -497,7 +508,7 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                         ob += __shfl_sync(kFull, vb, 31);
                         oc += __shfl_sync(kFull, vc, 31);
                     } else {
-                        double vr = in ? R[i] : 0.0, vw = in ? W[i] : 0.0;
+                        double vr = in ? ld_f64(rec) : 0.0, vw = in ? ld_f64(rec + 8) : 0.0;
 #pragma unroll
                         for (int k = 1; k < 32; k <<= 1) {
                             const double xr = __shfl_up_sync(kFull, vr, k);
@@ -508,9 +519,10 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                             }
                         }
                         const double cr = orr + vr, cw = ow + vw;
+                        __syncwarp();
                         if (in) {
-                            R[i] = cr;
-                            W[i] = cw;
+                            st_f64(rec, cr);
+                            st_f64(rec + 8, cw);
                         }
                         tf = (float)cr;
                         wf = (float)cw;
@@ -518,7 +530,7 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                         ow += __shfl_sync(kFull, vw, 31);
                     }
                     if (in) {
-                        scr[i] = make_float2(tf, wf);
+                        st_f2(scr_s + (uint32_t)i * 8u, make_float2(tf, wf));
                         tmax = fmaxf(tmax, fabsf(tf));
                     }
                 }
@@ -531,30 +543,28 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
             for (int w = 0; w < kWarps; ++w) tmax = fmaxf(tmax, s.red_t[w]);
 
             auto iv_prefix = [&](int i) -> double {
-                return MODE == MODE_UNIFORM ? (double)C[i] * cv.w_uniform : ldexp(W[i], -e_i);
+                return MODE == MODE_UNIFORM ? (double)prefix_c(hq, i) * cv.w_uniform
+                                            : ldexp(ld_f64(hq + (uint32_t)i * 16u + 8u), -e_i);
             };
             auto exact = [&](int n, int d) -> double {
-                return box_objective(box_sums<MODE>(A, B, C, R, W, cv, n, d), cv, obj);
+                return box_objective(box_sums<MODE>(hq, cv, n, d), cv, obj);
             };
             if (a.debug_prefix != nullptr && q == 0) {   // test hook: this period's prefixes
                 for (int i = tid; i < L; i += kThreads) {
-                    const double r_i = MODE == MODE_UNIFORM ? ldexp((double)prefix_r(A, B, i), -e_r)
-                                                            : ldexp(R[i], -e_r);
+                    const double r_i = MODE == MODE_UNIFORM
+                                           ? ldexp((double)prefix_r(hq, i), -e_r)
+                                           : ldexp(ld_f64(hq + (uint32_t)i * 16u), -e_r);
                     a.debug_prefix[i] = r_i + cv.ybar * iv_prefix(i);
                     a.debug_prefix[hl + i] = iv_prefix(i);
                 }
             }
 
-            // ---- sweep: each lane one start, all durations ------------------------
+            // ---- sweep: durations outer (the reference's order), two starts per lane ----
             const float Et = cv.exact_all ? CUDART_INF_F : tmax * (1.0f / 2097152.0f);  // 2^-21
             const float Wt = MODE == MODE_UNIFORM ? (float)cv.n_points : (float)cv.i_total;
             const float Ei = MODE == MODE_UNIFORM ? 0.0f : Wt * (1.0f / 2097152.0f);
             const float floor_q =
                 MODE == MODE_GENERAL ? (float)ldexp(cv.ivar_floor, e_i) * (1.0f + 1e-3f) : 0.0f;
-            int dmin = 1 << 29;
-            for (int k = 0; k < n_dur; ++k)
-                if (s.dur[k] < nb) dmin = min(dmin, s.dur[k]);
-            const int nmax = nb - dmin;                // largest start of any box
 
             bool has = false, ex_ok = false;
             int bn = 0, bdi = 0;
@@ -597,57 +607,56 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                 }
                 return false;
             };
-
-            for (int n0 = warp * 32; n0 <= nmax; n0 += kThreads) {
-                const int n = n0 + lane;
-                bool upd = false;
-                if (n <= nmax) {
-                    const float2 av = scr[n];
-                    for (int di0 = 0; di0 < n_dur; di0 += 4) {
-                        float tt[4], dl[4], dh[4];
-                        bool cand[4], sv[4];
-                        int dd[4];
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const int d = s.dur[di0 + k];          // padded with kNoBox
-                            const bool inb = (d < nb) & (n + d <= nb);
-                            const float2 bv = scr[inb ? n + d : n];
-                            const float t = bv.x - av.x;
-                            const float iv = bv.y - av.y;        // count, or scaled weight
-                            const float ov = Wt - iv;
-                            float den_lo, den_hi;
-                            bool ok, sure_valid;
-                            if (MODE == MODE_UNIFORM) {
-                                den_lo = obj ? iv * ov * ov : iv * ov;   // > 0 iff valid
-                                den_hi = den_lo;
-                                sure_valid = true;
-                                ok = den_lo > 0.0f;
-                            } else {
-                                const float il = fmaxf(iv - Ei, 0.0f), ol = fmaxf(ov - Ei, 0.0f);
-                                const float ih = iv + Ei, oh = ov + Ei;
-                                den_lo = obj ? il * ol * ol : il * ol;
-                                den_hi = obj ? ih * oh * oh : ih * oh;
-                                sure_valid = (il >= floor_q) & (ol >= floor_q);
-                                // an empty box is exactly 0 in the FP64 prefix
-                                ok = (den_lo > 0.0f) || (inb && W[n + d] != W[n]);
-                            }
-                            const float th = fabsf(t) + Et;
-                            cand[k] = inb & ok & (t <= Et) & !(th * th < thr * den_lo);
-                            tt[k] = t;
-                            dl[k] = den_lo;
-                            dh[k] = den_hi;
-                            sv[k] = sure_valid;
-                            dd[k] = d;
-                        }
-                        if (cand[0] | cand[1] | cand[2] | cand[3]) {
-#pragma unroll
-                            for (int k = 0; k < 4; ++k)
-                                if (cand[k]) upd |= consider(n, di0 + k, dd[k], tt[k], dl[k], dh[k], sv[k]);
-                        }
+            // the screen of box (n, d) from its two screen records
+            auto screen = [&](float2 av, float2 bv, int n, int d, float& t, float& den_lo,
+                              float& den_hi, bool& sure_valid) -> bool {
+                t = bv.x - av.x;
+                const float iv = bv.y - av.y;              // count, or scaled weight
+                const float ov = Wt - iv;
+                bool ok;
+                if (MODE == MODE_UNIFORM) {
+                    den_lo = obj ? iv * ov * ov : iv * ov;  // exact counts: > 0 iff valid
+                    den_hi = den_lo;
+                    sure_valid = true;
+                    ok = den_lo > 0.0f;
+                } else {
+                    const float il = fmaxf(iv - Ei, 0.0f), ol = fmaxf(ov - Ei, 0.0f);
+                    const float ih = iv + Ei, oh = ov + Ei;
+                    den_lo = obj ? il * ol * ol : il * ol;
+                    den_hi = obj ? ih * oh * oh : ih * oh;
+                    sure_valid = (il >= floor_q) & (ol >= floor_q);
+                    ok = den_lo > 0.0f;
+                    if (!ok) {   // an empty box is exactly 0 in the FP64 prefix
+                        ok = ld_f64(hq + (uint32_t)(n + d) * 16u + 8u) !=
+                             ld_f64(hq + (uint32_t)n * 16u + 8u);
                     }
                 }
-                if (__any_sync(kFull, upd))
-                    thr = warp_max(has ? lb * (1.0f - 2.0f * kRel) : -1.0f);
+                const float th = fabsf(t) + Et;
+                return ok & (t <= Et) & !(th * th < thr * den_lo);
+            };
+
+            for (int di = 0; di < n_dur; ++di) {
+                const int d = s.dur[di];
+                if (d >= nb) continue;
+                const int nmax = nb - d;
+                const uint32_t d8 = (uint32_t)d * 8u;
+                for (int n0 = warp * 32; n0 <= nmax; n0 += 2 * kThreads) {
+                    const int n1 = n0 + lane, n2 = n1 + kThreads;
+                    const bool in1 = n1 <= nmax, in2 = n2 <= nmax;
+                    const uint32_t s1 = scr_s + (uint32_t)(in1 ? n1 : 0) * 8u;
+                    const uint32_t s2 = scr_s + (uint32_t)(in2 ? n2 : 0) * 8u;
+                    const float2 a1 = ld_f2(s1), b1 = ld_f2(s1 + d8);
+                    const float2 a2 = ld_f2(s2), b2 = ld_f2(s2 + d8);
+                    float t1, l1, h1, t2, l2, h2;
+                    bool v1, v2;
+                    const bool c1 = in1 && screen(a1, b1, n1, d, t1, l1, h1, v1);
+                    const bool c2 = in2 && screen(a2, b2, n2, d, t2, l2, h2, v2);
+                    bool upd = false;
+                    if (c1) upd |= consider(n1, di, d, t1, l1, h1, v1);
+                    if (c2) upd |= consider(n2, di, d, t2, l2, h2, v2);
+                    if (__any_sync(kFull, upd))
+                        thr = warp_max(has ? lb * (1.0f - 2.0f * kRel) : -1.0f);
+                }
             }
 
             // ---- reduce: lanes whose best may be their warp's maximum -------------
@@ -682,12 +691,7 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
         __syncthreads();
         if (tid < pt) {
             const int q = tid;
-            unsigned char* hq = smem + (size_t)q * pbytes;
-            const uint32_t* A = reinterpret_cast<const uint32_t*>(hq);
-            const int32_t* B = reinterpret_cast<const int32_t*>(A + hlp);
-            const uint32_t* C = A + 2 * hlp;
-            const double* R = reinterpret_cast<const double*>(hq);
-            const double* W = R + hlp;
+            const uint32_t hq = smem_s + (uint32_t)(q * pbytes);
             double* op = out + q;
             if (!(s.win_v[q] > -CUDART_INF)) {
                 op[0] = -CUDART_INF;
@@ -695,7 +699,7 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
             } else {
                 const int vn = s.win_n[q];
                 const int d = s.dur[s.win_di[q]];
-                const BoxSums b = box_sums<MODE>(A, B, C, R, W, cv, vn, d);
+                const BoxSums b = box_sums<MODE>(hq, cv, vn, d);
                 const double iv_out = cv.sum_ivar - b.iv_in;
                 const double yin = b.y_in / b.iv_in;
                 const double yout = (cv.sum_y - b.y_in) / iv_out;

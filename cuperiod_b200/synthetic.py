@@ -1,0 +1,108 @@
+"""Seeded synthetic light curves with the shapes of the BLS benchmark workloads.
+
+No survey data is available offline, so these stand in for it with the stated
+cadences, lengths and value distributions:
+
+* :func:`batched_curves` -- light curves of N ~ U[500, 20000] points over a 27 d
+  baseline at 2-minute cadence with a 1 d gap in the middle and 5% random
+  dropouts; flux 1 + N(0, sigma), sigma log-uniform in [2e-4, 5e-3]; half of
+  them carry box transits (depth log-uniform [1e-4, 1e-2], period log-uniform
+  [0.5, 13] d, duration U[0.02, 0.25] d); unit errors.  Searched over 50,000
+  log-spaced periods in [0.3, 13] d with the default 8 durations per segment.
+* :func:`single_curve` -- 2000 points uniform over 90 d, a 2e-3 transit at 3.7 d
+  lasting 0.1 d, 1e-3 noise, unit errors; 10,000 log periods in [0.5, 30] d with
+  durations {0.05, 0.08, 0.12, 0.16, 0.2} d and the likelihood objective.
+* :func:`long_baseline_curves` -- 60,000 points at 30-minute cadence over four
+  years with times offset by ~1.4e3 d, depths down to 5e-5; 200,000 log periods
+  in [0.5, 400] d with 12 durations per segment.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class Curve:
+    t: np.ndarray
+    y: np.ndarray
+    dy: np.ndarray | None
+    transit: tuple[float, float, float] | None     # (period, duration, depth)
+
+
+def _box(t, rng, period, duration, depth, y):
+    t0 = rng.uniform(0.0, period)
+    y[np.mod(t - t0, period) < duration] -= depth
+
+
+def batched_curves(n_curves: int, *, seed: int = 0, n_range=(500, 20000)) -> list[Curve]:
+    """The batched workload's light curves (see the module docstring)."""
+    rng = np.random.default_rng(seed)
+    cadence = 2.0 / 1440.0
+    base = np.arange(0.0, 27.0, cadence)
+    base = base[(base < 13.0) | (base >= 14.0)]            # 1 d mid-baseline gap
+    out = []
+    for _ in range(n_curves):
+        keep = base[rng.random(base.size) > 0.05]          # 5% dropouts
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        if keep.size > n:
+            keep = np.sort(rng.choice(keep, n, replace=False))
+        sigma = 10.0 ** rng.uniform(np.log10(2e-4), np.log10(5e-3))
+        y = 1.0 + rng.normal(0.0, sigma, keep.size)
+        transit = None
+        if rng.random() < 0.5:
+            period = 10.0 ** rng.uniform(np.log10(0.5), np.log10(13.0))
+            duration = rng.uniform(0.02, 0.25)
+            depth = 10.0 ** rng.uniform(-4.0, -2.0)
+            _box(keep, rng, period, duration, depth, y)
+            transit = (period, duration, depth)
+        out.append(Curve(keep + 2460000.0, y, None, transit))
+    return out
+
+
+def batched_periods() -> np.ndarray:
+    """50,000 log-spaced trial periods over [0.3, 13] d."""
+    return np.geomspace(0.3, 13.0, 50000)
+
+
+def single_curve(seed: int = 0) -> Curve:
+    """The single-curve workload's light curve."""
+    rng = np.random.default_rng(seed)
+    n = 2000
+    t = np.sort(rng.uniform(0.0, 90.0, n))
+    y = 1.0 + rng.normal(0.0, 1e-3, n)
+    t0 = rng.uniform(0.0, 1.0) * 3.7
+    y[np.mod(t - t0, 3.7) < 0.1] -= 2e-3
+    return Curve(t, y, np.ones(n), (3.7, 0.1, 2e-3))
+
+
+SINGLE_PERIODS = (0.5, 30.0, 10000)
+SINGLE_DURATIONS = (0.05, 0.08, 0.12, 0.16, 0.2)
+
+
+def long_baseline_curves(n_curves: int, *, seed: int = 0) -> list[Curve]:
+    """The long-baseline precision workload's light curves."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(60000) * (30.0 / 1440.0)                 # 30-min cadence, 1250 d
+    t = t * (1461.0 / t[-1]) + 1400.0                      # four years, offset ~1.4e3 d
+    out = []
+    for _ in range(n_curves):
+        sigma = 10.0 ** rng.uniform(np.log10(2e-4), np.log10(5e-3))
+        y = (1.0 + rng.normal(0.0, sigma, t.size)).astype(np.float32).astype(np.float64)
+        period = 10.0 ** rng.uniform(np.log10(0.5), np.log10(400.0))
+        duration = rng.uniform(0.02, 0.25)
+        depth = 10.0 ** rng.uniform(np.log10(5e-5), -2.0)
+        _box(t, rng, period, duration, depth, y)
+        out.append(Curve(t.copy(), y, None, (period, duration, depth)))
+    return out
+
+
+def long_baseline_periods() -> np.ndarray:
+    """200,000 log-spaced trial periods over [0.5, 400] d."""
+    return np.geomspace(0.5, 400.0, 200000)
+
+
+__all__ = ["Curve", "batched_curves", "batched_periods", "long_baseline_curves",
+           "long_baseline_periods", "single_curve"]
