@@ -43,6 +43,11 @@ METRIC = "BLS light curves/s on 1 B200: plain vs learned-pruned at ≥99% same-b
 UNIT = "light curves/s"
 WORKLOAD = ("batched plain full-grid BLS: 4096 curves, N~U[500,20000], 27 d at 2-min cadence, "
             "50,000 log periods 0.3-13 d, 8 durations/segment, snr objective")
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one search launch
+# over the first 256 curves of this workload, from one ncu capture
+# (profiles/bls_search_kernel_launches_256curves.txt); a launch's traffic grows in
+# proportion to its curves (points in, 7 fields x periods out)
+TRAFFIC_256 = 69360640 + 680540928
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -203,8 +208,12 @@ def run_ours(args) -> None:
 
     curves, segments, grid, packed = workload(args.curves, args.seed + rank)
     engine = _lib.Engine(device=local)
-    stream = torch.cuda.current_stream()
+    # a stream of our own: the C ABI reads a NULL stream as "the engine's stream",
+    # so torch's legacy default stream (handle 0) would leave the events unordered
+    # with the launches
+    stream = torch.cuda.Stream(device=local)
     handle = stream.cuda_stream
+    assert handle != 0
     engine.prepare(grid, packed, stream=handle)
     info = engine.info()
     for _ in range(args.warmup):
@@ -268,6 +277,9 @@ def run_ours(args) -> None:
         t_fp64 = info["folds"] * 2 / (108.0 * n_sm * f_clk)
         t_fp32 = info["boxes"] * 10 / (188.0 * n_sm * f_clk)
         t_pipe = max(t_atom, t_fp64, t_fp32)
+        # one search launch per accumulation mode present (one weight per curve,
+        # per-point weights) and one counter reset per step
+        n_modes = int(info["uniform_curves"] > 0) + int(info["uniform_curves"] < info["n_curves"])
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -280,7 +292,8 @@ def run_ours(args) -> None:
                        "boxes_per_step": info["boxes"] * world,
                        "trials_per_s": info["trials"] * world / (ms_per_step / 1000.0)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None,
+                         "frac": achieved / hbm,
+                         "traffic": TRAFFIC_256 * args.curves / 256.0,
                          "peak_source": hbm_src,
                          "note": "the search is SM-bound (shared atomics, FP64/FP32 pipes); "
                                  "see sm_roofline"},
@@ -289,7 +302,7 @@ def run_ours(args) -> None:
                             "model_ms": 1000.0 * t_pipe, "kernel_ms": kernel_ms,
                             "frac": 1000.0 * t_pipe / kernel_ms},
             "clocks": clocks,
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * n_modes,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": info["h2d_bytes"],
                     "d2h_bytes_per_step": 32 * args.curves},
         }

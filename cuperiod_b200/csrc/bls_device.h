@@ -78,10 +78,18 @@ struct WorkItem {
     int32_t p_count;        // periods in the tile (<= kMaxTile)
 };
 
+// The work of one launch is regular: every curve of one accumulation mode is cut
+// into the same tiles (segment s: ceil(n_periods / seg_cap[s]) tiles), so work
+// index i is curve order[i / tiles_per_curve] and tile i % tiles_per_curve of
+// that curve, located by a search of the per-segment tile prefix.
 struct BatchArgs {
     const CurveDesc* curves;
     const SegmentDesc* segments;
-    const WorkItem* items;
+    const int32_t* order;       // this mode's curves, most points first
+    const int32_t* seg_tiles;   // n_segments + 1: prefix of tiles per curve
+    const int32_t* seg_cap;     // n_segments: periods per tile
+    int32_t tiles_per_curve;
+    int32_t n_segments;
     const double* tau;          // per point: t - t_min (FP64)
     const uint32_t* pay_r;      // per point: r_q as low 13 bits | signed high part << 16
     const double* r64;          // GENERAL: (y*ivar - ybar*ivar) * 2^e_r per point

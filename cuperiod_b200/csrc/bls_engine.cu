@@ -553,53 +553,60 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
                     "BLS: %zu bytes of shared memory per period exceed the device's %zu; "
                     "narrow the period range (max_period_days)",
                     smem, e->smem_optin);
-    struct ItemCost {
-        WorkItem w;
-        double cost;
-        int mode;
-    };
-    std::vector<ItemCost> items;
-    double folds = 0.0, boxes = 0.0, trials = 0.0;
-    for (int c = 0; c < nc; ++c) {
-        const int m = curves[c].d.mode;
-        for (int s = 0; s < ns; ++s) {
-            const SegmentHost& sh = segs[s];
-            if (sh.empty_periods) continue;
-            const int hl = sh.d.hist_len;
-            const int cap = tile_cap(m, hl, smem, e->tune.max_tile);
-            if (cap < 1) return fail(BLS_E_RESOURCE, "segment %d does not fit shared memory", s);
-            double box_per_period = 0.0;
-            for (int32_t k : sh.dur) box_per_period += std::max(0, hl - k);
-            for (int32_t p = 0; p < sh.d.n_periods; p += cap) {
-                ItemCost it;
-                it.w.curve = c;
-                it.w.segment = s;
-                it.w.p_begin = p;
-                it.w.p_count = std::min(cap, sh.d.n_periods - p);
-                it.mode = m;
-                it.cost = it.w.p_count * ((double)curves[c].d.n_points + 1.2 * box_per_period);
-                items.push_back(it);
-            }
-            const int64_t p0 = sh.d.period_off;
-            for (int32_t p = 0; p < sh.d.n_periods; ++p) {
-                const int nb = pc[p0 + p].nb;
-                for (int32_t k : sh.dur)
-                    if (k < nb) boxes += (double)(nb - k + 1);
-            }
-            folds += (double)curves[c].d.n_points * sh.d.n_periods;
-            trials += (double)sh.d.n_periods * sh.dur.size();
+    // per segment: boxes of one curve (the same for every curve)
+    double seg_box_sum = 0.0, trials_per_curve = 0.0;
+    for (int s = 0; s < ns; ++s) {
+        const SegmentHost& sh = segs[s];
+        if (sh.empty_periods) continue;
+        const int64_t p0 = sh.d.period_off;
+        for (int32_t p = 0; p < sh.d.n_periods; ++p) {
+            const int nb = pc[p0 + p].nb;
+            for (int32_t k : sh.dur)
+                if (k < nb) seg_box_sum += (double)(nb - k + 1);
         }
+        trials_per_curve += (double)sh.d.n_periods * sh.dur.size();
     }
-    std::stable_sort(items.begin(), items.end(), [](const ItemCost& a, const ItemCost& b) {
-        if (a.mode != b.mode) return a.mode < b.mode;
-        return a.cost > b.cost;
-    });
+    // per mode: tiles of each segment, their prefix, and the curves largest first
+    // (so the last work items of a launch are the cheapest)
+    std::vector<int32_t> plan_tiles[2], plan_cap[2], plan_order[2];
+    int64_t n_items_mode[2] = {0, 0};
+    for (int m = 0; m < 2; ++m) {
+        plan_tiles[m].assign(ns + 1, 0);
+        plan_cap[m].assign(std::max(ns, 1), 1);
+        if (!modes[m]) continue;
+        int64_t acc = 0;
+        for (int s = 0; s < ns; ++s) {
+            plan_tiles[m][s] = (int32_t)acc;
+            if (segs[s].empty_periods) continue;
+            const int cap = tile_cap(m, segs[s].d.hist_len, smem, e->tune.max_tile);
+            if (cap < 1) return fail(BLS_E_RESOURCE, "segment %d does not fit shared memory", s);
+            plan_cap[m][s] = cap;
+            acc += (segs[s].d.n_periods + cap - 1) / cap;
+            if (acc > INT32_MAX) return fail(BLS_E_RESOURCE, "too many period tiles per curve");
+        }
+        plan_tiles[m][ns] = (int32_t)acc;
+        for (int c = 0; c < nc; ++c)
+            if (curves[c].d.mode == m) plan_order[m].push_back(c);
+        std::stable_sort(plan_order[m].begin(), plan_order[m].end(), [&](int x, int y) {
+            return curves[x].d.n_points > curves[y].d.n_points;
+        });
+        n_items_mode[m] = acc * (int64_t)plan_order[m].size();
+        if (n_items_mode[m] > INT32_MAX)
+            return fail(BLS_E_RESOURCE,
+                        "%lld work items exceed one launch; split the batch into fewer curves",
+                        (long long)n_items_mode[m]);
+    }
+    const double folds = (double)n_pts * (double)P_total;   // each point, each period
+    const double boxes = seg_box_sum * nc;
+    const double trials = trials_per_curve * nc;
 
     // ---- stage metadata and upload ---------------------------------------------
-    const size_t n_items = items.size();
+    const int64_t n_items = n_items_mode[0] + n_items_mode[1];
     const size_t grid_bytes = (size_t)P_total * (8 + 8 + 4 + 4) + dur_all.size() * 4 + 64;
+    // descriptors, then per mode: order (nc in all), seg_tiles (ns + 1), seg_cap (ns)
+    const size_t plan_words = (size_t)nc + 2 * (size_t)(ns + 1) + 2 * (size_t)std::max(ns, 1);
     const size_t meta_bytes = sizeof(CurveDesc) * nc + sizeof(SegmentDesc) * std::max(ns, 1) +
-                              sizeof(WorkItem) * std::max<size_t>(n_items, 1) + 64;
+                              sizeof(int32_t) * plan_words + 64;
     if ((rc = e->h_grid.ensure(grid_bytes))) return rc;
     if ((rc = e->h_meta.ensure(meta_bytes))) return rc;
     char* gp = e->h_grid.as<char>();
@@ -618,14 +625,28 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     char* mp = e->h_meta.as<char>();
     CurveDesc* hcur = reinterpret_cast<CurveDesc*>(mp);
     SegmentDesc* hseg = reinterpret_cast<SegmentDesc*>(hcur + nc);
-    WorkItem* hitem = reinterpret_cast<WorkItem*>(hseg + std::max(ns, 1));
+    int32_t* hplan = reinterpret_cast<int32_t*>(hseg + std::max(ns, 1));
     for (int c = 0; c < nc; ++c) hcur[c] = curves[c].d;
     for (int s = 0; s < ns; ++s) hseg[s] = segs[s].d;
-    e->n_items_mode[0] = e->n_items_mode[1] = 0;
-    for (size_t i = 0; i < n_items; ++i) {
-        hitem[i] = items[i].w;
-        e->n_items_mode[items[i].mode]++;
+    size_t plan_off[2][3];          // per mode: order, seg_tiles, seg_cap (in words)
+    {
+        size_t w = 0;
+        for (int m = 0; m < 2; ++m) {
+            plan_off[m][0] = w;
+            std::copy(plan_order[m].begin(), plan_order[m].end(), hplan + w);
+            w += plan_order[m].size();
+        }
+        for (int m = 0; m < 2; ++m) {
+            plan_off[m][1] = w;
+            std::copy(plan_tiles[m].begin(), plan_tiles[m].end(), hplan + w);
+            w += ns + 1;
+            plan_off[m][2] = w;
+            std::copy(plan_cap[m].begin(), plan_cap[m].end(), hplan + w);
+            w += std::max(ns, 1);
+        }
     }
+    e->n_items_mode[0] = (int32_t)n_items_mode[0];
+    e->n_items_mode[1] = (int32_t)n_items_mode[1];
 
     const size_t out_elems = (size_t)kFields * nc * std::max<int64_t>(P_total, 1);
     if ((rc = e->d_tau.ensure(sizeof(double) * std::max<int64_t>(n_pts, 1)))) return rc;
@@ -669,14 +690,18 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     const char* dmp = e->d_curves.as<char>();
     const CurveDesc* dcur = reinterpret_cast<const CurveDesc*>(dmp);
     const SegmentDesc* dseg = reinterpret_cast<const SegmentDesc*>(dcur + nc);
-    const WorkItem* ditem = reinterpret_cast<const WorkItem*>(dseg + std::max(ns, 1));
+    const int32_t* dplan = reinterpret_cast<const int32_t*>(dseg + std::max(ns, 1));
     int32_t* ctl = e->d_ctl.as<int32_t>();
     int ctas_total = 0;
     for (int m = 0; m < 2; ++m) {
         BatchArgs& a = e->args[m];
         a.curves = dcur;
         a.segments = dseg;
-        a.items = ditem + (m == 0 ? 0 : e->n_items_mode[0]);
+        a.order = dplan + plan_off[m][0];
+        a.seg_tiles = dplan + plan_off[m][1];
+        a.seg_cap = dplan + plan_off[m][2];
+        a.tiles_per_curve = plan_tiles[m][ns];
+        a.n_segments = ns;
         a.n_items = e->n_items_mode[m];
         a.tau = e->d_tau.as<double>();
         a.pay_r = e->d_pay_r.as<uint32_t>();

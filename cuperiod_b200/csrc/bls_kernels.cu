@@ -323,9 +323,23 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
         const int it = s.next;
         if (it >= a.n_items) break;
         if (tid == 0) {
-            s.item = a.items[it];
-            s.curve = a.curves[s.item.curve];
-            s.seg = a.segments[s.item.segment];
+            const int r = it / a.tiles_per_curve;
+            const int j = it - r * a.tiles_per_curve;
+            int lo = 0, hi = a.n_segments;          // seg_tiles[lo] <= j < seg_tiles[hi]
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (__ldg(a.seg_tiles + mid) <= j) lo = mid;
+                else hi = mid;
+            }
+            const int cap = __ldg(a.seg_cap + lo);
+            s.seg = a.segments[lo];
+            WorkItem w;
+            w.curve = __ldg(a.order + r);
+            w.segment = lo;
+            w.p_begin = (j - __ldg(a.seg_tiles + lo)) * cap;
+            w.p_count = min(cap, s.seg.n_periods - w.p_begin);
+            s.item = w;
+            s.curve = a.curves[w.curve];
         }
         __syncthreads();
         const int pt = s.item.p_count;
