@@ -77,6 +77,7 @@ def load() -> ctypes.CDLL:
         lib.bls_download.argtypes = [_vp, _vp, _vp]
         lib.bls_device_output.argtypes = [_vp, P(_vp)]
         lib.bls_download_best.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
+        lib.bls_launch_best_noalloc.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
         lib.bls_search.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_batch_info.argtypes = [_vp, P(BlsBatchInfo)]
         lib.bls_debug_fold_bins.argtypes = [_vp, _vp, _i64, _dbl, _dbl, _i32, _vp, _vp]
@@ -84,7 +85,8 @@ def load() -> ctypes.CDLL:
                                          _vp]
         for name in ("bls_engine_create", "bls_engine_destroy", "bls_prepare", "bls_launch",
                      "bls_download", "bls_device_output", "bls_download_best", "bls_search",
-                     "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix"):
+                     "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix",
+                     "bls_launch_best_noalloc"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib
@@ -226,6 +228,18 @@ class Engine:
         val, mean, std = (np.empty(n, dtype=np.float64) for _ in range(3))
         _check(self._lib.bls_download_best(self._h, idx.ctypes.data, val.ctypes.data,
                                            mean.ctypes.data, std.ctypes.data, stream))
+        return idx, val, mean, std
+
+    def launch_best_noalloc(self, stream: int | None = None):
+        """Search the prepared batch and return its per-curve best, allocating
+        nothing (scratch in the library's static device array; at most 65,536
+        curves; overlapping calls on one device race)."""
+        assert self._curves is not None
+        n = self._curves.n_curves
+        idx = np.empty(n, dtype=np.int64)
+        val, mean, std = (np.empty(n, dtype=np.float64) for _ in range(3))
+        _check(self._lib.bls_launch_best_noalloc(self._h, idx.ctypes.data, val.ctypes.data,
+                                                 mean.ctypes.data, std.ctypes.data, stream))
         return idx, val, mean, std
 
     def device_output(self) -> int:

@@ -890,6 +890,53 @@ int bls_download_best(BlsEngine* e, int64_t* best_index, double* best_power, dou
     return BLS_OK;
 }
 
+int bls_launch_best_noalloc(BlsEngine* e, int64_t* best_index, double* best_power,
+                            double* power_mean, double* power_std, void* stream) {
+    if (!e || !best_index || !best_power || !power_mean || !power_std)
+        return fail(BLS_E_INVALID, "engine and outputs are required");
+    if (!e->prepared) return fail(BLS_E_STATE, "bls_launch_best_noalloc before bls_prepare");
+    const int nc = e->n_curves;
+    if (nc > kStaticMaxCurves)
+        return fail(BLS_E_INVALID,
+                    "bls_launch_best_noalloc: %d curves exceed its static scratch of %d curves; "
+                    "split the batch, or use bls_launch and bls_download_best",
+                    nc, kStaticMaxCurves);
+    CUDA_TRY(cudaSetDevice(e->device), "select device");
+    cudaStream_t st = pick(e, stream);
+    void* scr = nullptr;
+    CUDA_TRY(static_scratch_address(e->device, &scr), "static scratch address");
+    int32_t* ctl = static_cast<int32_t*>(scr);
+    CUDA_TRY(cudaMemsetAsync(ctl, 0, 64, st), "reset work counters and error flag");
+    for (int m = 0; m < 2; ++m) {
+        if (e->args[m].n_items <= 0) continue;
+        BatchArgs a = e->args[m];
+        a.work_counter = ctl + m;
+        a.error_flag = ctl + 8;
+        CUDA_TRY(launch_search(a, m, e->ctas_mode[m], e->smem, st), "search launch");
+    }
+    int64_t* di = reinterpret_cast<int64_t*>(static_cast<char*>(scr) + kStaticResultsOffset);
+    double* dv = reinterpret_cast<double*>(di + kStaticMaxCurves);
+    double* dmean = dv + kStaticMaxCurves;
+    double* dstd = dmean + kStaticMaxCurves;
+    CUDA_TRY(launch_best(e->d_out.as<double>(), nc, e->n_periods, di, dv, dmean, dstd, st),
+             "best-of-spectrum launch");
+    // copies into the caller's (pageable) arrays complete before they return
+    int32_t flag = 0;
+    CUDA_TRY(cudaMemcpyAsync(best_index, di, sizeof(int64_t) * nc, cudaMemcpyDeviceToHost, st),
+             "download best index");
+    CUDA_TRY(cudaMemcpyAsync(best_power, dv, sizeof(double) * nc, cudaMemcpyDeviceToHost, st),
+             "download best power");
+    CUDA_TRY(cudaMemcpyAsync(power_mean, dmean, sizeof(double) * nc, cudaMemcpyDeviceToHost, st),
+             "download power mean");
+    CUDA_TRY(cudaMemcpyAsync(power_std, dstd, sizeof(double) * nc, cudaMemcpyDeviceToHost, st),
+             "download power std");
+    CUDA_TRY(cudaMemcpyAsync(&flag, ctl + 8, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
+             "read error flag");
+    CUDA_TRY(cudaStreamSynchronize(st), "synchronize");
+    if (flag != 0) return fail(BLS_E_DEVICE, "a kernel met an impossible work descriptor");
+    return BLS_OK;
+}
+
 int bls_search(BlsEngine* e, const BlsGrid* grid, const BlsCurves* curves, double* out,
                void* stream) {
     int rc;

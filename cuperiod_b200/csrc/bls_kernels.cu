@@ -31,6 +31,8 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "bls_device.h"
 #include "bls_launch.h"
 
@@ -843,6 +845,25 @@ cudaError_t launch_fold_bins(const double* tau, int n, double P, double f, uint3
     fold_bins_kernel<<<(n + 255) / 256, 256, 0, stream>>>(tau, n, P, f, S, bin, width, fb, mu,
                                                           mphi, fast, out, used_fast);
     return cudaGetLastError();
+}
+
+// 2 MiB + 256 B per device, in the library's module (no allocation at run time).
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+cudaError_t static_scratch_address(int device, void** ptr) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static void* addr[kMaxDevices] = {};
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) return e;
+        addr[device] = p;
+    }
+    *ptr = addr[device];
+    return cudaSuccess;
 }
 
 int search_threads() { return kThreads; }

@@ -25,6 +25,20 @@ cudaError_t launch_fold_bins(const double* tau, int n, double P, double f, uint3
 cudaError_t launch_best(const double* power, int n_curves, int64_t n_periods, int64_t* best_index,
                         double* best_power, double* mean, double* sd, cudaStream_t stream);
 
+// Scratch of the allocation-free search (bls_launch_best_noalloc): one
+// file-scope device array per device.  Bytes [0, 64): the work counters of the
+// two accumulation modes (words 0 and 1) and the error flag (word 8), which
+// must all be zero when a search starts.  From byte 256: per curve the best
+// index (int64), then best power, power mean and power standard deviation
+// (double), kStaticMaxCurves entries each, written in full by best_kernel.
+constexpr int kStaticMaxCurves = 65536;
+constexpr size_t kStaticResultsOffset = 256;
+constexpr size_t kStaticScratchBytes = kStaticResultsOffset + (size_t)kStaticMaxCurves * 32;
+
+// Device address of that array on `device`, which must be the current device.
+// Looked up once per device (cudaGetSymbolAddress) and cached.
+cudaError_t static_scratch_address(int device, void** ptr);
+
 // Bytes of one period's histogram in the kernel's layout.
 size_t period_hist_bytes(int mode, int hl);
 

@@ -134,6 +134,24 @@ int bls_device_output(BlsEngine* engine, const double** out);
 int bls_download_best(BlsEngine* engine, int64_t* best_index, double* best_power,
                       double* power_mean, double* power_std, void* stream);
 
+/* No counterpart in the reference.  bls_launch followed by bls_download_best,
+ * for callers that must not allocate once their batch is prepared: a service
+ * whose device memory is committed to other work, or whose latency cannot absorb
+ * the device synchronisation of cudaMalloc/cudaFree, and callers whose memory
+ * is handed out by another framework's pool.  The call allocates nothing --
+ * no device or pinned memory, no graph: the search's work counters and error
+ * flag and the per-curve results live in a static device array of this library
+ * (2 MiB + 256 B per device); the counters and flag are zeroed by the call
+ * before the search starts.  Limits: at most 65,536 curves in the prepared
+ * batch (larger batches are refused with BLS_E_INVALID); calls that overlap in
+ * time on one device (from several threads, streams or engines) share that
+ * array and race -- serialise them.  The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress, which may load the module), so make it
+ * outside any stream capture.  Results as bls_download_best; waits for the
+ * stream. */
+int bls_launch_best_noalloc(BlsEngine* engine, int64_t* best_index, double* best_power,
+                            double* power_mean, double* power_std, void* stream);
+
 /* prepare + launch + download in one call. */
 int bls_search(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* curves, double* out,
                void* stream);
