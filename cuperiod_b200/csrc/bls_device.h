@@ -38,6 +38,11 @@ constexpr int kChunkThreads = 256;
 constexpr int kChunkPts = 8;
 constexpr int kChunk = kChunkThreads * kChunkPts;
 
+// The box sweep reads the FP32 screen records of starts up to 2 x kChunkThreads
+// + 31 past the last admissible start; that many records after a period's last
+// bin hold a sentinel that fails every screen, so the sweep needs no bounds test.
+constexpr int kScreenPad = 2 * kChunkThreads + 32;
+
 struct SegmentDesc {
     int64_t period_off;     // first period of this segment in the grid arrays
     int32_t n_periods;

@@ -385,7 +385,7 @@ void parallel_for(int n, F&& fn) {
 
 constexpr size_t kDefaultSmem = 108 * 1024;     // two CTAs per SM with the static state
 
-size_t screen_bytes(int /*mode*/, int hl) { return (size_t)hl * 8; }
+size_t screen_bytes(int /*mode*/, int hl) { return ((size_t)hl + kScreenPad) * 8; }
 size_t period_bytes(int mode, int hl) { return period_hist_bytes(mode, hl); }
 
 int tile_cap(int mode, int hl, size_t smem, int max_tile) {

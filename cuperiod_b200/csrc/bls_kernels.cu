@@ -55,7 +55,7 @@ struct TileShared {
     double freq[kMaxTile];
     uint32_t scale[kMaxTile];
     int32_t nb[kMaxTile];
-    int32_t dur[kMaxDur + 4];       // padded with kNoBox for groups of four
+    alignas(16) int32_t dur[kMaxDur + 4];   // padded with kNoBox; read four at a time
     double win_v[kMaxTile];         // per period of the tile: the best box
     int32_t win_di[kMaxTile];
     int32_t win_n[kMaxTile];
@@ -70,6 +70,7 @@ struct TileShared {
     int red_di[kWarps];
     int red_n[kWarps];
     int next;
+    uint32_t thr_bits;              // the sweep's shared threshold (bits of a float >= 0)
 };
 
 // The reference's IEEE fold (no contraction): the fallback of the fast path.
@@ -123,6 +124,12 @@ __device__ __forceinline__ void st_f64(uint32_t a, double v) {
 __device__ __forceinline__ float2 ld_f2(uint32_t a) {
     float2 v;
     asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+    return v;
+}
+template <int OFF>
+__device__ __forceinline__ float2 ld_f2_off(uint32_t a) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2+%3];" : "=f"(v.x), "=f"(v.y) : "r"(a), "n"(OFF));
     return v;
 }
 __device__ __forceinline__ void st_f2(uint32_t a, float2 v) {
@@ -296,6 +303,17 @@ __device__ __forceinline__ uint32_t prefix_c(uint32_t hq, int i) {
 // Exact sums of box (n, d) in the reference's units from one period's prefixes
 // (hq: the period's region).
 template <int MODE>
+__device__ __forceinline__ BoxSums box_sums(uint32_t hq, const CurveDesc& cv, int n, int d);
+
+// The reference's objective of box (n, d), out of line: the sweep reaches it
+// rarely and keeps its own loop small.
+template <int MODE>
+__device__ __noinline__ double exact_objective(uint32_t hq, const CurveDesc* cv, int n, int d,
+                                               int obj) {
+    return box_objective(box_sums<MODE>(hq, *cv, n, d), *cv, obj);
+}
+
+template <int MODE>
 __device__ __forceinline__ BoxSums box_sums(uint32_t hq, const CurveDesc& cv, int n, int d) {
     BoxSums b;
     if (MODE == MODE_UNIFORM) {
@@ -310,7 +328,7 @@ __device__ __forceinline__ BoxSums box_sums(uint32_t hq, const CurveDesc& cv, in
     return b;
 }
 
-template <int MODE>
+template <int MODE, int OBJ>
 __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ TileShared s;
@@ -400,7 +418,7 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
         const size_t hist_bytes = (size_t)pt * pbytes;               // multiple of 16
         const uint32_t scr_s = smem_s + (uint32_t)hist_bytes;        // FP32 screen copy
         const CurveDesc& cv = s.curve;
-        const int obj = a.obj_flag;
+        constexpr int obj = OBJ;          // 0 snr, 1 log-likelihood
         const int e_r = cv.e_r, e_i = cv.e_i;
         const int o = s.seg.oversample;
         constexpr uint32_t kRec = (uint32_t)bin_bytes<MODE>();
@@ -437,6 +455,7 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
             // prefix scan, pass 1: per-warp totals of each contiguous range
             const int E = ((L + kWarps * 32 - 1) / (kWarps * 32)) * 32;
             const int lo_i = warp * E;
+            if (tid == 0) s.thr_bits = 0u;      // every warp left the last sweep
             const int hi_i = min(L, lo_i + E);
             if (!overlap) {
                 for (int k = lane; k < o; k += 32) {
@@ -553,6 +572,9 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                 tmax = warp_max(tmax);
                 if (lane == 0) s.red_t[warp] = tmax;
             }
+            // sentinel records past the last bin: t = NaN fails every screen
+            for (int i = L + tid; i < L + kScreenPad; i += kThreads)
+                st_f2(scr_s + (uint32_t)i * 8u, make_float2(CUDART_NAN_F, 0.0f));
             __syncthreads();
             tmax = 0.0f;
 #pragma unroll
@@ -563,7 +585,7 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                                             : ldexp(ld_f64(hq + (uint32_t)i * 16u + 8u), -e_i);
             };
             auto exact = [&](int n, int d) -> double {
-                return box_objective(box_sums<MODE>(hq, cv, n, d), cv, obj);
+                return exact_objective<MODE>(hq, &cv, n, d, obj);
             };
             if (a.debug_prefix != nullptr && q == 0) {   // test hook: this period's prefixes
                 for (int i = tid; i < L; i += kThreads) {
@@ -586,7 +608,8 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
             int bn = 0, bdi = 0;
             float lb = -1.0f, hb = -1.0f;
             double ex_v = -CUDART_INF;
-            float thr = -1.0f;
+            float thr = 0.0f;
+            const uint32_t thr_s = smem_addr(&s.thr_bits);
 
             // one box that passed the screen: keep it if it may be this lane's best
             auto consider = [&](int n, int di, int d, float t, float den_lo, float den_hi,
@@ -642,7 +665,9 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                     den_hi = obj ? ih * oh * oh : ih * oh;
                     sure_valid = (il >= floor_q) & (ol >= floor_q);
                     ok = den_lo > 0.0f;
-                    if (!ok) {   // an empty box is exactly 0 in the FP64 prefix
+                    // an empty box is exactly 0 in the FP64 prefix; t <= Et also
+                    // keeps sentinel boxes (t = NaN) away from these loads
+                    if (!ok && t <= Et) {
                         ok = ld_f64(hq + (uint32_t)(n + d) * 16u + 8u) !=
                              ld_f64(hq + (uint32_t)n * 16u + 8u);
                     }
@@ -651,55 +676,190 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                 return ok & (t <= Et) & !(th * th < thr * den_lo);
             };
 
+            // Pilot: the lower key bounds of the warp's first chunk of the first
+            // admissible duration set the screen's threshold before any box is
+            // kept.  Each such box passes the screen again in the sweep below
+            // (its upper bound is at least its lower bound), so its lane keeps it
+            // or something better, and every box discarded against this
+            // threshold is worse than a box that is kept.  Without it a warp's
+            // first chunk of every period would pass the screen whole.
+            {
+                int dp = 0;
+                while (dp < n_dur && s.dur[dp] >= nb) ++dp;
+                if (dp < n_dur) {
+                    const int d = s.dur[dp];
+                    const int nmax = nb - d;
+                    float kbest = -1.0f;
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        const int n = warp * 32 + lane + c * kThreads;
+                        if (n <= nmax) {
+                            const uint32_t sa = scr_s + (uint32_t)n * 8u;
+                            float t, den_lo, den_hi;
+                            bool sure_valid;
+                            // thr is still -1 here: the screen checks admissibility only
+                            const bool ok = screen(ld_f2(sa), ld_f2(sa + (uint32_t)d * 8u), n, d, t,
+                                                   den_lo, den_hi, sure_valid);
+                            const float tl = fmaxf(fabsf(t) - Et, 0.0f);
+                            const float klo = __fdividef(tl * tl, den_hi) * (1.0f - kRel);
+                            if (ok & (t < -Et) & sure_valid & (den_lo > 0.0f) & (klo > 0.0f) &
+                                (klo < CUDART_INF_F))
+                                kbest = fmaxf(kbest, klo);
+                        }
+                    }
+                    kbest = warp_max(kbest);
+                    if (kbest > 0.0f) {
+                        thr = kbest * (1.0f - 2.0f * kRel);
+                        if (lane == 0) atomicMax(&s.thr_bits, __float_as_uint(thr));
+                    }
+                }
+            }
+
+            // One weight per curve: a cheaper screen in front of `screen`.  With
+            // counts exact in FP32, den = c (N - c) (times N - c for the
+            // likelihood) and th = Et - t bounds |t_exact| for every dip
+            // (t_exact < 0 and |t - t_exact| <= Et), so a box failing
+            // th |th| >= thr den cannot be the best; `screen` then repeats its
+            // own test on the few that pass.  The threshold is shared by the
+            // CTA's warps through s.thr_bits (non-negative floats order as
+            // their bits), each value a lower bound of a box some lane keeps.
+            if (MODE == MODE_UNIFORM) {
+                auto quick = [&](float2 av, float2 bv) -> bool {
+                    const float t = bv.x - av.x;
+                    const float c = bv.y - av.y;
+                    const float oc = Wt - c;
+                    const float den = OBJ ? c * oc * oc : c * oc;
+                    const float th = Et - t;
+                    return (den > 0.0f) & (th * fabsf(th) >= thr * den);
+                };
+                // Starts outer: each lane's two start records (n, n + kThreads) load
+                // once per chunk; widths inner in groups of four (one broadcast
+                // load), so a lane screens eight independent boxes per step and
+                // the warp votes once.  A width with no admissible start in the
+                // chunk (too wide, past the chunk, or a kNoBox slot) reads the
+                // sentinel record instead and fails.  Ties are ordered explicitly
+                // by (duration index, start) in `consider` and the reductions.
+                int dmin = nb;
+                for (int k = 0; k < n_dur; ++k) dmin = min(dmin, s.dur[k]);
+                const int nmax_all = nb - dmin;
+                const int n_groups = (n_dur + 3) >> 2;
+                const uint32_t sent = scr_s + (uint32_t)L * 8u;    // first sentinel record
+                constexpr int kHalf = kThreads * 8;                 // bytes to the second start
+                uint32_t sa = scr_s + (uint32_t)(warp * 32 + lane) * 8u;
+                for (int n0 = warp * 32; n0 <= nmax_all; n0 += 2 * kThreads, sa += 2u * kHalf) {
+                    thr = fmaxf(thr, __uint_as_float(ld_u32(thr_s)));
+                    const float2 a1 = ld_f2(sa), a2 = ld_f2_off<kHalf>(sa);
+                    for (int g = 0; g < n_groups; ++g) {
+                        const int4 dg = *reinterpret_cast<const int4*>(&s.dur[4 * g]);
+                        const int dk[4] = {dg.x, dg.y, dg.z, dg.w};
+                        uint32_t m = 0u;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int d = dk[k];
+                            const bool fits = (d < nb) & (n0 <= nb - d);
+                            const uint32_t sb = fits ? sa + (uint32_t)d * 8u : sent;
+                            const float2 b1 = ld_f2(sb), b2 = ld_f2_off<kHalf>(sb);
+                            m |= (quick(a1, b1) ? 1u : 0u) << (2 * k);
+                            m |= (quick(a2, b2) ? 2u : 0u) << (2 * k);
+                        }
+                        if (__any_sync(kFull, m != 0u)) {
+                            const int n1 = n0 + lane, n2 = n1 + kThreads;
+                            bool upd = false;
+#pragma unroll 1
+                            for (int k = 0; k < 4; ++k) {
+                                if ((m >> (2 * k) & 3u) == 0u) continue;
+                                const int di = 4 * g + k;
+                                const int d = s.dur[di];
+                                const int nmax = nb - d;
+                                float t, l, h;
+                                bool v;
+                                if ((m >> (2 * k) & 1u) && n1 <= nmax &&
+                                    screen(a1, ld_f2(sa + (uint32_t)d * 8u), n1, d, t, l, h, v))
+                                    upd |= consider(n1, di, d, t, l, h, v);
+                                if ((m >> (2 * k) & 2u) && n2 <= nmax &&
+                                    screen(a2, ld_f2_off<kHalf>(sa + (uint32_t)d * 8u), n2, d, t,
+                                           l, h, v))
+                                    upd |= consider(n2, di, d, t, l, h, v);
+                            }
+                            if (__any_sync(kFull, upd)) {
+                                thr = fmaxf(thr,
+                                            warp_max(has ? lb * (1.0f - 2.0f * kRel) : -1.0f));
+                                if (lane == 0) atomicMax(&s.thr_bits, __float_as_uint(thr));
+                            }
+                        }
+                    }
+                }
+            } else
             for (int di = 0; di < n_dur; ++di) {
                 const int d = s.dur[di];
                 if (d >= nb) continue;
                 const int nmax = nb - d;
                 const uint32_t d8 = (uint32_t)d * 8u;
-                for (int n0 = warp * 32; n0 <= nmax; n0 += 2 * kThreads) {
+                // starts past nmax read sentinel records (at most 2 x kThreads + 31
+                // past it, inside the padding) and fail the screen
+                uint32_t sa = scr_s + (uint32_t)(warp * 32 + lane) * 8u;
+                for (int n0 = warp * 32; n0 <= nmax; n0 += 2 * kThreads, sa += 2u * kThreads * 8u) {
                     const int n1 = n0 + lane, n2 = n1 + kThreads;
-                    const bool in1 = n1 <= nmax, in2 = n2 <= nmax;
-                    const uint32_t s1 = scr_s + (uint32_t)(in1 ? n1 : 0) * 8u;
-                    const uint32_t s2 = scr_s + (uint32_t)(in2 ? n2 : 0) * 8u;
-                    const float2 a1 = ld_f2(s1), b1 = ld_f2(s1 + d8);
-                    const float2 a2 = ld_f2(s2), b2 = ld_f2(s2 + d8);
+                    const float2 a1 = ld_f2(sa), b1 = ld_f2(sa + d8);
+                    const float2 a2 = ld_f2(sa + kThreads * 8u), b2 = ld_f2(sa + kThreads * 8u + d8);
                     float t1, l1, h1, t2, l2, h2;
                     bool v1, v2;
-                    const bool c1 = in1 && screen(a1, b1, n1, d, t1, l1, h1, v1);
-                    const bool c2 = in2 && screen(a2, b2, n2, d, t2, l2, h2, v2);
-                    bool upd = false;
-                    if (c1) upd |= consider(n1, di, d, t1, l1, h1, v1);
-                    if (c2) upd |= consider(n2, di, d, t2, l2, h2, v2);
-                    if (__any_sync(kFull, upd))
-                        thr = warp_max(has ? lb * (1.0f - 2.0f * kRel) : -1.0f);
+                    const bool c1 = screen(a1, b1, n1, d, t1, l1, h1, v1);
+                    const bool c2 = screen(a2, b2, n2, d, t2, l2, h2, v2);
+                    if (__any_sync(kFull, c1 | c2)) {
+                        bool upd = false;
+                        if (c1 && n1 <= nmax) upd |= consider(n1, di, d, t1, l1, h1, v1);
+                        if (c2 && n2 <= nmax) upd |= consider(n2, di, d, t2, l2, h2, v2);
+                        if (__any_sync(kFull, upd)) {
+                            thr = fmaxf(thr, warp_max(has ? lb * (1.0f - 2.0f * kRel) : -1.0f));
+                            if (lane == 0) atomicMax(&s.thr_bits, __float_as_uint(thr));
+                        }
+                    }
                 }
             }
 
-            // ---- reduce: lanes whose best may be their warp's maximum -------------
-            const float Lw = warp_max(has ? lb : -1.0f);
-            double v = -CUDART_INF;
-            int vdi = 1 << 30, vn = 1 << 30;
-            if (has && hb >= Lw) {
-                if (!ex_ok) { ex_v = exact(bn, s.dur[bdi]); ex_ok = true; }
-                v = ex_v; vdi = bdi; vn = bn;
-            }
-#pragma unroll
-            for (int k = 16; k > 0; k >>= 1) {
-                const double ov = __shfl_xor_sync(kFull, v, k);
-                const int odi = __shfl_xor_sync(kFull, vdi, k);
-                const int on = __shfl_xor_sync(kFull, vn, k);
-                if (better(ov, odi, on, v, vdi, vn)) { v = ov; vdi = odi; vn = on; }
-            }
-            if (lane == 0) { s.red_v[warp] = v; s.red_di[warp] = vdi; s.red_n[warp] = vn; }
+            // ---- reduce: lanes whose best may be the CTA's maximum --------------
+            // After the barrier s.thr_bits is final: the largest published lower
+            // bound (times 1 - 2 kRel), at most the CTA's best lower bound, so a
+            // lane whose upper bound is below it cannot hold the best box.  The
+            // lane holding that largest lower bound is always a candidate; when
+            // it is the only one its box is the period's best and needs no FP64
+            // comparison (the epilogue evaluates it).  Several candidates (near
+            // ties, or every box in exact mode) are compared in FP64 with the
+            // reference's first-wins order.
             __syncthreads();
-            if (tid == 0) {
-                for (int w = 1; w < kWarps; ++w)
-                    if (better(s.red_v[w], s.red_di[w], s.red_n[w], v, vdi, vn)) {
-                        v = s.red_v[w]; vdi = s.red_di[w]; vn = s.red_n[w];
+            const float Lc = __uint_as_float(ld_u32(thr_s));
+            const bool cand = has && hb >= Lc;
+            const int n_cand = __syncthreads_count(cand);
+            if (n_cand == 1) {
+                if (cand) { s.win_v[q] = 0.0; s.win_di[q] = bdi; s.win_n[q] = bn; }
+            } else {
+                double v = -CUDART_INF;
+                int vdi = 1 << 30, vn = 1 << 30;
+                if (cand) {
+                    if (!ex_ok) { ex_v = exact(bn, s.dur[bdi]); ex_ok = true; }
+                    v = ex_v; vdi = bdi; vn = bn;
+                }
+                if (__any_sync(kFull, cand)) {
+#pragma unroll
+                    for (int k = 16; k > 0; k >>= 1) {
+                        const double ov = __shfl_xor_sync(kFull, v, k);
+                        const int odi = __shfl_xor_sync(kFull, vdi, k);
+                        const int on = __shfl_xor_sync(kFull, vn, k);
+                        if (better(ov, odi, on, v, vdi, vn)) { v = ov; vdi = odi; vn = on; }
                     }
-                s.win_v[q] = v;
-                s.win_di[q] = vdi;
-                s.win_n[q] = vn;
+                }
+                if (lane == 0) { s.red_v[warp] = v; s.red_di[warp] = vdi; s.red_n[warp] = vn; }
+                __syncthreads();
+                if (tid == 0) {
+                    for (int w = 1; w < kWarps; ++w)
+                        if (better(s.red_v[w], s.red_di[w], s.red_n[w], v, vdi, vn)) {
+                            v = s.red_v[w]; vdi = s.red_di[w]; vn = s.red_n[w];
+                        }
+                    s.win_v[q] = v;
+                    s.win_di[q] = vdi;
+                    s.win_n[q] = vn;
+                }
             }
         }
 
@@ -814,19 +974,28 @@ __global__ void best_kernel(const double* power, int64_t n_periods, int64_t* bes
 }  // namespace
 
 cudaError_t configure_search(size_t smem) {
-    cudaError_t e = cudaFuncSetAttribute(bls_search_kernel<MODE_UNIFORM>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(bls_search_kernel<MODE_GENERAL>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const void* fns[4] = {(const void*)bls_search_kernel<MODE_UNIFORM, 0>,
+                          (const void*)bls_search_kernel<MODE_UNIFORM, 1>,
+                          (const void*)bls_search_kernel<MODE_GENERAL, 0>,
+                          (const void*)bls_search_kernel<MODE_GENERAL, 1>};
+    for (const void* f : fns) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_search(const BatchArgs& args, int mode, int n_ctas, size_t smem,
                           cudaStream_t stream) {
-    if (mode == MODE_UNIFORM)
-        bls_search_kernel<MODE_UNIFORM><<<n_ctas, kThreads, smem, stream>>>(args);
-    else
-        bls_search_kernel<MODE_GENERAL><<<n_ctas, kThreads, smem, stream>>>(args);
+    const bool ll = args.obj_flag != 0;
+    if (mode == MODE_UNIFORM) {
+        if (ll) bls_search_kernel<MODE_UNIFORM, 1><<<n_ctas, kThreads, smem, stream>>>(args);
+        else bls_search_kernel<MODE_UNIFORM, 0><<<n_ctas, kThreads, smem, stream>>>(args);
+    } else {
+        if (ll) bls_search_kernel<MODE_GENERAL, 1><<<n_ctas, kThreads, smem, stream>>>(args);
+        else bls_search_kernel<MODE_GENERAL, 0><<<n_ctas, kThreads, smem, stream>>>(args);
+    }
     return cudaGetLastError();
 }
 
@@ -874,14 +1043,20 @@ size_t period_hist_bytes(int mode, int hl) {
 }
 
 int max_resident_ctas(int mode, size_t smem) {
-    int blocks = 0;
-    if (mode == MODE_UNIFORM)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, bls_search_kernel<MODE_UNIFORM>,
+    // the smaller of the two objectives' occupancies
+    int b0 = 0, b1 = 0;
+    if (mode == MODE_UNIFORM) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, bls_search_kernel<MODE_UNIFORM, 0>,
                                                       kThreads, smem);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, bls_search_kernel<MODE_GENERAL>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, bls_search_kernel<MODE_UNIFORM, 1>,
                                                       kThreads, smem);
-    return blocks;
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, bls_search_kernel<MODE_GENERAL, 0>,
+                                                      kThreads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, bls_search_kernel<MODE_GENERAL, 1>,
+                                                      kThreads, smem);
+    }
+    return b0 < b1 ? b0 : b1;
 }
 
 }  // namespace blsb200
