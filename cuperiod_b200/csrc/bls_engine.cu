@@ -142,7 +142,9 @@ FoldParams fold_params(int64_t width, double bin, double tau_max, double f_max, 
     while ((int64_t(1) << (lw + 1)) <= width) ++lw;          // floor(log2(width))
     fp.fb = 31 - lw;                                         // width * 2^fb < 2^32
     const double two32 = 4294967296.0;
-    // our phase error (cycles): RN(x*RN(1/P)) and the 2^-32 grid
+    // our phase error (cycles): RN(1/P) and the product x*RN(1/P) (the kernel
+    // adds it to 1.5*2^20 in one FMA, so the product is not rounded on its own:
+    // this bound is conservative) and the 2^-32 grid
     const double e_phi = q_max * std::ldexp(1.0, -52) * 1.01 + std::ldexp(1.0, -33);
     // the reference's floor(RN(x/P)) is exact unless the phase is this close to a cycle edge
     const double e_phi_ref = q_max * std::ldexp(1.0, -53);

@@ -16,7 +16,7 @@
 //      13 bits and the signed high part of r_q (its quantised centred
 //      flux*weight) to two words and 1 to the bin's count.  With per-point
 //      weights the two sums stay FP64.  A lane holds 8 time-consecutive points
-//      and merges equal bins in registers before it touches shared memory;
+//      (the lanes of a warp 8 points apart, so their bins rarely collide);
 //   2. per period: applies the reference's wrap pad (_bls_core.py:377-381),
 //      turns the bins into prefix sums in place and writes an FP32 screen copy;
 //   3. sweeps every (duration, start) box.  An FP32 bound on the box objective
@@ -69,6 +69,7 @@ struct TileShared {
     double red_v[kWarps];
     int red_di[kWarps];
     int red_n[kWarps];
+    int red_ne[kWarps];             // GENERAL scan: last non-empty bin per warp
     int next;
     uint32_t thr_bits;              // the sweep's shared threshold (bits of a float >= 0)
 };
@@ -88,9 +89,10 @@ __device__ __forceinline__ int fold_exact(double x, double P, double bin, int wi
 __device__ __forceinline__ int fold_fast(double x, double f, uint32_t S, int fb, uint32_t fmask,
                                          uint32_t mu, uint32_t fr_span, uint32_t mphi,
                                          uint32_t phi_span) {
-    const double q = __dmul_rn(x, f);
-    const double qm = __dadd_rn(q, 1572864.0);          // 1.5 * 2^20: ulp 2^-32
-    const uint32_t phi = (uint32_t)__double2loint(qm);   // round(frac(q) * 2^32)
+    // x*f + 1.5*2^20 in one rounding: the ulp there is 2^-32, so the low word is
+    // round(frac(x*f) * 2^32)
+    const double qm = __fma_rn(x, f, 1572864.0);
+    const uint32_t phi = (uint32_t)__double2loint(qm);
     const uint32_t v = __umulhi(phi, S);                 // phase * P/bin * 2^fb
     const bool ok = ((phi - mphi) < phi_span) & (((v & fmask) - mu) < fr_span);
     return ok ? (int)(v >> fb) + 1 : -1;
@@ -249,10 +251,40 @@ __device__ __forceinline__ void fold_points(const TileShared& s, uint32_t hist_s
     const double bin = g.bin_duration;
     const int width = g.width;
     const uint32_t pbytes = (uint32_t)hist_period_bytes<MODE>(hl);
+    constexpr uint32_t kB = (uint32_t)bin_bytes<MODE>();
     for (int q = 0; q < pt; ++q) {
         const double f = s.freq[q];
         const uint32_t S = s.scale[q];
         const uint32_t hq = hist_s + (uint32_t)q * pbytes;
+        if (!TAIL && fast) {
+            // common case: every point's fast fold (fold_fast, inlined here) is
+            // provably the reference's bin, and the records take their atomics
+            // with no per-point test
+            uint32_t rec[kPts];
+            bool all_ok = true;
+#pragma unroll
+            for (int r = 0; r < kPts; ++r) {
+                const double qm = __fma_rn(p.x[r], f, 1572864.0);
+                const uint32_t phi = (uint32_t)__double2loint(qm);
+                const uint32_t v = __umulhi(phi, S);
+                all_ok &= ((phi - mphi) < phi_span) & (((v & fmask) - mu) < fr_span);
+                rec[r] = hq + kB + (v >> fb) * kB;
+            }
+            if (all_ok) {
+#pragma unroll
+                for (int r = 0; r < kPts; ++r) {
+                    if (MODE == MODE_UNIFORM) {
+                        red_add_u32<0>(rec[r], p.lo[r]);
+                        red_add_u32<4>(rec[r], p.hi[r]);
+                        red_add_u32<8>(rec[r], 1u);
+                    } else {
+                        shared_add_f64(rec[r], p.rv[r], flag);
+                        shared_add_f64(rec[r] + 8, p.iv[r], flag);
+                    }
+                }
+                continue;
+            }
+        }
         // 1. the fast fold of all points, straight-line (-1: near an edge, -2: skip)
         int ind[kPts];
         bool miss = false;
@@ -452,11 +484,15 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                 __syncthreads();
             }
 
-            // prefix scan, pass 1: per-warp totals of each contiguous range
-            const int E = ((L + kWarps * 32 - 1) / (kWarps * 32)) * 32;
-            const int lo_i = warp * E;
+            // prefix scan.  Lane `lane` of warp `warp` owns K consecutive bins from
+            // (warp * 32 + lane) * K, K odd so that the lanes' 12-byte records sit
+            // in distinct banks.  Pass 1: each lane sums its bins, the warp scans
+            // the 32 lane totals once and publishes its own total.
+            const int K = ((L + kThreads - 1) / kThreads) | 1;
+            const int lo_i = warp * 32 * K;
+            const int hi_i = min(L, lo_i + 32 * K);
+            const int l0 = min(L, lo_i + lane * K), l1 = min(L, l0 + K);
             if (tid == 0) s.thr_bits = 0u;      // every warp left the last sweep
-            const int hi_i = min(L, lo_i + E);
             if (!overlap) {
                 for (int k = lane; k < o; k += 32) {
                     const int dst = nb - o + k;
@@ -464,110 +500,110 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
                 }
                 __syncwarp();
             }
+            uint32_t ea = 0u, ec = 0u;          // this lane's exclusive offsets in the warp
+            int32_t eb = 0;
+            double er = 0.0, ew = 0.0;
+            // GENERAL: the lane's leading empty bins and its last non-empty bin
+            // (the FP64 prefix of a run of empty bins is made exactly constant)
+            int lead = 0, last_ne = -1;
             {
-                uint32_t ta = 0u, tc = 0u;
-                int32_t tb = 0;
-                double tr = 0.0, tw = 0.0;
-                for (int i = lo_i + lane; i < hi_i; i += 32) {
+                uint32_t ua = 0u, uc = 0u;
+                int32_t ub = 0;
+                double ur = 0.0, uw = 0.0;
+                for (int i = l0; i < l1; ++i) {
                     const uint32_t rec = hq + (uint32_t)i * kRec;
                     if (MODE == MODE_UNIFORM) {
-                        ta += ld_u32(rec);
-                        tb += (int32_t)ld_u32(rec + 4);
-                        tc += ld_u32(rec + 8);
+                        ua += ld_u32(rec);
+                        ub += (int32_t)ld_u32(rec + 4);
+                        uc += ld_u32(rec + 8);
                     } else {
-                        tr += ld_f64(rec);
-                        tw += ld_f64(rec + 8);
+                        const double br = ld_f64(rec), bw = ld_f64(rec + 8);
+                        ur += br;
+                        uw += bw;
+                        const bool empty = (br == 0.0) & (bw == 0.0);
+                        if (!empty) last_ne = i;
+                        else if (last_ne < 0) ++lead;
                     }
                 }
                 if (MODE == MODE_UNIFORM) {
-                    ta = warp_sum(ta);
-                    tb = warp_sum(tb);
-                    tc = warp_sum(tc);
+                    uint32_t ia = ua, ic = uc;
+                    int32_t ib = ub;
+#pragma unroll
+                    for (int k = 1; k < 32; k <<= 1) {
+                        const uint32_t xa = __shfl_up_sync(kFull, ia, k);
+                        const int32_t xb = __shfl_up_sync(kFull, ib, k);
+                        const uint32_t xc = __shfl_up_sync(kFull, ic, k);
+                        if (lane >= k) { ia += xa; ib += xb; ic += xc; }
+                    }
+                    ea = ia - ua; eb = ib - ub; ec = ic - uc;
+                    if (lane == 31) { s.tot_a[warp] = ia; s.tot_b[warp] = ib; s.tot_c[warp] = ic; }
                 } else {
-                    tr = warp_sum(tr);
-                    tw = warp_sum(tw);
-                }
-                if (lane == 0) {
-                    s.tot_a[warp] = ta;
-                    s.tot_b[warp] = tb;
-                    s.tot_c[warp] = tc;
-                    s.tot_rd[warp] = tr;
-                    s.tot_wd[warp] = tw;
+                    double ir = ur, iw = uw;
+#pragma unroll
+                    for (int k = 1; k < 32; k <<= 1) {
+                        const double xr = __shfl_up_sync(kFull, ir, k);
+                        const double xw = __shfl_up_sync(kFull, iw, k);
+                        if (lane >= k) { ir += xr; iw += xw; }
+                    }
+                    // the lane's offset as the sum of the lanes before it
+                    er = __shfl_up_sync(kFull, ir, 1);
+                    ew = __shfl_up_sync(kFull, iw, 1);
+                    if (lane == 0) { er = 0.0; ew = 0.0; }
+                    if (lane == 31) { s.tot_rd[warp] = ir; s.tot_wd[warp] = iw; }
+                    // last non-empty bin before this lane: exclusive max-scan
+                    int im = last_ne;
+#pragma unroll
+                    for (int k = 1; k < 32; k <<= 1) {
+                        const int x = __shfl_up_sync(kFull, im, k);
+                        if (lane >= k) im = max(im, x);
+                    }
+                    if (lane == 31) s.red_ne[warp] = im;
+                    last_ne = __shfl_up_sync(kFull, im, 1);
+                    if (lane == 0) last_ne = -1;
                 }
             }
             __syncthreads();
-            // pass 2: inclusive scan inside each range, prefix written in place,
-            // FP32 screen copy {t prefix, weight prefix}
+            if (MODE == MODE_GENERAL)
+                for (int w = 0; w < warp; ++w) last_ne = max(last_ne, s.red_ne[w]);
+            // pass 2: the lane walks its bins again from its offset, writes the
+            // prefix in place and the FP32 screen copy {t prefix, weight prefix}
             float tmax = 0.0f;
             {
-                uint32_t oa = 0u, oc = 0u;
-                int32_t ob = 0;
-                double orr = 0.0, ow = 0.0;
+                uint32_t ra = ea, rc = ec;
+                int32_t rb = eb;
+                double rr = er, rw = ew;
                 for (int w = 0; w < warp; ++w) {
-                    oa += s.tot_a[w];
-                    ob += s.tot_b[w];
-                    oc += s.tot_c[w];
-                    orr += s.tot_rd[w];
-                    ow += s.tot_wd[w];
+                    if (MODE == MODE_UNIFORM) {
+                        ra += s.tot_a[w];
+                        rb += s.tot_b[w];
+                        rc += s.tot_c[w];
+                    } else {
+                        rr += s.tot_rd[w];
+                        rw += s.tot_wd[w];
+                    }
                 }
-                for (int g = lo_i; g < hi_i; g += 32) {
-                    const int i = g + lane;
-                    const bool in = i < hi_i;
-                    const uint32_t rec = hq + (uint32_t)(in ? i : lo_i) * kRec;
+                for (int i = l0; i < l1; ++i) {
+                    const uint32_t rec = hq + (uint32_t)i * kRec;
                     float tf, wf;
                     if (MODE == MODE_UNIFORM) {
-                        uint32_t va = in ? ld_u32(rec) : 0u, vc = in ? ld_u32(rec + 8) : 0u;
-                        int32_t vb = in ? (int32_t)ld_u32(rec + 4) : 0;
-#pragma unroll
-                        for (int k = 1; k < 32; k <<= 1) {
-                            const uint32_t xa = __shfl_up_sync(kFull, va, k);
-                            const int32_t xb = __shfl_up_sync(kFull, vb, k);
-                            const uint32_t xc = __shfl_up_sync(kFull, vc, k);
-                            if (lane >= k) {
-                                va += xa;
-                                vb += xb;
-                                vc += xc;
-                            }
-                        }
-                        const uint32_t pa = oa + va, pc = oc + vc;
-                        const int32_t pb = ob + vb;
-                        __syncwarp();
-                        if (in) {
-                            st_u32(rec, pa);
-                            st_u32(rec + 4, (uint32_t)pb);
-                            st_u32(rec + 8, pc);
-                        }
-                        tf = (float)((long long)pb * (1ll << kHalfBits) + (long long)pa);
-                        wf = (float)pc;
-                        oa += __shfl_sync(kFull, va, 31);
-                        ob += __shfl_sync(kFull, vb, 31);
-                        oc += __shfl_sync(kFull, vc, 31);
+                        ra += ld_u32(rec);
+                        rb += (int32_t)ld_u32(rec + 4);
+                        rc += ld_u32(rec + 8);
+                        st_u32(rec, ra);
+                        st_u32(rec + 4, (uint32_t)rb);
+                        st_u32(rec + 8, rc);
+                        tf = (float)((long long)rb * (1ll << kHalfBits) + (long long)ra);
+                        wf = (float)rc;
                     } else {
-                        double vr = in ? ld_f64(rec) : 0.0, vw = in ? ld_f64(rec + 8) : 0.0;
-#pragma unroll
-                        for (int k = 1; k < 32; k <<= 1) {
-                            const double xr = __shfl_up_sync(kFull, vr, k);
-                            const double xw = __shfl_up_sync(kFull, vw, k);
-                            if (lane >= k) {
-                                vr += xr;
-                                vw += xw;
-                            }
-                        }
-                        const double cr = orr + vr, cw = ow + vw;
-                        __syncwarp();
-                        if (in) {
-                            st_f64(rec, cr);
-                            st_f64(rec + 8, cw);
-                        }
-                        tf = (float)cr;
-                        wf = (float)cw;
-                        orr += __shfl_sync(kFull, vr, 31);
-                        ow += __shfl_sync(kFull, vw, 31);
+                        rr += ld_f64(rec);
+                        rw += ld_f64(rec + 8);
+                        st_f64(rec, rr);
+                        st_f64(rec + 8, rw);
+                        tf = (float)rr;
+                        wf = (float)rw;
                     }
-                    if (in) {
-                        st_f2(scr_s + (uint32_t)i * 8u, make_float2(tf, wf));
-                        tmax = fmaxf(tmax, fabsf(tf));
-                    }
+                    st_f2(scr_s + (uint32_t)i * 8u, make_float2(tf, wf));
+                    tmax = fmaxf(tmax, fabsf(tf));
                 }
                 tmax = warp_max(tmax);
                 if (lane == 0) s.red_t[warp] = tmax;
@@ -576,6 +612,25 @@ __global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
             for (int i = L + tid; i < L + kScreenPad; i += kThreads)
                 st_f2(scr_s + (uint32_t)i * 8u, make_float2(CUDART_NAN_F, 0.0f));
             __syncthreads();
+            if (MODE == MODE_GENERAL) {
+                // The lanes' partial sums associate differently from one running
+                // sum, so at a lane boundary an empty bin could move the FP64
+                // prefix by a rounding.  The reference's running sum keeps it
+                // exactly constant, which makes boxes that differ only by empty
+                // end bins tie exactly (first wins); copy the prefix of the last
+                // non-empty bin into this lane's leading empty bins.
+                if (lead > 0 && last_ne >= 0) {
+                    const uint32_t rs = hq + (uint32_t)last_ne * kRec;
+                    const double pr = ld_f64(rs), pw = ld_f64(rs + 8);
+                    for (int i = l0; i < l0 + lead; ++i) {
+                        const uint32_t rec = hq + (uint32_t)i * kRec;
+                        st_f64(rec, pr);
+                        st_f64(rec + 8, pw);
+                        st_f2(scr_s + (uint32_t)i * 8u, make_float2((float)pr, (float)pw));
+                    }
+                }
+                __syncthreads();
+            }
             tmax = 0.0f;
 #pragma unroll
             for (int w = 0; w < kWarps; ++w) tmax = fmaxf(tmax, s.red_t[w]);
