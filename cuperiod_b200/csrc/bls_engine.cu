@@ -209,7 +209,7 @@ struct BlsEngine {
     int64_t n_periods = 0;
     int n_items_mode[2] = {0, 0};
     int ctas_mode[2] = {0, 0};
-    size_t smem = 0;
+    size_t smem_mode[2] = {0, 0};
     BatchArgs args[2]{};
     BlsBatchInfo info{};
 
@@ -385,7 +385,9 @@ void parallel_for(int n, F&& fn) {
     for (auto& x : th) x.join();
 }
 
-constexpr size_t kDefaultSmem = 108 * 1024;     // two CTAs per SM with the static state
+// Dynamic shared memory per CTA: one weight per curve runs three CTAs per SM
+// (the kernel is built for 80 registers), per-point weights two.
+constexpr size_t kDefaultSmem[2] = {72 * 1024, 108 * 1024};
 
 size_t screen_bytes(int /*mode*/, int hl) { return ((size_t)hl + kScreenPad) * 8; }
 size_t period_bytes(int mode, int hl) { return period_hist_bytes(mode, hl); }
@@ -538,23 +540,24 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     }
 
     // ---- shared memory, tiles, work items (largest first) ----------------------
-    size_t smem = e->tune.smem_per_cta > 0 ? (size_t)e->tune.smem_per_cta : kDefaultSmem;
     bool modes[2] = {n_uniform > 0, n_uniform < nc};
-    for (int s = 0; s < ns; ++s) {
-        if (segs[s].empty_periods) continue;
-        for (int m = 0; m < 2; ++m) {
-            if (!modes[m]) continue;
+    size_t smem_mode[2];
+    for (int m = 0; m < 2; ++m) {
+        size_t sm = e->tune.smem_per_cta > 0 ? (size_t)e->tune.smem_per_cta : kDefaultSmem[m];
+        for (int s = 0; s < ns && modes[m]; ++s) {
+            if (segs[s].empty_periods) continue;
             const size_t need = screen_bytes(m, segs[s].d.hist_len) + 16 +
                                 period_bytes(m, segs[s].d.hist_len);
-            if (need > smem) smem = need;
+            if (need > sm) sm = need;
         }
+        sm = (sm + 15) & ~size_t(15);
+        if (modes[m] && sm > e->smem_optin)
+            return fail(BLS_E_RESOURCE,
+                        "BLS: %zu bytes of shared memory per period exceed the device's %zu; "
+                        "narrow the period range (max_period_days)",
+                        sm, e->smem_optin);
+        smem_mode[m] = sm;
     }
-    smem = (smem + 15) & ~size_t(15);
-    if (smem > e->smem_optin)
-        return fail(BLS_E_RESOURCE,
-                    "BLS: %zu bytes of shared memory per period exceed the device's %zu; "
-                    "narrow the period range (max_period_days)",
-                    smem, e->smem_optin);
     // per segment: boxes of one curve (the same for every curve)
     double seg_box_sum = 0.0, trials_per_curve = 0.0;
     for (int s = 0; s < ns; ++s) {
@@ -580,7 +583,7 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
         for (int s = 0; s < ns; ++s) {
             plan_tiles[m][s] = (int32_t)acc;
             if (segs[s].empty_periods) continue;
-            const int cap = tile_cap(m, segs[s].d.hist_len, smem, e->tune.max_tile);
+            const int cap = tile_cap(m, segs[s].d.hist_len, smem_mode[m], e->tune.max_tile);
             if (cap < 1) return fail(BLS_E_RESOURCE, "segment %d does not fit shared memory", s);
             plan_cap[m][s] = cap;
             acc += (segs[s].d.n_periods + cap - 1) / cap;
@@ -681,7 +684,8 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
              "upload descriptors");
     h2d += (int64_t)(grid_bytes + meta_bytes);
     CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, 64, st), "reset control words");
-    CUDA_TRY(configure_search(smem), "shared-memory opt-in");
+    for (int m = 0; m < 2; ++m)
+        if (modes[m]) CUDA_TRY(configure_search(m, smem_mode[m]), "shared-memory opt-in");
 
     const char* dgp = e->d_period.as<char>();
     const double* dper = reinterpret_cast<const double*>(dgp);
@@ -720,11 +724,12 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
         a.error_flag = ctl + 8;
         a.debug_prefix = nullptr;
         a.obj_flag = g->objective;
-        const int per_sm = std::max(1, max_resident_ctas(m, smem));
+        const int per_sm = std::max(1, max_resident_ctas(m, smem_mode[m]));
         e->ctas_mode[m] = std::min(a.n_items, e->n_sm * per_sm);
         ctas_total = std::max(ctas_total, e->ctas_mode[m]);
     }
-    e->smem = smem;
+    e->smem_mode[0] = smem_mode[0];
+    e->smem_mode[1] = smem_mode[1];
     e->n_curves = nc;
     e->n_periods = P_total;
     BlsBatchInfo& in = e->info;
@@ -738,7 +743,7 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     in.trials = trials;
     in.h2d_bytes = h2d;
     in.ctas = ctas_total;
-    in.smem_per_cta = (int32_t)smem;
+    in.smem_per_cta = (int32_t)(modes[0] ? smem_mode[0] : smem_mode[1]);
     in.uniform_curves = n_uniform;
     in.fast_fold_segments = fast_segments;
     e->prepared = true;
@@ -750,7 +755,8 @@ int enqueue_search(BlsEngine* e, cudaStream_t st) {
     CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, 2 * sizeof(int32_t), st), "reset work counters");
     for (int m = 0; m < 2; ++m) {
         if (e->args[m].n_items <= 0) continue;
-        CUDA_TRY(launch_search(e->args[m], m, e->ctas_mode[m], e->smem, st), "search launch");
+        CUDA_TRY(launch_search(e->args[m], m, e->ctas_mode[m], e->smem_mode[m], st),
+                 "search launch");
     }
     return BLS_OK;
 }
@@ -914,7 +920,7 @@ int bls_launch_best_noalloc(BlsEngine* e, int64_t* best_index, double* best_powe
         BatchArgs a = e->args[m];
         a.work_counter = ctl + m;
         a.error_flag = ctl + 8;
-        CUDA_TRY(launch_search(a, m, e->ctas_mode[m], e->smem, st), "search launch");
+        CUDA_TRY(launch_search(a, m, e->ctas_mode[m], e->smem_mode[m], st), "search launch");
     }
     int64_t* di = reinterpret_cast<int64_t*>(static_cast<char*>(scr) + kStaticResultsOffset);
     double* dv = reinterpret_cast<double*>(di + kStaticMaxCurves);

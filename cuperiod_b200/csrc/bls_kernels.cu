@@ -361,7 +361,8 @@ __device__ __forceinline__ BoxSums box_sums(uint32_t hq, const CurveDesc& cv, in
 }
 
 template <int MODE, int OBJ>
-__global__ void __launch_bounds__(kThreads, 2) bls_search_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
+    bls_search_kernel(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ TileShared s;
     const int tid = threadIdx.x;
@@ -1028,11 +1029,12 @@ __global__ void best_kernel(const double* power, int64_t n_periods, int64_t* bes
 
 }  // namespace
 
-cudaError_t configure_search(size_t smem) {
-    const void* fns[4] = {(const void*)bls_search_kernel<MODE_UNIFORM, 0>,
-                          (const void*)bls_search_kernel<MODE_UNIFORM, 1>,
-                          (const void*)bls_search_kernel<MODE_GENERAL, 0>,
-                          (const void*)bls_search_kernel<MODE_GENERAL, 1>};
+cudaError_t configure_search(int mode, size_t smem) {
+    const void* fns[2] = {
+        mode == MODE_UNIFORM ? (const void*)bls_search_kernel<MODE_UNIFORM, 0>
+                             : (const void*)bls_search_kernel<MODE_GENERAL, 0>,
+        mode == MODE_UNIFORM ? (const void*)bls_search_kernel<MODE_UNIFORM, 1>
+                             : (const void*)bls_search_kernel<MODE_GENERAL, 1>};
     for (const void* f : fns) {
         const cudaError_t e =
             cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

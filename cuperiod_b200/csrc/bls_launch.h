@@ -8,9 +8,9 @@
 
 namespace blsb200 {
 
-// Opt the search kernels in to `smem` bytes of dynamic shared memory (called
-// outside any stream capture).
-cudaError_t configure_search(size_t smem);
+// Opt the search kernels of one accumulation mode in to `smem` bytes of dynamic
+// shared memory (called outside any stream capture).
+cudaError_t configure_search(int mode, size_t smem);
 
 // Persistent search over every work item of the batch in `args`.
 cudaError_t launch_search(const BatchArgs& args, int mode, int n_ctas, size_t smem,
