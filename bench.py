@@ -186,6 +186,7 @@ def run_ours(args) -> None:
     import torch.distributed as dist
 
     from cuperiod_b200 import _lib
+    from cuperiod_b200.sharding import max_over_ranks
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -199,12 +200,6 @@ def run_ours(args) -> None:
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     curves, segments, grid, packed = workload(args.curves, args.seed + rank)
     engine = _lib.Engine(device=local)
