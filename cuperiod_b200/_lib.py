@@ -78,6 +78,7 @@ def load() -> ctypes.CDLL:
         lib.bls_device_output.argtypes = [_vp, P(_vp)]
         lib.bls_download_best.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
         lib.bls_launch_best_noalloc.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
+        lib.bls_download_rows.argtypes = [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp]
         lib.bls_search.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_batch_info.argtypes = [_vp, P(BlsBatchInfo)]
         lib.bls_debug_fold_bins.argtypes = [_vp, _vp, _i64, _dbl, _dbl, _i32, _vp, _vp]
@@ -86,7 +87,7 @@ def load() -> ctypes.CDLL:
         for name in ("bls_engine_create", "bls_engine_destroy", "bls_prepare", "bls_launch",
                      "bls_download", "bls_device_output", "bls_download_best", "bls_search",
                      "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix",
-                     "bls_launch_best_noalloc"):
+                     "bls_launch_best_noalloc", "bls_download_rows"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib
@@ -229,6 +230,23 @@ class Engine:
         _check(self._lib.bls_download_best(self._h, idx.ctypes.data, val.ctypes.data,
                                            mean.ctypes.data, std.ctypes.data, stream))
         return idx, val, mean, std
+
+    def rows(self, n_best: int, harmonic_max: int, min_separation, alias_tolerance,
+             stream: int | None = None):
+        """The prepared batch's result-row peaks ranked on the device:
+        ``(n_peaks (C,), index (C, n_best), fields (C, n_best, 8))`` with fields
+        period, frequency, power, depth, depth_snr, duration, t0, sde."""
+        assert self._curves is not None
+        n = self._curves.n_curves
+        sep = np.ascontiguousarray(min_separation, dtype=np.float64).reshape(n)
+        tol = np.ascontiguousarray(alias_tolerance, dtype=np.float64).reshape(n)
+        counts = np.empty(n, dtype=np.int32)
+        index = np.empty((n, n_best), dtype=np.int64)
+        fields = np.empty((n, n_best, 8), dtype=np.float64)
+        _check(self._lib.bls_download_rows(self._h, int(n_best), int(harmonic_max),
+                                           sep.ctypes.data, tol.ctypes.data, counts.ctypes.data,
+                                           index.ctypes.data, fields.ctypes.data, stream))
+        return counts, index, fields
 
     def launch_best_noalloc(self, stream: int | None = None):
         """Search the prepared batch and return its per-curve best, allocating

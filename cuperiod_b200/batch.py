@@ -118,13 +118,10 @@ def batch_periodograms(inputs: Iterable[tuple[str, Any]], method: str = "BLS", *
                 ok.append((key, lc))
             if not ok:
                 continue
-            pgs = m.power_many(g, [lc for _, lc in ok], s, engine=eng)
+            # peaks ranked on the device: only the rows leave the GPU
+            summary.rows.extend(m.rows_many(g, ok, s, n_best=n_best,
+                                            extra_keys=PEAK_EXTRA_COLUMNS, engine=eng))
             summary.launches += 1
-            for (key, _), pg in zip(ok, pgs):
-                summary.rows.append(periodogram_to_row(key, pg.with_peak_defaults(s),
-                                                       n_best=n_best,
-                                                       extra_keys=PEAK_EXTRA_COLUMNS,
-                                                       alias_diverse=True))
     if sink is not None and summary.rows:
         import pyarrow as pa
         import pyarrow.parquet as pq

@@ -204,6 +204,74 @@ class BLSMethod:
         return [_assemble(_fields(out[:, i, :], segments), f.n, f.baseline, f.meta)
                 for i, (f, _) in enumerate(prepared)]
 
+    def rows_many(self, grid: GridSpec, keyed: Sequence[tuple[str, LightCurve]],
+                  settings: BLSSettings, *, n_best: int = 10, extra_keys: Sequence[str] = (),
+                  engine: _lib.Engine | None = None) -> list[dict]:
+        """Result rows of many light curves over one grid with their peaks ranked
+        on the device: what ``periodogram_to_row(pg.with_peak_defaults(settings),
+        n_best=..., alias_diverse=True)`` gives for each curve's periodogram
+        (batch/io.py:507-571, core/result.py:285-367), without bringing the
+        spectra back.  ``extra_keys``: the per-peak extras every rank carries
+        (NaN past the last peak)."""
+        from .result import DEFAULT_HARMONIC_MAX, DEFAULT_SEPARATION_RAYLEIGH
+        from .settings import peak_defaults
+        segments = _grid_segments(grid, settings)
+        if not segments:
+            raise InsufficientDataError("BLS: empty trial grid")
+        count = max(int(n_best), 1)
+        prepared = [_prepared_curve(lc, settings) for _, lc in keyed]
+        eng = engine or _lib.default_engine()
+        periods = np.concatenate([np.asarray(p, dtype=np.float64) for p, _ in segments])
+        if count > 1024 or periods.size < 1 or not np.all(np.diff(periods) > 0.0):
+            # outside the device ranking's preconditions: rank on the host
+            from .batch import periodogram_to_row
+            out = self._search(segments, [(f.time, f.value, e) for f, e in prepared], settings,
+                               eng)
+            return [periodogram_to_row(key, _assemble(_fields(out[:, i, :], segments), f.n,
+                                                      f.baseline, f.meta)
+                                       .with_peak_defaults(settings), n_best=count,
+                                       extra_keys=extra_keys, alias_diverse=True)
+                    for i, ((key, _), (f, _)) in enumerate(zip(keyed, prepared))]
+        grid_p = _lib.PackedGrid.from_segments(segments, settings.bins_per_duration,
+                                               _objective_flag(settings.objective))
+        eng.prepare(grid_p, _lib.PackedCurves.from_arrays(
+            [(f.time, f.value, e) for f, e in prepared]))
+        eng.launch()
+        d = peak_defaults(settings)
+        sep_r = float(d.get("min_separation_rayleigh", DEFAULT_SEPARATION_RAYLEIGH))
+        order = int(d.get("harmonic_max", DEFAULT_HARMONIC_MAX))
+        tol_set = d.get("alias_tolerance")
+        sep = np.empty(len(prepared))
+        tol = np.empty(len(prepared))
+        for i, (f, _) in enumerate(prepared):
+            resolved = f.baseline > 0.0
+            separation = sep_r / f.baseline if resolved else 0.0
+            t = tol_set if tol_set is not None else (
+                min(separation, 1.0 / f.baseline) if resolved else 0.0)
+            sep[i] = max(separation, 1e-12)
+            tol[i] = max(float(t), 1e-12)
+        n_peaks, _, fields = eng.rows(count, order, sep, tol)
+        names = ("depth", "depth_snr", "duration", "t0", "sde")
+        rows = []
+        for i, ((key, _), (f, _)) in enumerate(zip(keyed, prepared)):
+            k_have = int(n_peaks[i])
+            row: dict[str, Any] = {"key": key, "method": self.name, "backend": BACKEND_NAME,
+                                   "n_samples": f.n, "baseline": f.baseline}
+            row["best_period"] = float(fields[i, 0, 0]) if k_have else float("nan")
+            for rank in range(1, int(n_best) + 1):
+                have = rank <= k_have
+                fr = fields[i, rank - 1]
+                row[f"period_{rank}"] = float(fr[0]) if have else float("nan")
+                row[f"power_{rank}"] = float(fr[2]) if have else float("nan")
+                extra = {n: float(fr[3 + j]) for j, n in enumerate(names)} if have else {}
+                for ekey in extra_keys:
+                    row[f"{ekey}_{rank}"] = extra.get(ekey, float("nan"))
+                for ekey, v in extra.items():
+                    if ekey not in extra_keys:
+                        row[f"{ekey}_{rank}"] = v
+            rows.append(row)
+        return rows
+
     def _search(self, segments, curves, settings, engine):
         grid = _lib.PackedGrid.from_segments(segments, settings.bins_per_duration,
                                              _objective_flag(settings.objective))

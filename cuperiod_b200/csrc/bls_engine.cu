@@ -199,9 +199,9 @@ struct BlsEngine {
 
     // device buffers
     DevBuf d_tau, d_pay_r, d_r64, d_iv64, d_period, d_freq, d_scale, d_nbins, d_dur, d_curves,
-        d_segments, d_items, d_out, d_ctl, d_best;
+        d_segments, d_rows, d_out, d_ctl, d_best;
     // pinned staging
-    HostBuf h_tau, h_pay_r, h_r64, h_iv64, h_grid, h_meta, h_ctl, h_best;
+    HostBuf h_tau, h_pay_r, h_r64, h_iv64, h_grid, h_meta, h_ctl, h_best, h_rows;
 
     // the prepared batch
     bool prepared = false;
@@ -220,9 +220,10 @@ struct BlsEngine {
     ~BlsEngine() {
         if (graph) cudaGraphExecDestroy(graph);
         for (DevBuf* b : {&d_tau, &d_pay_r, &d_r64, &d_iv64, &d_period, &d_freq, &d_scale, &d_nbins,
-                          &d_dur, &d_curves, &d_segments, &d_items, &d_out, &d_ctl, &d_best})
+                          &d_dur, &d_curves, &d_segments, &d_rows, &d_out, &d_ctl, &d_best})
             b->release();
-        for (HostBuf* b : {&h_tau, &h_pay_r, &h_r64, &h_iv64, &h_grid, &h_meta, &h_ctl, &h_best})
+        for (HostBuf* b : {&h_tau, &h_pay_r, &h_r64, &h_iv64, &h_grid, &h_meta, &h_ctl, &h_best,
+                           &h_rows})
             b->release();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -895,6 +896,62 @@ int bls_download_best(BlsEngine* e, int64_t* best_index, double* best_power, dou
     std::memcpy(best_power, hv, sizeof(double) * nc);
     std::memcpy(power_mean, hv + nc, sizeof(double) * nc);
     std::memcpy(power_std, hv + 2 * nc, sizeof(double) * nc);
+    return BLS_OK;
+}
+
+int bls_download_rows(BlsEngine* e, int32_t n_best, int32_t harmonic_max,
+                      const double* min_separation, const double* alias_tolerance,
+                      int32_t* n_peaks, int64_t* index, double* fields, void* stream) {
+    if (!e || !min_separation || !alias_tolerance || !n_peaks || !index || !fields)
+        return fail(BLS_E_INVALID, "engine, per-curve parameters and outputs are required");
+    if (!e->prepared) return fail(BLS_E_STATE, "bls_download_rows before bls_prepare");
+    if (n_best < 1 || n_best > 1024) return fail(BLS_E_INVALID, "n_best must be in 1..1024");
+    if (harmonic_max < 1 || harmonic_max > 4096)
+        return fail(BLS_E_INVALID, "harmonic_max must be in 1..4096");
+    const int nc = e->n_curves;
+    const int64_t P = e->n_periods;
+    if (P < 1) return fail(BLS_E_INVALID, "the prepared grid has no periods");
+    // frequency order is reversed grid order only for strictly increasing periods
+    const double* hper = e->h_grid.as<double>();
+    for (int64_t i = 1; i < P; ++i)
+        if (!(hper[i] > hper[i - 1]))
+            return fail(BLS_E_INVALID, "rows need strictly increasing trial periods");
+    const size_t mask_bytes = sizeof(uint32_t) * (size_t)((P + 31) / 32);
+    if (mask_bytes + 4096 > e->smem_optin)
+        return fail(BLS_E_RESOURCE, "%lld periods exceed the peak search's shared memory",
+                    (long long)P);
+    for (int c = 0; c < nc; ++c)
+        if (!(min_separation[c] > 0.0) || !(alias_tolerance[c] > 0.0))
+            return fail(BLS_E_INVALID, "separation and alias tolerance must be > 0 (curve %d)", c);
+    CUDA_TRY(cudaSetDevice(e->device), "select device");
+    cudaStream_t st = pick(e, stream);
+    const size_t in_bytes = sizeof(double) * 2 * nc;
+    const size_t idx_bytes = sizeof(int64_t) * (size_t)nc * n_best;
+    const size_t fld_bytes = sizeof(double) * 8 * (size_t)nc * n_best;
+    const size_t cnt_bytes = sizeof(int32_t) * (size_t)nc;
+    const size_t out_bytes = idx_bytes + fld_bytes + ((cnt_bytes + 15) & ~size_t(15));
+    int rc;
+    if ((rc = e->d_rows.ensure(in_bytes + out_bytes))) return rc;
+    if ((rc = e->h_rows.ensure(in_bytes + out_bytes))) return rc;
+    char* hb = e->h_rows.as<char>();
+    std::memcpy(hb, min_separation, sizeof(double) * nc);
+    std::memcpy(hb + sizeof(double) * nc, alias_tolerance, sizeof(double) * nc);
+    char* db = e->d_rows.as<char>();
+    CUDA_TRY(cudaMemcpyAsync(db, hb, in_bytes, cudaMemcpyHostToDevice, st), "upload row parameters");
+    const double* dsep = reinterpret_cast<const double*>(db);
+    const double* dtol = dsep + nc;
+    int64_t* didx = reinterpret_cast<int64_t*>(db + in_bytes);
+    double* dfld = reinterpret_cast<double*>(db + in_bytes + idx_bytes);
+    int32_t* dcnt = reinterpret_cast<int32_t*>(db + in_bytes + idx_bytes + fld_bytes);
+    CUDA_TRY(launch_rows(e->d_out.as<double>(), (int64_t)nc * P, nc, P, e->args[0].period, dsep,
+                         dtol, n_best, harmonic_max, dcnt, didx, dfld, st),
+             "peak search launch");
+    CUDA_TRY(cudaMemcpyAsync(hb + in_bytes, db + in_bytes, out_bytes, cudaMemcpyDeviceToHost, st),
+             "download rows");
+    if ((rc = check_device_flag(e, st))) return rc;
+    std::memcpy(index, hb + in_bytes, idx_bytes);
+    std::memcpy(fields, hb + in_bytes + idx_bytes, fld_bytes);
+    std::memcpy(n_peaks, hb + in_bytes + idx_bytes + fld_bytes, cnt_bytes);
     return BLS_OK;
 }
 

@@ -953,6 +953,192 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
     }
 }
 
+// ---- per-curve result rows: SDE normalisation and alias-diverse peaks -------
+// The reference's row (src/cuperiod/batch/io.py:507-571) ranks the peaks of the
+// assembled spectrum (methods/bls.py:274-301): power with non-finite values as
+// 0, SDE = (power - mean) / std, candidates = interior local maxima in ascending
+// frequency (strictly above the lower-frequency neighbour, >= the higher) plus
+// the boundary points (core/result.py:369-406), then greedy highest-score
+// candidates skipping any alias-related to one already chosen
+// (core/peaks.py:128-231).  Greedy selection equals taking, n times, the best
+// remaining candidate and dropping every candidate related to it, which is what
+// one CTA per curve does here.  The grid is in ascending period, so frequency
+// order is reversed grid order.
+
+__device__ __forceinline__ double nan_to_zero(double v) { return isfinite(v) ? v : 0.0; }
+
+// is_alias_related(f_new, f_chosen) with the reference's FP64 operations in its
+// order (no contraction): duplicate within `sep`, harmonics and subharmonics up
+// to `hmax`, sidereal/solar day offsets (x1, x2) and the yearly offset.
+__device__ bool alias_related(double fn, double fc, double tol, int hmax, double sep,
+                              const double* offs) {
+    if (fabs(__dsub_rn(fn, fc)) < sep) return true;
+    for (int m = 2; m <= hmax; ++m) {
+        const double md = (double)m;
+        if (fabs(__dsub_rn(fn, __dmul_rn(md, fc))) < __dmul_rn(md, tol)) return true;
+        if (fabs(__dsub_rn(fn, __ddiv_rn(fc, md))) < tol) return true;
+    }
+    for (int k = 0; k < 5; ++k) {
+        const double off = offs[k];
+        if (fabs(__dsub_rn(fn, fabs(__dsub_rn(fc, off)))) < tol ||
+            fabs(__dsub_rn(fn, __dadd_rn(fc, off))) < tol)
+            return true;
+    }
+    return false;
+}
+
+// Position of grid index j among the reference's candidates: interior maxima in
+// ascending frequency, then the lowest-frequency point, then the highest.  Among
+// equal scores the later position ranks first (a stable ascending sort, reversed).
+__device__ __forceinline__ long long cand_pos(long long j, long long P) {
+    if (P == 1) return 0;
+    if (j == P - 1) return P;
+    if (j == 0) return P + 1;
+    return P - 1 - j;
+}
+
+__global__ void __launch_bounds__(kThreads) rows_kernel(
+    const double* __restrict__ out, int64_t out_stride, int64_t P,
+    const double* __restrict__ period, const double* __restrict__ sep_c,
+    const double* __restrict__ tol_c, int n_best, int hmax, int32_t* n_peaks,
+    int64_t* index, double* fields) {
+    extern __shared__ uint32_t cand[];                   // ceil(P / 32) words
+    __shared__ double red_d[kWarps];
+    __shared__ double red_s[kWarps];
+    __shared__ long long red_p[kWarps];
+    __shared__ long long red_j[kWarps];
+    __shared__ double s_mean, s_std;
+    __shared__ long long s_win;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int c = blockIdx.x;
+    const double* pw = out + (int64_t)c * P;             // field 0 (power) of curve c
+    const int64_t nw = (P + 31) / 32;
+    const double sep = sep_c[c], tol = tol_c[c];
+    double offs[5];
+    offs[0] = 1.0027379;                                 // sidereal day, cycles/day
+    offs[1] = __dmul_rn(2.0, 1.0027379);
+    offs[2] = 1.0;                                       // solar day
+    offs[3] = 2.0;
+    offs[4] = __ddiv_rn(1.0, 365.25);                    // year
+
+    // mean and population standard deviation of the power (two passes)
+    double sum = 0.0;
+    for (int64_t j = tid; j < P; j += kThreads) sum += nan_to_zero(pw[j]);
+    sum = warp_sum(sum);
+    if (lane == 0) red_d[warp] = sum;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kWarps; ++w) t += red_d[w];
+        s_mean = t / (double)P;
+    }
+    __syncthreads();
+    const double mean = s_mean;
+    double ss = 0.0;
+    for (int64_t j = tid; j < P; j += kThreads) {
+        const double d = nan_to_zero(pw[j]) - mean;
+        ss += d * d;
+    }
+    ss = warp_sum(ss);
+    if (lane == 0) red_d[warp] = ss;
+    // candidate words, each owned by one thread
+    for (int64_t w = tid; w < nw; w += kThreads) {
+        uint32_t bits = 0u;
+        for (int b = 0; b < 32; ++b) {
+            const int64_t j = w * 32 + b;
+            if (j >= P) break;
+            const double v = nan_to_zero(pw[j]);
+            bool is;
+            if (P == 1) {
+                is = true;
+            } else if (j == P - 1) {                     // lowest frequency
+                is = v >= nan_to_zero(pw[j - 1]);
+            } else if (j == 0) {                         // highest frequency
+                is = v > nan_to_zero(pw[1]);
+            } else {                                     // above the lower frequency, >= the higher
+                is = (v > nan_to_zero(pw[j + 1])) & (v >= nan_to_zero(pw[j - 1]));
+            }
+            if (is) bits |= 1u << b;
+        }
+        cand[w] = bits;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kWarps; ++w) t += red_d[w];
+        s_std = sqrt(t / (double)P);
+    }
+
+    int count = 0;
+    for (int r = 0; r < n_best; ++r) {
+        // the best remaining candidate: highest score, then later position
+        double bs = -CUDART_INF;
+        long long bp = -1, bj = -1;
+        for (int64_t w = tid; w < nw; w += kThreads) {
+            uint32_t bits = cand[w];
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1u;
+                const long long j = w * 32 + b;
+                const double v = nan_to_zero(pw[j]);
+                const long long pos = cand_pos(j, P);
+                if (v > bs || (v == bs && pos > bp)) { bs = v; bp = pos; bj = j; }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double os = __shfl_xor_sync(kFull, bs, o);
+            const long long op = __shfl_xor_sync(kFull, bp, o);
+            const long long oj = __shfl_xor_sync(kFull, bj, o);
+            if (oj >= 0 && (bj < 0 || os > bs || (os == bs && op > bp))) { bs = os; bp = op; bj = oj; }
+        }
+        if (lane == 0) { red_s[warp] = bs; red_p[warp] = bp; red_j[warp] = bj; }
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 1; w < kWarps; ++w)
+                if (red_j[w] >= 0 && (bj < 0 || red_s[w] > bs || (red_s[w] == bs && red_p[w] > bp))) {
+                    bs = red_s[w]; bp = red_p[w]; bj = red_j[w];
+                }
+            s_win = bj;
+            if (bj >= 0) {
+                const double f = __ddiv_rn(1.0, period[bj]);
+                const double v = nan_to_zero(pw[bj]);
+                double* fo = fields + ((int64_t)c * n_best + r) * 8;
+                fo[0] = __ddiv_rn(1.0, f);                          // period = 1 / frequency
+                fo[1] = f;
+                fo[2] = v;                                          // power
+                fo[3] = out[1 * out_stride + (int64_t)c * P + bj];  // depth
+                fo[4] = out[3 * out_stride + (int64_t)c * P + bj];  // depth_snr
+                fo[5] = out[4 * out_stride + (int64_t)c * P + bj];  // duration
+                fo[6] = out[5 * out_stride + (int64_t)c * P + bj];  // t0
+                fo[7] = s_std > 0.0 ? (v - s_mean) / s_std : 0.0;  // sde
+                index[(int64_t)c * n_best + r] = bj;
+            }
+        }
+        __syncthreads();
+        const long long win = s_win;
+        if (win < 0) break;
+        ++count;
+        // drop the winner and every candidate alias-related to it, either way
+        const double fc = __ddiv_rn(1.0, period[win]);
+        for (int64_t w = tid; w < nw; w += kThreads) {
+            uint32_t bits = cand[w], keep = bits;
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1u;
+                const long long j = w * 32 + b;
+                const double fn = __ddiv_rn(1.0, period[j]);
+                if (j == win || alias_related(fn, fc, tol, hmax, sep, offs) ||
+                    alias_related(fc, fn, tol, hmax, sep, offs))
+                    keep &= ~(1u << b);
+            }
+            cand[w] = keep;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) n_peaks[c] = count;
+}
+
 // Phase bins of every point at one period through the fast path with its
 // fallback (the tests compare them with the reference's fold bit for bit).
 __global__ void fold_bins_kernel(const double* tau, int n, double P, double f, uint32_t S,
@@ -1061,6 +1247,20 @@ cudaError_t launch_best(const double* power, int n_curves, int64_t n_periods, in
     if (n_curves <= 0) return cudaSuccess;
     best_kernel<<<n_curves, kThreads, 0, stream>>>(power, n_periods, best_index, best_power, mean,
                                                    sd);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rows(const double* out, int64_t out_stride, int n_curves, int64_t n_periods,
+                        const double* period, const double* sep, const double* tol, int n_best,
+                        int harmonic_max, int32_t* n_peaks, int64_t* index, double* fields,
+                        cudaStream_t stream) {
+    if (n_curves <= 0) return cudaSuccess;
+    const size_t smem = sizeof(uint32_t) * (size_t)((n_periods + 31) / 32);
+    cudaError_t e = cudaFuncSetAttribute(rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    rows_kernel<<<n_curves, kThreads, smem, stream>>>(out, out_stride, n_periods, period, sep, tol,
+                                                      n_best, harmonic_max, n_peaks, index, fields);
     return cudaGetLastError();
 }
 

@@ -134,6 +134,23 @@ int bls_device_output(BlsEngine* engine, const double** out);
 int bls_download_best(BlsEngine* engine, int64_t* best_index, double* best_power,
                       double* power_mean, double* power_std, void* stream);
 
+/* Per curve, the result row's peaks, ranked on the device: the reference's
+ * periodogram_to_row / Periodogram.best_periods(alias_diverse=True) /
+ * select_diverse_peaks (batch/io.py:507-571, core/result.py:285-406,
+ * core/peaks.py:128-231) over the assembled spectrum of methods/bls.py:274-301
+ * (non-finite power as 0, SDE normalisation).  Inputs per curve: the minimum
+ * frequency separation (the reference's max(rayleigh/baseline, 1e-12)) and the
+ * alias tolerance (max(tol, 1e-12)); n_best peaks at most; harmonics up to
+ * harmonic_max.  Outputs: n_peaks[c]; index[c*n_best + k] (grid order) and
+ * fields[(c*n_best + k)*8 + f], f = period, frequency, power, depth, depth_snr,
+ * duration, t0, sde.  Needs strictly increasing trial periods (frequency order
+ * is then reversed grid order).  Among candidates of exactly equal power the
+ * later in the reference's candidate order ranks first (its stable-sort
+ * order).  Waits for the stream. */
+int bls_download_rows(BlsEngine* engine, int32_t n_best, int32_t harmonic_max,
+                      const double* min_separation, const double* alias_tolerance,
+                      int32_t* n_peaks, int64_t* index, double* fields, void* stream);
+
 /* No counterpart in the reference.  bls_launch followed by bls_download_best,
  * for callers that must not allocate once their batch is prepared: a service
  * whose device memory is committed to other work, or whose latency cannot absorb
