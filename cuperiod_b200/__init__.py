@@ -17,7 +17,8 @@ from .core import BLSPower, bls_power, bls_power_many, bls_power_segments
 from .errors import (BackendUnavailableError, CuPeriodError, EngineError, GridTooLargeError,
                      InsufficientDataError, UnknownMethodError)
 from .grid import GridSpec, check_grid_size, log_period_grid
-from .lightcurve import Domain, LightCurve
+from .lightcurve import Domain, LightCurve, MultiBandLightCurve
+from .multiband import bls_multiband_power
 from .result import Peak, Periodogram
 from .settings import BLSSettings
 
@@ -26,8 +27,8 @@ __version__ = "0.1.0"
 __all__ = [
     "BLSMethod", "BLSPower", "BLSSettings", "BackendUnavailableError", "BatchSummary",
     "CuPeriodError", "Domain", "EngineError", "GridSpec", "GridTooLargeError",
-    "InsufficientDataError", "LightCurve", "Peak", "Periodogram", "UnknownMethodError",
-    "batch_periodograms", "bls_power", "bls_power_many", "bls_power_segments",
+    "InsufficientDataError", "LightCurve", "MultiBandLightCurve", "Peak", "Periodogram", "UnknownMethodError",
+    "batch_periodograms", "bls_multiband_power", "bls_power", "bls_power_many", "bls_power_segments",
     "check_grid_size", "get_method", "log_period_grid", "periodogram", "periodogram_to_row",
     "register", "to_input",
 ]

@@ -9,14 +9,24 @@ import numpy as np
 
 from .bls import get_method
 from .grid import GridSpec
-from .lightcurve import Domain, LightCurve
+from .lightcurve import Domain, LightCurve, MultiBandLightCurve
 from .result import Periodogram
 from .settings import BLSSettings
 
 
-def to_input(data: Any, *, domain: Domain | str | None = None) -> LightCurve:
+def to_input(data: Any, *, domain: Domain | str | None = None) -> LightCurve | MultiBandLightCurve:
     """A ``LightCurve`` from a LightCurve or a ``(t, y[, dy])`` tuple; a bare tuple
-    is read as magnitudes unless ``domain`` says otherwise (api.py:47-106)."""
+    is read as magnitudes unless ``domain`` says otherwise.  A MultiBandLightCurve,
+    or a ``{band: LightCurve or (t, y[, dy])}`` mapping, gives a
+    MultiBandLightCurve (api.py:47-106)."""
+    if isinstance(data, MultiBandLightCurve):
+        if domain is None:
+            return data
+        return MultiBandLightCurve({k: to_input(lc, domain=domain) for k, lc in data.bands.items()},
+                                   data.meta)
+    if isinstance(data, Mapping):
+        return MultiBandLightCurve.from_light_curves(
+            {str(k): to_input(v, domain=domain) for k, v in data.items()})
     if isinstance(data, LightCurve):
         return data if domain is None else LightCurve(data.time, data.value, data.error,
                                                       Domain(domain), data.meta)
@@ -52,6 +62,10 @@ def periodogram(data: Any, method: str = "BLS", *, backend: str | None = "auto",
     lc = to_input(data, domain=domain)
     s = _settings(settings)
     m.resolve_backend(backend if backend not in (None, "auto") else s.backend)
+    if isinstance(lc, MultiBandLightCurve):
+        from .multiband import multiband_default_grid
+        g = grid or multiband_default_grid(m, lc, s)
+        return m.multiband_power(g, lc, s, engine=engine).with_peak_defaults(s)
     single = lc.in_domain(m.natural_domain)
     g = grid or m.default_grid(single, s)
     pg = m.power(g, single, s, engine=engine)

@@ -16,7 +16,7 @@ from .api import _settings, to_input
 from .bls import get_method
 from .errors import CuPeriodError
 from .grid import GridSpec
-from .lightcurve import Domain
+from .lightcurve import Domain, MultiBandLightCurve
 from .result import Periodogram
 
 #: Per-peak extras of a BLS row (io.py:66-70).
@@ -96,7 +96,19 @@ def batch_periodograms(inputs: Iterable[tuple[str, Any]], method: str = "BLS", *
     groups: dict[str, tuple[GridSpec, list[tuple[str, Any]]]] = {}
     for key, data in inputs:
         try:
-            lc = to_input(data, domain=domain).in_domain(m.natural_domain)
+            lc = to_input(data, domain=domain)
+            if isinstance(lc, MultiBandLightCurve):
+                # one star's bands: one launch of its own, peaks ranked on the host
+                from .multiband import multiband_default_grid
+                pg = m.multiband_power(grid or multiband_default_grid(m, lc, s), lc, s,
+                                       engine=eng)
+                summary.rows.append(periodogram_to_row(str(key), pg.with_peak_defaults(s),
+                                                       n_best=n_best,
+                                                       extra_keys=PEAK_EXTRA_COLUMNS,
+                                                       alias_diverse=True))
+                summary.launches += 1
+                continue
+            lc = lc.in_domain(m.natural_domain)
             g = grid or m.default_grid(lc, s)
         except (CuPeriodError, ValueError) as exc:
             summary.errors[str(key)] = f"{type(exc).__name__}: {exc}"

@@ -204,6 +204,15 @@ class BLSMethod:
         return [_assemble(_fields(out[:, i, :], segments), f.n, f.baseline, f.meta)
                 for i, (f, _) in enumerate(prepared)]
 
+    def multiband_power(self, grid: GridSpec, mblc: Any, settings: BLSSettings,
+                        backend: str = BACKEND_NAME, engine: _lib.Engine | None = None, *,
+                        ephemeris: str | None = None) -> Periodogram:
+        """Multi-band BLS on a shared period grid (bls.py:397-411 ->
+        multiband/bls_mb.py:120-275); all bands in one engine launch."""
+        from .multiband import bls_multiband_power
+        self.resolve_backend(backend)
+        return bls_multiband_power(grid, mblc, settings, ephemeris=ephemeris, engine=engine)
+
     def rows_many(self, grid: GridSpec, keyed: Sequence[tuple[str, LightCurve]],
                   settings: BLSSettings, *, n_best: int = 10, extra_keys: Sequence[str] = (),
                   engine: _lib.Engine | None = None) -> list[dict]:

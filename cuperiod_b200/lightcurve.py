@@ -89,4 +89,62 @@ class LightCurve:
         return LightCurve(self.time, mag, err, Domain.MAGNITUDE, self.meta)
 
 
-__all__ = ["Domain", "LightCurve"]
+@dataclass(frozen=True, eq=False)
+class MultiBandLightCurve:
+    """Several bands (filters) of one star in one brightness domain
+    (src/cuperiod/core/lightcurve.py:330-575); band order is insertion order."""
+
+    bands: Mapping[str, LightCurve]
+    meta: Mapping[str, Any] = field(default_factory=dict)
+
+    def __post_init__(self) -> None:
+        if not self.bands:
+            raise ValueError("MultiBandLightCurve requires at least one band")
+        for name, lc in self.bands.items():
+            if not isinstance(lc, LightCurve):
+                raise TypeError(f"band {name!r} is a {type(lc).__name__}, not a LightCurve")
+        domains = {lc.domain for lc in self.bands.values()}
+        if len(domains) > 1:
+            listing = ", ".join(f"{k}: {lc.domain.value}" for k, lc in self.bands.items())
+            raise ValueError(f"bands are in different brightness domains ({listing})")
+        object.__setattr__(self, "bands", dict(self.bands))
+
+    @classmethod
+    def from_light_curves(cls, bands: Mapping[str, LightCurve], *,
+                          meta: Mapping[str, Any] | None = None) -> "MultiBandLightCurve":
+        return cls(dict(bands), dict(meta or {}))
+
+    @property
+    def band_names(self) -> tuple[str, ...]:
+        return tuple(self.bands)
+
+    @property
+    def n_bands(self) -> int:
+        return len(self.bands)
+
+    def finite(self) -> "MultiBandLightCurve":
+        """Each band's non-finite points removed (lightcurve.py:520-524)."""
+        return MultiBandLightCurve({k: lc.finite() for k, lc in self.bands.items()}, self.meta)
+
+    def stacked(self):
+        """All bands in ascending time: ``(time, value, error or None, band)``;
+        ``error`` is None when a band has none (lightcurve.py:544-575)."""
+        times, values, errors, labels = [], [], [], []
+        missing = False
+        for name, lc in self.bands.items():
+            times.append(lc.time)
+            values.append(lc.value)
+            if lc.error is None:
+                missing = True
+            else:
+                errors.append(lc.error)
+            labels.append(np.full(lc.n, name, dtype=object))
+        time = np.concatenate(times)
+        value = np.concatenate(values)
+        band = np.concatenate(labels)
+        error = None if missing else np.concatenate(errors)
+        order = np.argsort(time, kind="stable")
+        return time[order], value[order], None if error is None else error[order], band[order]
+
+
+__all__ = ["Domain", "LightCurve", "MultiBandLightCurve"]

@@ -303,6 +303,64 @@ def method_power(t, flux, err, periods, meta, s: Settings, n_threads: int | None
     return frequency[order], power[order], {k: v[order] for k, v in extras.items()}
 
 
+def robust_scatter(flux: np.ndarray) -> float:
+    """``_robust_scatter``, ``multiband/bls_mb.py:63-76``: 1.4826 x MAD, else the
+    standard deviation, else 1."""
+    sigma = 1.4826 * float(np.median(np.abs(flux - np.median(flux))))
+    if not (np.isfinite(sigma) and sigma > 0.0):
+        sigma = float(np.std(flux))
+    if not (np.isfinite(sigma) and sigma > 0.0):
+        sigma = 1.0
+    return sigma
+
+
+def multiband_power(bands, periods, meta, s: Settings, n_threads: int | None = None):
+    """``bls_multiband_power`` in its independent mode (``multiband/bls_mb.py:120-275``)
+    on finite flux-domain bands ``[(name, t, flux, err or None), ...]``: bands with
+    at least 3 points are searched over the common segments, the per-period power
+    is the sum of the squared clipped depth-SNRs and the box comes from the band
+    with the largest.  Returns ``(frequency, power, extras, used_band_names,
+    n_samples, baseline)`` in ascending frequency."""
+    used = [b for b in bands if len(b[1]) >= 3]
+    n_total = sum(len(b[1]) for b in used)
+    stacked = np.concatenate([np.asarray(b[1], dtype=np.float64) for b in used])
+    baseline = float(stacked.max() - stacked.min())
+    if all(b[3] is not None for b in used):
+        errors = [np.asarray(b[3], dtype=np.float64) for b in used]
+    else:
+        errors = [np.full(len(b[1]), robust_scatter(np.asarray(b[2], dtype=np.float64)))
+                  for b in used]
+    parts = {k: [] for k in ("period", "power", "depth", "depth_snr", "duration", "t0",
+                             "band_index")}
+    for per, dur in grid_segments(periods, meta, s):
+        seg = [bls_power(np.asarray(b[1], dtype=np.float64), np.asarray(b[2], dtype=np.float64),
+                         e, per, dur, s.bins_per_duration, objective=s.objective,
+                         n_threads=n_threads) for b, e in zip(used, errors)]
+        dsnr = np.vstack([np.clip(o["depth_snr"], 0.0, None) for o in seg])
+        combined = np.sum(dsnr ** 2, axis=0)
+        best = np.argmax(dsnr, axis=0)
+        cols = np.arange(dsnr.shape[1])
+        parts["period"].append(per)
+        parts["power"].append(combined)
+        parts["depth_snr"].append(np.sqrt(combined))
+        parts["depth"].append(np.vstack([o["depth"] for o in seg])[best, cols])
+        parts["duration"].append(np.vstack([o["duration"] for o in seg])[best, cols])
+        parts["t0"].append(np.vstack([o["transit_time"] for o in seg])[best, cols])
+        parts["band_index"].append(best.astype(np.float64))
+    joined = {k: np.concatenate(v) for k, v in parts.items()}
+    period = joined.pop("period")
+    power = np.nan_to_num(joined.pop("power"), nan=0.0, posinf=0.0)
+    mean, std = float(power.mean()), float(power.std())
+    sde = (power - mean) / std if std > 0.0 else np.zeros_like(power)
+    frequency = 1.0 / period
+    order = np.argsort(frequency, kind="stable")
+    extras = {"depth": joined["depth"], "depth_snr": joined["depth_snr"],
+              "duration": joined["duration"], "t0": joined["t0"], "sde": sde,
+              "band_index": joined["band_index"]}
+    return (frequency[order], power[order], {k: v[order] for k, v in extras.items()},
+            [b[0] for b in used], n_total, baseline)
+
+
 def best_index(power: np.ndarray) -> int:
     """Index of ``Periodogram.best_period`` (``core/result.py:369-438``): the highest
     finite candidate among interior local maxima and boundary peaks."""

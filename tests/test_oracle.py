@@ -43,3 +43,31 @@ def test_oracle_method_level_on_golden(case):
         np.testing.assert_array_equal(extras[name], z[f"{k}_x_{name}"])
     i = oracle.best_index(power)
     assert 1.0 / freq[i] == meta["best_period"]
+
+
+def _multiband_cases():
+    index = json.load(open(os.path.join(GOLDEN, "multiband_cases.json")))
+    z = np.load(os.path.join(GOLDEN, "multiband_cases.npz"))
+    return [(m, z) for m in index]
+
+
+def multiband_inputs(meta, z):
+    """The golden case's bands as ``(name, t, flux, err or None)``."""
+    k = meta["key"]
+    return [(b, z[f"{k}_{b}_t"], z[f"{k}_{b}_y"], z[f"{k}_{b}_dy"] if has else None)
+            for b, has in zip(meta["bands"], meta["with_error"])]
+
+
+@pytest.mark.parametrize("case", _multiband_cases(), ids=lambda c: c[0]["key"])
+def test_oracle_multiband_on_golden(case):
+    meta, z = case
+    k = meta["key"]
+    freq, power, extras, used, n, baseline = oracle.multiband_power(
+        multiband_inputs(meta, z), z[f"{k}_periods"], meta["grid_meta"], oracle.Settings(),
+        n_threads=4)
+    assert used == meta["used_bands"] and n == meta["n_samples"] and baseline == meta["baseline"]
+    np.testing.assert_array_equal(freq, z[f"{k}_frequency"])
+    np.testing.assert_array_equal(power, z[f"{k}_power"])
+    for name in meta["extras"]:
+        np.testing.assert_array_equal(extras[name], z[f"{k}_x_{name}"])
+    assert 1.0 / freq[oracle.best_index(power)] == meta["best_period"]
