@@ -16,10 +16,17 @@ namespace blsb200 {
 // bin's sum is (signed) B * 2^13 + A with no carry lost for up to 2^17 points.
 //  UNIFORM: every point has the same inverse variance w: r_q (the quantised
 //           centred flux * weight) and a count per bin (three atomics).
-//  GENERAL: per-point weights.  Their dynamic range can span many decades, so
-//           the two sums (centred flux*weight and weight, both scaled by powers
-//           of two) stay FP64, like the reference's, with FP64 shared atomics.
-enum : int { MODE_UNIFORM = 0, MODE_GENERAL = 1 };
+//  GENERAL: per-point weights spanning more than 2^8: the two sums (centred
+//           flux*weight and weight, both scaled by powers of two) stay FP64, like
+//           the reference's, with FP64 shared atomics.
+//  WIDE:    per-point weights within a factor 2^8 of each other: centred
+//           flux*weight and weight each quantised to 38-bit fixed point
+//           (|v| < 2^37 after a power-of-two scale) and added as three 32-bit
+//           parts (13, 13 and a signed 12-bit high part): six native atomics,
+//           exact integer sums for up to 2^17 points.
+enum : int { MODE_UNIFORM = 0, MODE_GENERAL = 1, MODE_WIDE = 2 };
+constexpr int kModes = 3;
+constexpr int kWideBits = 13;       // WIDE: bits of the low and middle parts
 
 constexpr int kFields = 7;          // power, depth, depth_err, depth_snr, duration, t0, loglike
 constexpr int kMaxDur = 32;         // deduplicated box widths per segment
@@ -97,8 +104,9 @@ struct BatchArgs {
     int32_t n_segments;
     const double* tau;          // per point: t - t_min (FP64)
     const uint32_t* pay_r;      // per point: r_q as low 13 bits | signed high part << 16
-    const double* r64;          // GENERAL: (y*ivar - ybar*ivar) * 2^e_r per point
-    const double* iv64;         // GENERAL: ivar * 2^e_i per point
+    const double* r64;          // GENERAL: (y*ivar - ybar*ivar) * 2^e_r per point;
+                                // WIDE: the same rounded to an int64 (bit pattern)
+    const double* iv64;         // GENERAL: ivar * 2^e_i per point; WIDE: int64 likewise
     const double* period;       // per grid period
     const double* freq;         // RN(1/P)
     const uint32_t* scale;      // round(P/bin * 2^frac_bits)

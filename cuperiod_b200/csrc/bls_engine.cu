@@ -207,10 +207,10 @@ struct BlsEngine {
     bool prepared = false;
     int n_curves = 0;
     int64_t n_periods = 0;
-    int n_items_mode[2] = {0, 0};
-    int ctas_mode[2] = {0, 0};
-    size_t smem_mode[2] = {0, 0};
-    BatchArgs args[2]{};
+    int n_items_mode[kModes] = {0, 0, 0};
+    int ctas_mode[kModes] = {0, 0, 0};
+    size_t smem_mode[kModes] = {0, 0, 0};
+    BatchArgs args[kModes]{};
     BlsBatchInfo info{};
 
     // CUDA graph of one launch
@@ -332,7 +332,30 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
         pay_r[point_slot(j, n)] = split_word(std::llrint(std::ldexp(r[j], e_r)));
     int e_i = 0;
     double i_total = 0.0;
-    if (!uniform) {
+    // per-point weights within a factor 2^8 of each other: 38-bit fixed point
+    // (the smallest weight keeps >= 2^28 steps, a relative 2^-29)
+    double min_i = max_i;
+    for (int64_t j = 0; j < n && !uniform; ++j) min_i = std::min(min_i, iv[j]);
+    const bool wide = !uniform && min_i > 0.0 && std::isfinite(max_i) &&
+                      max_i <= 256.0 * min_i && max_r > 0.0 && std::isfinite(max_r);
+    if (wide) {
+        int kr = 0, ki = 0;
+        std::frexp(max_r, &kr);            // max_r < 2^kr
+        std::frexp(max_i, &ki);
+        const int e_rw = 37 - kr, e_iw = 37 - ki;       // |v| < 2^37
+        int64_t total = 0;
+        for (int64_t j = 0; j < n; ++j) {
+            const int64_t m = point_slot(j, n);
+            const long long rq = std::llrint(std::ldexp(r[j], e_rw));
+            const long long iq = std::llrint(std::ldexp(iv[j], e_iw));
+            std::memcpy(&r64[m], &rq, sizeof(rq));
+            std::memcpy(&iv64[m], &iq, sizeof(iq));
+            total += iq;
+        }
+        e_r = e_rw;
+        e_i = e_iw;
+        i_total = (double)total;
+    } else if (!uniform) {
         // per-point weights: FP64 values scaled by powers of two (exact)
         if (max_i > 0.0 && std::isfinite(max_i)) {
             std::frexp(max_i, &k);
@@ -348,7 +371,7 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
     const double eps = DBL_EPSILON;
     double floor_v = 4.0 * (double)n * eps * sum_ivar;            // _ivar_floor, 75-94
     if (!(floor_v > 0.0)) floor_v = DBL_MIN;
-    d.mode = uniform ? MODE_UNIFORM : MODE_GENERAL;
+    d.mode = uniform ? MODE_UNIFORM : (wide ? MODE_WIDE : MODE_GENERAL);
     d.exact_all = !(sum_abs >= 1e-150 && sum_abs <= 1e150 && sum_ivar >= 1e-150 &&
                     sum_ivar <= 1e150);
     d.skip = !(sum_ivar > 0.0 && std::isfinite(sum_ivar));
@@ -387,8 +410,9 @@ void parallel_for(int n, F&& fn) {
 }
 
 // Dynamic shared memory per CTA: one weight per curve runs three CTAs per SM
-// (the kernel is built for 80 registers), per-point weights two.
-constexpr size_t kDefaultSmem[2] = {72 * 1024, 108 * 1024};
+// (the kernel is built for 80 registers), per-point weights (FP64 or wide
+// fixed point) two.
+constexpr size_t kDefaultSmem[kModes] = {72 * 1024, 108 * 1024, 108 * 1024};
 
 size_t screen_bytes(int /*mode*/, int hl) { return ((size_t)hl + kScreenPad) * 8; }
 size_t period_bytes(int mode, int hl) { return period_hist_bytes(mode, hl); }
@@ -442,11 +466,13 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     });
     double tau_max = 0.0;
     int n_uniform = 0;
+    int n_mode[kModes] = {0, 0, 0};
     for (int c = 0; c < nc; ++c) {
         if (curves[c].status) return fail(curves[c].status, "%s", curves[c].err.c_str());
         if (e->tune.exact_sweep) curves[c].d.exact_all = 1;
         tau_max = std::max(tau_max, curves[c].tau_max);
         n_uniform += curves[c].d.mode == MODE_UNIFORM;
+        n_mode[curves[c].d.mode]++;
     }
 
     // ---- segments and period constants (reference binning) ---------------------
@@ -541,9 +567,9 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     }
 
     // ---- shared memory, tiles, work items (largest first) ----------------------
-    bool modes[2] = {n_uniform > 0, n_uniform < nc};
-    size_t smem_mode[2];
-    for (int m = 0; m < 2; ++m) {
+    bool modes[kModes] = {n_mode[0] > 0, n_mode[1] > 0, n_mode[2] > 0};
+    size_t smem_mode[kModes];
+    for (int m = 0; m < kModes; ++m) {
         size_t sm = e->tune.smem_per_cta > 0 ? (size_t)e->tune.smem_per_cta : kDefaultSmem[m];
         for (int s = 0; s < ns && modes[m]; ++s) {
             if (segs[s].empty_periods) continue;
@@ -574,9 +600,9 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     }
     // per mode: tiles of each segment, their prefix, and the curves largest first
     // (so the last work items of a launch are the cheapest)
-    std::vector<int32_t> plan_tiles[2], plan_cap[2], plan_order[2];
-    int64_t n_items_mode[2] = {0, 0};
-    for (int m = 0; m < 2; ++m) {
+    std::vector<int32_t> plan_tiles[kModes], plan_cap[kModes], plan_order[kModes];
+    int64_t n_items_mode[kModes] = {0, 0, 0};
+    for (int m = 0; m < kModes; ++m) {
         plan_tiles[m].assign(ns + 1, 0);
         plan_cap[m].assign(std::max(ns, 1), 1);
         if (!modes[m]) continue;
@@ -607,10 +633,11 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     const double trials = trials_per_curve * nc;
 
     // ---- stage metadata and upload ---------------------------------------------
-    const int64_t n_items = n_items_mode[0] + n_items_mode[1];
+    const int64_t n_items = n_items_mode[0] + n_items_mode[1] + n_items_mode[2];
     const size_t grid_bytes = (size_t)P_total * (8 + 8 + 4 + 4) + dur_all.size() * 4 + 64;
     // descriptors, then per mode: order (nc in all), seg_tiles (ns + 1), seg_cap (ns)
-    const size_t plan_words = (size_t)nc + 2 * (size_t)(ns + 1) + 2 * (size_t)std::max(ns, 1);
+    const size_t plan_words =
+        (size_t)nc + kModes * (size_t)(ns + 1) + kModes * (size_t)std::max(ns, 1);
     const size_t meta_bytes = sizeof(CurveDesc) * nc + sizeof(SegmentDesc) * std::max(ns, 1) +
                               sizeof(int32_t) * plan_words + 64;
     if ((rc = e->h_grid.ensure(grid_bytes))) return rc;
@@ -634,15 +661,15 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     int32_t* hplan = reinterpret_cast<int32_t*>(hseg + std::max(ns, 1));
     for (int c = 0; c < nc; ++c) hcur[c] = curves[c].d;
     for (int s = 0; s < ns; ++s) hseg[s] = segs[s].d;
-    size_t plan_off[2][3];          // per mode: order, seg_tiles, seg_cap (in words)
+    size_t plan_off[kModes][3];     // per mode: order, seg_tiles, seg_cap (in words)
     {
         size_t w = 0;
-        for (int m = 0; m < 2; ++m) {
+        for (int m = 0; m < kModes; ++m) {
             plan_off[m][0] = w;
             std::copy(plan_order[m].begin(), plan_order[m].end(), hplan + w);
             w += plan_order[m].size();
         }
-        for (int m = 0; m < 2; ++m) {
+        for (int m = 0; m < kModes; ++m) {
             plan_off[m][1] = w;
             std::copy(plan_tiles[m].begin(), plan_tiles[m].end(), hplan + w);
             w += ns + 1;
@@ -651,8 +678,7 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
             w += std::max(ns, 1);
         }
     }
-    e->n_items_mode[0] = (int32_t)n_items_mode[0];
-    e->n_items_mode[1] = (int32_t)n_items_mode[1];
+    for (int m = 0; m < kModes; ++m) e->n_items_mode[m] = (int32_t)n_items_mode[m];
 
     const size_t out_elems = (size_t)kFields * nc * std::max<int64_t>(P_total, 1);
     if ((rc = e->d_tau.ensure(sizeof(double) * std::max<int64_t>(n_pts, 1)))) return rc;
@@ -670,7 +696,7 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
                              st),
              "upload flux words");
     h2d += (int64_t)n_pts * 12;
-    if (n_uniform < nc) {
+    if (n_uniform < nc) {               // FP64 or fixed-point per-point values
         CUDA_TRY(cudaMemcpyAsync(e->d_r64.p, hr64, sizeof(double) * n_pts, cudaMemcpyHostToDevice,
                                  st),
                  "upload flux*weight");
@@ -685,7 +711,7 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
              "upload descriptors");
     h2d += (int64_t)(grid_bytes + meta_bytes);
     CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, 64, st), "reset control words");
-    for (int m = 0; m < 2; ++m)
+    for (int m = 0; m < kModes; ++m)
         if (modes[m]) CUDA_TRY(configure_search(m, smem_mode[m]), "shared-memory opt-in");
 
     const char* dgp = e->d_period.as<char>();
@@ -700,7 +726,7 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     const int32_t* dplan = reinterpret_cast<const int32_t*>(dseg + std::max(ns, 1));
     int32_t* ctl = e->d_ctl.as<int32_t>();
     int ctas_total = 0;
-    for (int m = 0; m < 2; ++m) {
+    for (int m = 0; m < kModes; ++m) {
         BatchArgs& a = e->args[m];
         a.curves = dcur;
         a.segments = dseg;
@@ -729,8 +755,7 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
         e->ctas_mode[m] = std::min(a.n_items, e->n_sm * per_sm);
         ctas_total = std::max(ctas_total, e->ctas_mode[m]);
     }
-    e->smem_mode[0] = smem_mode[0];
-    e->smem_mode[1] = smem_mode[1];
+    for (int m = 0; m < kModes; ++m) e->smem_mode[m] = smem_mode[m];
     e->n_curves = nc;
     e->n_periods = P_total;
     BlsBatchInfo& in = e->info;
@@ -744,7 +769,7 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     in.trials = trials;
     in.h2d_bytes = h2d;
     in.ctas = ctas_total;
-    in.smem_per_cta = (int32_t)(modes[0] ? smem_mode[0] : smem_mode[1]);
+    in.smem_per_cta = (int32_t)(modes[0] ? smem_mode[0] : modes[2] ? smem_mode[2] : smem_mode[1]);
     in.uniform_curves = n_uniform;
     in.fast_fold_segments = fast_segments;
     e->prepared = true;
@@ -753,8 +778,8 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
 
 // Enqueue one search (both accumulation modes) on `st`.
 int enqueue_search(BlsEngine* e, cudaStream_t st) {
-    CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, 2 * sizeof(int32_t), st), "reset work counters");
-    for (int m = 0; m < 2; ++m) {
+    CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, kModes * sizeof(int32_t), st), "reset work counters");
+    for (int m = 0; m < kModes; ++m) {
         if (e->args[m].n_items <= 0) continue;
         CUDA_TRY(launch_search(e->args[m], m, e->ctas_mode[m], e->smem_mode[m], st),
                  "search launch");
@@ -972,7 +997,7 @@ int bls_launch_best_noalloc(BlsEngine* e, int64_t* best_index, double* best_powe
     CUDA_TRY(static_scratch_address(e->device, &scr), "static scratch address");
     int32_t* ctl = static_cast<int32_t*>(scr);
     CUDA_TRY(cudaMemsetAsync(ctl, 0, 64, st), "reset work counters and error flag");
-    for (int m = 0; m < 2; ++m) {
+    for (int m = 0; m < kModes; ++m) {
         if (e->args[m].n_items <= 0) continue;
         BatchArgs a = e->args[m];
         a.work_counter = ctl + m;
@@ -1032,7 +1057,8 @@ int bls_debug_prefix(BlsEngine* e, const double* t, const double* y, const doubl
     BlsCurves c{1, offs, t, y, dy};
     int rc;
     if ((rc = do_prepare(e, &g, &c, e->stream))) return rc;
-    const int mode = e->args[0].n_items > 0 ? 0 : 1;
+    int mode = 0;
+    while (mode < kModes - 1 && e->args[mode].n_items <= 0) ++mode;
     int32_t hl = 0;
     CUDA_TRY(cudaStreamSynchronize(e->stream), "synchronize");
     {

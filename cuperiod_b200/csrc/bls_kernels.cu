@@ -46,6 +46,10 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr float kRel = 1.0f / 262144.0f;    // 2^-18: relative slack of FP32 key bounds
 constexpr int kCasLimit = 1 << 16;          // retries of one FP64 shared add
 constexpr int kNoBox = 1 << 29;             // duration slot past the last real duration
+// WIDE: the FP32 screen holds weights scaled by 2^-13 (fixed-point weights are
+// below 2^37 per point), the range of the FP64 mode's, so that the likelihood's
+// iv_in * iv_out^2 stays finite in FP32
+constexpr int kWideScreenShift = 13;
 
 struct TileShared {
     WorkItem item;
@@ -59,9 +63,7 @@ struct TileShared {
     double win_v[kMaxTile];         // per period of the tile: the best box
     int32_t win_di[kMaxTile];
     int32_t win_n[kMaxTile];
-    uint32_t tot_a[kWarps];
-    int32_t tot_b[kWarps];
-    uint32_t tot_c[kWarps];
+    uint32_t tot_w[6][kWarps];      // integer prefix scan: per-warp totals of each word
     double tot_rd[kWarps];
     double tot_wd[kWarps];
     float red_f[kWarps];
@@ -199,10 +201,14 @@ __device__ __forceinline__ double box_objective(const BoxSums& s, const CurveDes
 //  UNIFORM: {A, B, C}, 12 bytes -- sum of the low 13 bits of r_q, sum of its
 //           signed high part, count (32-bit words);
 //  GENERAL: {R, W}, 16 bytes -- FP64 sums of the scaled centred flux*weight and
-//           of the scaled weight.
+//           of the scaled weight;
+//  WIDE:    {R0, R1, R2, I0, I1, I2}, 24 bytes -- the three parts of the
+//           fixed-point centred flux*weight and of the weight (32-bit words).
 // A period's region is padded to 16 bytes.
 template <int MODE>
-__device__ __host__ constexpr int bin_bytes() { return MODE == MODE_UNIFORM ? 12 : 16; }
+__device__ __host__ constexpr int bin_bytes() {
+    return MODE == MODE_UNIFORM ? 12 : (MODE == MODE_WIDE ? 24 : 16);
+}
 template <int MODE>
 __device__ __host__ __forceinline__ size_t hist_period_bytes(int hl) {
     return ((size_t)hl * bin_bytes<MODE>() + 15) & ~size_t(15);
@@ -213,7 +219,24 @@ struct PointRegs {
     double x[kPts];
     uint32_t lo[MODE == MODE_UNIFORM ? kPts : 1], hi[MODE == MODE_UNIFORM ? kPts : 1];
     double rv[MODE == MODE_GENERAL ? kPts : 1], iv[MODE == MODE_GENERAL ? kPts : 1];
+    long long rq[MODE == MODE_WIDE ? kPts : 1], iq[MODE == MODE_WIDE ? kPts : 1];
 };
+
+// WIDE: the three 32-bit parts of a fixed-point value (|v| < 2^37): low and
+// middle 13 bits, and the signed high part.
+__device__ __forceinline__ uint32_t wide_part(long long v, int k) {
+    return k == 0 ? (uint32_t)(v & ((1ll << kWideBits) - 1))
+                  : (k == 1 ? (uint32_t)((v >> kWideBits) & ((1ll << kWideBits) - 1))
+                            : (uint32_t)(int32_t)(v >> (2 * kWideBits)));
+}
+// WIDE: the value of three prefix parts.
+__device__ __forceinline__ long long wide_value(uint32_t p0, uint32_t p1, uint32_t p2) {
+    return (long long)(int32_t)p2 * (1ll << (2 * kWideBits)) +
+           (long long)p1 * (1ll << kWideBits) + (long long)p0;
+}
+template <int MODE>
+__device__ __forceinline__ void add_point(uint32_t rec, const PointRegs<MODE>& p, int r,
+                                          int32_t* flag);
 
 template <int MODE, bool TAIL>
 __device__ __forceinline__ void load_points(const BatchArgs& a, const CurveDesc& c, int base,
@@ -229,6 +252,11 @@ __device__ __forceinline__ void load_points(const BatchArgs& a, const CurveDesc&
             const uint32_t w = ok ? __ldg(a.pay_r + c.point_off + j) : 0u;
             p.lo[r] = w & 0xffffu;
             p.hi[r] = (uint32_t)((int32_t)w >> 16);    // signed high part
+        } else if (MODE == MODE_WIDE) {
+            const long long* rq = reinterpret_cast<const long long*>(a.r64) + c.point_off;
+            const long long* iq = reinterpret_cast<const long long*>(a.iv64) + c.point_off;
+            p.rq[r] = ok ? __ldg(rq + j) : 0ll;
+            p.iq[r] = ok ? __ldg(iq + j) : 0ll;
         } else {
             p.rv[r] = ok ? __ldg(a.r64 + c.point_off + j) : 0.0;
             p.iv[r] = ok ? __ldg(a.iv64 + c.point_off + j) : 0.0;
@@ -272,16 +300,7 @@ __device__ __forceinline__ void fold_points(const TileShared& s, uint32_t hist_s
             }
             if (all_ok) {
 #pragma unroll
-                for (int r = 0; r < kPts; ++r) {
-                    if (MODE == MODE_UNIFORM) {
-                        red_add_u32<0>(rec[r], p.lo[r]);
-                        red_add_u32<4>(rec[r], p.hi[r]);
-                        red_add_u32<8>(rec[r], 1u);
-                    } else {
-                        shared_add_f64(rec[r], p.rv[r], flag);
-                        shared_add_f64(rec[r] + 8, p.iv[r], flag);
-                    }
-                }
+                for (int r = 0; r < kPts; ++r) add_point<MODE>(rec[r], p, r, flag);
                 continue;
             }
         }
@@ -310,17 +329,40 @@ __device__ __forceinline__ void fold_points(const TileShared& s, uint32_t hist_s
 #pragma unroll
         for (int r = 0; r < kPts; ++r) {
             if (ind[r] < 0) continue;
-            const uint32_t rec = hq + (uint32_t)ind[r] * (uint32_t)bin_bytes<MODE>();
-            if (MODE == MODE_UNIFORM) {
-                red_add_u32<0>(rec, p.lo[r]);
-                red_add_u32<4>(rec, p.hi[r]);
-                red_add_u32<8>(rec, 1u);
-            } else {
-                shared_add_f64(rec, p.rv[r], flag);
-                shared_add_f64(rec + 8, p.iv[r], flag);
-            }
+            add_point<MODE>(hq + (uint32_t)ind[r] * (uint32_t)bin_bytes<MODE>(), p, r, flag);
         }
     }
+}
+
+// One point's contribution to its bin record.
+template <int MODE>
+__device__ __forceinline__ void add_point(uint32_t rec, const PointRegs<MODE>& p, int r,
+                                          int32_t* flag) {
+    if (MODE == MODE_UNIFORM) {
+        red_add_u32<0>(rec, p.lo[r]);
+        red_add_u32<4>(rec, p.hi[r]);
+        red_add_u32<8>(rec, 1u);
+    } else if (MODE == MODE_WIDE) {
+        red_add_u32<0>(rec, wide_part(p.rq[r], 0));
+        red_add_u32<4>(rec, wide_part(p.rq[r], 1));
+        red_add_u32<8>(rec, wide_part(p.rq[r], 2));
+        red_add_u32<12>(rec, wide_part(p.iq[r], 0));
+        red_add_u32<16>(rec, wide_part(p.iq[r], 1));
+        red_add_u32<20>(rec, wide_part(p.iq[r], 2));
+    } else {
+        shared_add_f64(rec, p.rv[r], flag);
+        shared_add_f64(rec + 8, p.iv[r], flag);
+    }
+}
+
+// WIDE: exact prefixes at bin i of the centred flux*weight and of the weight.
+__device__ __forceinline__ long long wide_prefix_r(uint32_t hq, int i) {
+    const uint32_t rec = hq + (uint32_t)i * 24u;
+    return wide_value(ld_u32(rec), ld_u32(rec + 4), ld_u32(rec + 8));
+}
+__device__ __forceinline__ long long wide_prefix_i(uint32_t hq, int i) {
+    const uint32_t rec = hq + (uint32_t)i * 24u + 12u;
+    return wide_value(ld_u32(rec), ld_u32(rec + 4), ld_u32(rec + 8));
 }
 
 // Exact prefix of r_q at bin i from a UNIFORM record's two prefix words.
@@ -351,6 +393,10 @@ __device__ __forceinline__ BoxSums box_sums(uint32_t hq, const CurveDesc& cv, in
     if (MODE == MODE_UNIFORM) {
         b.iv_in = (double)(prefix_c(hq, n + d) - prefix_c(hq, n)) * cv.w_uniform;
         b.y_in = ldexp((double)(prefix_r(hq, n + d) - prefix_r(hq, n)), -cv.e_r) +
+                 cv.ybar * b.iv_in;
+    } else if (MODE == MODE_WIDE) {
+        b.iv_in = ldexp((double)(wide_prefix_i(hq, n + d) - wide_prefix_i(hq, n)), -cv.e_i);
+        b.y_in = ldexp((double)(wide_prefix_r(hq, n + d) - wide_prefix_r(hq, n)), -cv.e_r) +
                  cv.ybar * b.iv_in;
     } else {
         const uint32_t r1 = hq + (uint32_t)(n + d) * 16u, r0 = hq + (uint32_t)n * 16u;
@@ -455,6 +501,7 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
         const int e_r = cv.e_r, e_i = cv.e_i;
         const int o = s.seg.oversample;
         constexpr uint32_t kRec = (uint32_t)bin_bytes<MODE>();
+        constexpr int kNW = MODE == MODE_UNIFORM ? 3 : (MODE == MODE_WIDE ? 6 : 1);   // words
 
         for (int q = 0; q < pt; ++q) {
             const int nb = s.nb[q];
@@ -463,10 +510,9 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
             auto copy_bin = [&](int dst, int src) {
                 if (dst >= 0 && dst < s.seg.width && dst < hl && src < hl) {
                     const uint32_t rd = hq + (uint32_t)dst * kRec, rs = hq + (uint32_t)src * kRec;
-                    if (MODE == MODE_UNIFORM) {
-                        st_u32(rd, ld_u32(rs));
-                        st_u32(rd + 4, ld_u32(rs + 4));
-                        st_u32(rd + 8, ld_u32(rs + 8));
+                    if (MODE != MODE_GENERAL) {
+#pragma unroll
+                        for (int w = 0; w < kNW; ++w) st_u32(rd + 4 * w, ld_u32(rs + 4 * w));
                     } else {
                         st_f64(rd, ld_f64(rs));
                         st_f64(rd + 8, ld_f64(rs + 8));
@@ -501,22 +547,23 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
                 }
                 __syncwarp();
             }
-            uint32_t ea = 0u, ec = 0u;          // this lane's exclusive offsets in the warp
-            int32_t eb = 0;
+            uint32_t ex[kNW];                   // this lane's exclusive offsets in the warp
+#pragma unroll
+            for (int w = 0; w < kNW; ++w) ex[w] = 0u;
             double er = 0.0, ew = 0.0;
             // GENERAL: the lane's leading empty bins and its last non-empty bin
             // (the FP64 prefix of a run of empty bins is made exactly constant)
             int lead = 0, last_ne = -1;
             {
-                uint32_t ua = 0u, uc = 0u;
-                int32_t ub = 0;
+                uint32_t u[kNW];
+#pragma unroll
+                for (int w = 0; w < kNW; ++w) u[w] = 0u;
                 double ur = 0.0, uw = 0.0;
                 for (int i = l0; i < l1; ++i) {
                     const uint32_t rec = hq + (uint32_t)i * kRec;
-                    if (MODE == MODE_UNIFORM) {
-                        ua += ld_u32(rec);
-                        ub += (int32_t)ld_u32(rec + 4);
-                        uc += ld_u32(rec + 8);
+                    if (MODE != MODE_GENERAL) {
+#pragma unroll
+                        for (int w = 0; w < kNW; ++w) u[w] += ld_u32(rec + 4 * w);
                     } else {
                         const double br = ld_f64(rec), bw = ld_f64(rec + 8);
                         ur += br;
@@ -526,18 +573,24 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
                         else if (last_ne < 0) ++lead;
                     }
                 }
-                if (MODE == MODE_UNIFORM) {
-                    uint32_t ia = ua, ic = uc;
-                    int32_t ib = ub;
+                if (MODE != MODE_GENERAL) {
+                    // 32-bit words added modulo 2^32; every prefix fits its word
+                    uint32_t in[kNW];
+#pragma unroll
+                    for (int w = 0; w < kNW; ++w) in[w] = u[w];
 #pragma unroll
                     for (int k = 1; k < 32; k <<= 1) {
-                        const uint32_t xa = __shfl_up_sync(kFull, ia, k);
-                        const int32_t xb = __shfl_up_sync(kFull, ib, k);
-                        const uint32_t xc = __shfl_up_sync(kFull, ic, k);
-                        if (lane >= k) { ia += xa; ib += xb; ic += xc; }
+#pragma unroll
+                        for (int w = 0; w < kNW; ++w) {
+                            const uint32_t x = __shfl_up_sync(kFull, in[w], k);
+                            if (lane >= k) in[w] += x;
+                        }
                     }
-                    ea = ia - ua; eb = ib - ub; ec = ic - uc;
-                    if (lane == 31) { s.tot_a[warp] = ia; s.tot_b[warp] = ib; s.tot_c[warp] = ic; }
+#pragma unroll
+                    for (int w = 0; w < kNW; ++w) {
+                        ex[w] = in[w] - u[w];
+                        if (lane == 31) s.tot_w[w][warp] = in[w];
+                    }
                 } else {
                     double ir = ur, iw = uw;
 #pragma unroll
@@ -570,31 +623,37 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
             // prefix in place and the FP32 screen copy {t prefix, weight prefix}
             float tmax = 0.0f;
             {
-                uint32_t ra = ea, rc = ec;
-                int32_t rb = eb;
+                uint32_t run[kNW];
+#pragma unroll
+                for (int w = 0; w < kNW; ++w) run[w] = ex[w];
                 double rr = er, rw = ew;
-                for (int w = 0; w < warp; ++w) {
-                    if (MODE == MODE_UNIFORM) {
-                        ra += s.tot_a[w];
-                        rb += s.tot_b[w];
-                        rc += s.tot_c[w];
+                for (int wp = 0; wp < warp; ++wp) {
+                    if (MODE != MODE_GENERAL) {
+#pragma unroll
+                        for (int w = 0; w < kNW; ++w) run[w] += s.tot_w[w][wp];
                     } else {
-                        rr += s.tot_rd[w];
-                        rw += s.tot_wd[w];
+                        rr += s.tot_rd[wp];
+                        rw += s.tot_wd[wp];
                     }
                 }
                 for (int i = l0; i < l1; ++i) {
                     const uint32_t rec = hq + (uint32_t)i * kRec;
                     float tf, wf;
-                    if (MODE == MODE_UNIFORM) {
-                        ra += ld_u32(rec);
-                        rb += (int32_t)ld_u32(rec + 4);
-                        rc += ld_u32(rec + 8);
-                        st_u32(rec, ra);
-                        st_u32(rec + 4, (uint32_t)rb);
-                        st_u32(rec + 8, rc);
-                        tf = (float)((long long)rb * (1ll << kHalfBits) + (long long)ra);
-                        wf = (float)rc;
+                    if (MODE != MODE_GENERAL) {
+#pragma unroll
+                        for (int w = 0; w < kNW; ++w) {
+                            run[w] += ld_u32(rec + 4 * w);
+                            st_u32(rec + 4 * w, run[w]);
+                        }
+                        if (MODE == MODE_UNIFORM) {
+                            tf = (float)((long long)(int32_t)run[1] * (1ll << kHalfBits) +
+                                         (long long)run[0]);
+                            wf = (float)run[2];
+                        } else {
+                            tf = (float)wide_value(run[0], run[1], run[2]);
+                            wf = (float)ldexp((double)wide_value(run[3], run[4], run[5]),
+                                              -kWideScreenShift);
+                        }
                     } else {
                         rr += ld_f64(rec);
                         rw += ld_f64(rec + 8);
@@ -638,6 +697,7 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
 
             auto iv_prefix = [&](int i) -> double {
                 return MODE == MODE_UNIFORM ? (double)prefix_c(hq, i) * cv.w_uniform
+                       : MODE == MODE_WIDE  ? ldexp((double)wide_prefix_i(hq, i), -e_i)
                                             : ldexp(ld_f64(hq + (uint32_t)i * 16u + 8u), -e_i);
             };
             auto exact = [&](int n, int d) -> double {
@@ -645,9 +705,10 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
             };
             if (a.debug_prefix != nullptr && q == 0) {   // test hook: this period's prefixes
                 for (int i = tid; i < L; i += kThreads) {
-                    const double r_i = MODE == MODE_UNIFORM
-                                           ? ldexp((double)prefix_r(hq, i), -e_r)
-                                           : ldexp(ld_f64(hq + (uint32_t)i * 16u), -e_r);
+                    const double r_i =
+                        MODE == MODE_UNIFORM ? ldexp((double)prefix_r(hq, i), -e_r)
+                        : MODE == MODE_WIDE  ? ldexp((double)wide_prefix_r(hq, i), -e_r)
+                                             : ldexp(ld_f64(hq + (uint32_t)i * 16u), -e_r);
                     a.debug_prefix[i] = r_i + cv.ybar * iv_prefix(i);
                     a.debug_prefix[hl + i] = iv_prefix(i);
                 }
@@ -655,10 +716,15 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
 
             // ---- sweep: durations outer (the reference's order), two starts per lane ----
             const float Et = cv.exact_all ? CUDART_INF_F : tmax * (1.0f / 2097152.0f);  // 2^-21
-            const float Wt = MODE == MODE_UNIFORM ? (float)cv.n_points : (float)cv.i_total;
+            const float Wt = MODE == MODE_UNIFORM ? (float)cv.n_points
+                             : MODE == MODE_WIDE  ? (float)ldexp(cv.i_total, -kWideScreenShift)
+                                                  : (float)cv.i_total;
             const float Ei = MODE == MODE_UNIFORM ? 0.0f : Wt * (1.0f / 2097152.0f);
             const float floor_q =
-                MODE == MODE_GENERAL ? (float)ldexp(cv.ivar_floor, e_i) * (1.0f + 1e-3f) : 0.0f;
+                MODE != MODE_UNIFORM
+                    ? (float)ldexp(cv.ivar_floor,
+                                   MODE == MODE_WIDE ? e_i - kWideScreenShift : e_i) * (1.0f + 1e-3f)
+                    : 0.0f;
 
             bool has = false, ex_ok = false;
             int bn = 0, bdi = 0;
@@ -724,8 +790,9 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
                     // an empty box is exactly 0 in the FP64 prefix; t <= Et also
                     // keeps sentinel boxes (t = NaN) away from these loads
                     if (!ok && t <= Et) {
-                        ok = ld_f64(hq + (uint32_t)(n + d) * 16u + 8u) !=
-                             ld_f64(hq + (uint32_t)n * 16u + 8u);
+                        ok = MODE == MODE_WIDE ? wide_prefix_i(hq, n + d) != wide_prefix_i(hq, n)
+                                               : ld_f64(hq + (uint32_t)(n + d) * 16u + 8u) !=
+                                                     ld_f64(hq + (uint32_t)n * 16u + 8u);
                     }
                 }
                 const float th = fabsf(t) + Et;
@@ -1215,13 +1282,17 @@ __global__ void best_kernel(const double* power, int64_t n_periods, int64_t* bes
 
 }  // namespace
 
+namespace {
+template <int OBJ>
+const void* search_fn(int mode) {
+    return mode == MODE_UNIFORM ? (const void*)bls_search_kernel<MODE_UNIFORM, OBJ>
+           : mode == MODE_WIDE  ? (const void*)bls_search_kernel<MODE_WIDE, OBJ>
+                                : (const void*)bls_search_kernel<MODE_GENERAL, OBJ>;
+}
+}  // namespace
+
 cudaError_t configure_search(int mode, size_t smem) {
-    const void* fns[2] = {
-        mode == MODE_UNIFORM ? (const void*)bls_search_kernel<MODE_UNIFORM, 0>
-                             : (const void*)bls_search_kernel<MODE_GENERAL, 0>,
-        mode == MODE_UNIFORM ? (const void*)bls_search_kernel<MODE_UNIFORM, 1>
-                             : (const void*)bls_search_kernel<MODE_GENERAL, 1>};
-    for (const void* f : fns) {
+    for (const void* f : {search_fn<0>(mode), search_fn<1>(mode)}) {
         const cudaError_t e =
             cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -1235,6 +1306,9 @@ cudaError_t launch_search(const BatchArgs& args, int mode, int n_ctas, size_t sm
     if (mode == MODE_UNIFORM) {
         if (ll) bls_search_kernel<MODE_UNIFORM, 1><<<n_ctas, kThreads, smem, stream>>>(args);
         else bls_search_kernel<MODE_UNIFORM, 0><<<n_ctas, kThreads, smem, stream>>>(args);
+    } else if (mode == MODE_WIDE) {
+        if (ll) bls_search_kernel<MODE_WIDE, 1><<<n_ctas, kThreads, smem, stream>>>(args);
+        else bls_search_kernel<MODE_WIDE, 0><<<n_ctas, kThreads, smem, stream>>>(args);
     } else {
         if (ll) bls_search_kernel<MODE_GENERAL, 1><<<n_ctas, kThreads, smem, stream>>>(args);
         else bls_search_kernel<MODE_GENERAL, 0><<<n_ctas, kThreads, smem, stream>>>(args);
@@ -1296,23 +1370,15 @@ int search_threads() { return kThreads; }
 
 size_t period_hist_bytes(int mode, int hl) {
     return mode == MODE_UNIFORM ? hist_period_bytes<MODE_UNIFORM>(hl)
+           : mode == MODE_WIDE  ? hist_period_bytes<MODE_WIDE>(hl)
                                 : hist_period_bytes<MODE_GENERAL>(hl);
 }
 
 int max_resident_ctas(int mode, size_t smem) {
     // the smaller of the two objectives' occupancies
     int b0 = 0, b1 = 0;
-    if (mode == MODE_UNIFORM) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, bls_search_kernel<MODE_UNIFORM, 0>,
-                                                      kThreads, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, bls_search_kernel<MODE_UNIFORM, 1>,
-                                                      kThreads, smem);
-    } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, bls_search_kernel<MODE_GENERAL, 0>,
-                                                      kThreads, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, bls_search_kernel<MODE_GENERAL, 1>,
-                                                      kThreads, smem);
-    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, search_fn<0>(mode), kThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, search_fn<1>(mode), kThreads, smem);
     return b0 < b1 ? b0 : b1;
 }
 
