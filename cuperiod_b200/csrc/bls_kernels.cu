@@ -838,22 +838,31 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
                 }
             }
 
-            // One weight per curve: a cheaper screen in front of `screen`.  With
-            // counts exact in FP32, den = c (N - c) (times N - c for the
-            // likelihood) and th = Et - t bounds |t_exact| for every dip
-            // (t_exact < 0 and |t - t_exact| <= Et), so a box failing
-            // th |th| >= thr den cannot be the best; `screen` then repeats its
-            // own test on the few that pass.  The threshold is shared by the
-            // CTA's warps through s.thr_bits (non-negative floats order as
-            // their bits), each value a lower bound of a box some lane keeps.
-            if (MODE == MODE_UNIFORM) {
+            // A cheaper screen in front of `screen`: th = Et - t bounds |t_exact|
+            // for every dip (t_exact < 0 and |t - t_exact| <= Et), and den is a
+            // lower bound of the box's exact denominator -- with one weight the
+            // counts are exact in FP32 and den = c (N - c) (times N - c for the
+            // likelihood); with per-point weights each side is lowered by the
+            // weights' FP32 error Ei.  So a box failing th |th| >= thr den cannot
+            // be the best; `screen` repeats its own test on the few that pass
+            // (and decides, exactly, whether a box with den = 0 is empty).  The
+            // threshold is shared by the CTA's warps through s.thr_bits
+            // (non-negative floats order as their bits), each value a lower bound
+            // of a box some lane keeps.
+            {
                 auto quick = [&](float2 av, float2 bv) -> bool {
                     const float t = bv.x - av.x;
-                    const float c = bv.y - av.y;
-                    const float oc = Wt - c;
-                    const float den = OBJ ? c * oc * oc : c * oc;
                     const float th = Et - t;
-                    return (den > 0.0f) & (th * fabsf(th) >= thr * den);
+                    const float c = bv.y - av.y;
+                    if (MODE == MODE_UNIFORM) {
+                        const float oc = Wt - c;
+                        const float den = OBJ ? c * oc * oc : c * oc;
+                        return (den > 0.0f) & (th * fabsf(th) >= thr * den);
+                    } else {
+                        const float il = fmaxf(c - Ei, 0.0f), ol = fmaxf(Wt - c - Ei, 0.0f);
+                        const float den = OBJ ? il * ol * ol : il * ol;
+                        return (th >= 0.0f) & ((den <= 0.0f) | (th * fabsf(th) >= thr * den));
+                    }
                 };
                 // Starts outer: each lane's two start records (n, n + kThreads) load
                 // once per chunk; widths inner in groups of four (one broadcast
@@ -909,33 +918,6 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
                                             warp_max(has ? lb * (1.0f - 2.0f * kRel) : -1.0f));
                                 if (lane == 0) atomicMax(&s.thr_bits, __float_as_uint(thr));
                             }
-                        }
-                    }
-                }
-            } else
-            for (int di = 0; di < n_dur; ++di) {
-                const int d = s.dur[di];
-                if (d >= nb) continue;
-                const int nmax = nb - d;
-                const uint32_t d8 = (uint32_t)d * 8u;
-                // starts past nmax read sentinel records (at most 2 x kThreads + 31
-                // past it, inside the padding) and fail the screen
-                uint32_t sa = scr_s + (uint32_t)(warp * 32 + lane) * 8u;
-                for (int n0 = warp * 32; n0 <= nmax; n0 += 2 * kThreads, sa += 2u * kThreads * 8u) {
-                    const int n1 = n0 + lane, n2 = n1 + kThreads;
-                    const float2 a1 = ld_f2(sa), b1 = ld_f2(sa + d8);
-                    const float2 a2 = ld_f2(sa + kThreads * 8u), b2 = ld_f2(sa + kThreads * 8u + d8);
-                    float t1, l1, h1, t2, l2, h2;
-                    bool v1, v2;
-                    const bool c1 = screen(a1, b1, n1, d, t1, l1, h1, v1);
-                    const bool c2 = screen(a2, b2, n2, d, t2, l2, h2, v2);
-                    if (__any_sync(kFull, c1 | c2)) {
-                        bool upd = false;
-                        if (c1 && n1 <= nmax) upd |= consider(n1, di, d, t1, l1, h1, v1);
-                        if (c2 && n2 <= nmax) upd |= consider(n2, di, d, t2, l2, h2, v2);
-                        if (__any_sync(kFull, upd)) {
-                            thr = fmaxf(thr, warp_max(has ? lb * (1.0f - 2.0f * kRel) : -1.0f));
-                            if (lane == 0) atomicMax(&s.thr_bits, __float_as_uint(thr));
                         }
                     }
                 }
