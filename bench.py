@@ -47,7 +47,7 @@ WORKLOAD = ("batched plain full-grid BLS: 4096 curves, N~U[500,20000], 27 d at 2
 # over the first 256 curves of this workload, from one ncu capture
 # (profiles/bls_search_kernel_launches_256curves.txt); a launch's traffic grows in
 # proportion to its curves (points in, 7 fields x periods out)
-TRAFFIC_256 = 69814784 + 680514560
+TRAFFIC_256 = 65201408 + 679578368
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
