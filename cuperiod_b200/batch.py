@@ -94,6 +94,7 @@ def batch_periodograms(inputs: Iterable[tuple[str, Any]], method: str = "BLS", *
     eng = engine or _lib.default_engine()
     summary = BatchSummary()
     groups: dict[str, tuple[GridSpec, list[tuple[str, Any]]]] = {}
+    fixed_key = _grid_key(grid) if grid is not None else None     # one grid: hash it once
     for key, data in inputs:
         try:
             lc = to_input(data, domain=domain)
@@ -113,7 +114,7 @@ def batch_periodograms(inputs: Iterable[tuple[str, Any]], method: str = "BLS", *
         except (CuPeriodError, ValueError) as exc:
             summary.errors[str(key)] = f"{type(exc).__name__}: {exc}"
             continue
-        gk = _grid_key(g)
+        gk = fixed_key if fixed_key is not None else _grid_key(g)
         groups.setdefault(gk, (g, []))[1].append((str(key), lc))
     for g, members in groups.values():
         for start in range(0, len(members), chunk_size):

@@ -968,8 +968,8 @@ int bls_download_rows(BlsEngine* e, int32_t n_best, int32_t harmonic_max,
     int64_t* didx = reinterpret_cast<int64_t*>(db + in_bytes);
     double* dfld = reinterpret_cast<double*>(db + in_bytes + idx_bytes);
     int32_t* dcnt = reinterpret_cast<int32_t*>(db + in_bytes + idx_bytes + fld_bytes);
-    CUDA_TRY(launch_rows(e->d_out.as<double>(), (int64_t)nc * P, nc, P, e->args[0].period, dsep,
-                         dtol, n_best, harmonic_max, dcnt, didx, dfld, st),
+    CUDA_TRY(launch_rows(e->d_out.as<double>(), (int64_t)nc * P, nc, P, e->args[0].period,
+                         e->args[0].freq, dsep, dtol, n_best, harmonic_max, dcnt, didx, dfld, st),
              "peak search launch");
     CUDA_TRY(cudaMemcpyAsync(hb + in_bytes, db + in_bytes, out_bytes, cudaMemcpyDeviceToHost, st),
              "download rows");

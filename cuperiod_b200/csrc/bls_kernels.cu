@@ -31,6 +31,7 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include <cfloat>
 #include <mutex>
 
 #include "bls_device.h"
@@ -1036,6 +1037,56 @@ __device__ bool alias_related(double fn, double fc, double tol, int hmax, double
     return false;
 }
 
+// The alias test of candidates fn against one chosen peak fc, both directions,
+// with fc's multiples, subharmonics and offsets computed once per round.  The
+// only division per candidate, fn / m in the reverse subharmonic test, is taken
+// as fn * (1/m) unless the comparison is within a few ulps of the tolerance,
+// where the IEEE quotient decides as in the reference.
+struct AliasRound {
+    static constexpr int kMaxH = 32;
+    double fc, tol, sep;
+    int hmax;
+    double mfc[kMaxH + 1], mtol[kMaxH + 1], fcm[kMaxH + 1];
+    double lo[5], hi[5], off[5];
+
+    __device__ void init(double f, double t, double s, int h, const double* offs) {
+        fc = f; tol = t; sep = s; hmax = h;
+        for (int m = 2; m <= h; ++m) {
+            const double md = (double)m;
+            mfc[m] = __dmul_rn(md, f);
+            mtol[m] = __dmul_rn(md, t);
+            fcm[m] = __ddiv_rn(f, md);
+        }
+        for (int k = 0; k < 5; ++k) {
+            off[k] = offs[k];
+            lo[k] = fabs(__dsub_rn(f, offs[k]));
+            hi[k] = __dadd_rn(f, offs[k]);
+        }
+    }
+    // is_alias_related(fn, fc) or is_alias_related(fc, fn)
+    __device__ bool related(double fn) const {
+        if (fabs(__dsub_rn(fn, fc)) < sep) return true;          // either way
+        for (int m = 2; m <= hmax; ++m) {
+            const double md = (double)m;
+            if (fabs(__dsub_rn(fn, mfc[m])) < mtol[m]) return true;
+            if (fabs(__dsub_rn(fn, fcm[m])) < tol) return true;
+            if (fabs(__dsub_rn(fc, __dmul_rn(md, fn))) < mtol[m]) return true;
+            double q = __dmul_rn(fn, __drcp_rn(md));
+            const double gap = fabs(__dsub_rn(fc, q));
+            if (fabs(gap - tol) <= 8.0 * DBL_EPSILON * fmax(fabs(fc), fmax(fabs(q), tol)))
+                q = __ddiv_rn(fn, md);
+            if (fabs(__dsub_rn(fc, q)) < tol) return true;
+        }
+        for (int k = 0; k < 5; ++k) {
+            if (fabs(__dsub_rn(fn, lo[k])) < tol || fabs(__dsub_rn(fn, hi[k])) < tol) return true;
+            if (fabs(__dsub_rn(fc, fabs(__dsub_rn(fn, off[k])))) < tol ||
+                fabs(__dsub_rn(fc, __dadd_rn(fn, off[k]))) < tol)
+                return true;
+        }
+        return false;
+    }
+};
+
 // Position of grid index j among the reference's candidates: interior maxima in
 // ascending frequency, then the lowest-frequency point, then the highest.  Among
 // equal scores the later position ranks first (a stable ascending sort, reversed).
@@ -1048,7 +1099,8 @@ __device__ __forceinline__ long long cand_pos(long long j, long long P) {
 
 __global__ void __launch_bounds__(kThreads) rows_kernel(
     const double* __restrict__ out, int64_t out_stride, int64_t P,
-    const double* __restrict__ period, const double* __restrict__ sep_c,
+    const double* __restrict__ period, const double* __restrict__ freq,
+    const double* __restrict__ sep_c,
     const double* __restrict__ tol_c, int n_best, int hmax, int32_t* n_peaks,
     int64_t* index, double* fields) {
     extern __shared__ uint32_t cand[];                   // ceil(P / 32) words
@@ -1058,6 +1110,7 @@ __global__ void __launch_bounds__(kThreads) rows_kernel(
     __shared__ long long red_j[kWarps];
     __shared__ double s_mean, s_std;
     __shared__ long long s_win;
+    __shared__ AliasRound s_alias;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int c = blockIdx.x;
     const double* pw = out + (int64_t)c * P;             // field 0 (power) of curve c
@@ -1150,7 +1203,7 @@ __global__ void __launch_bounds__(kThreads) rows_kernel(
                 }
             s_win = bj;
             if (bj >= 0) {
-                const double f = __ddiv_rn(1.0, period[bj]);
+                const double f = freq[bj];
                 const double v = nan_to_zero(pw[bj]);
                 double* fo = fields + ((int64_t)c * n_best + r) * 8;
                 fo[0] = __ddiv_rn(1.0, f);                          // period = 1 / frequency
@@ -1169,16 +1222,21 @@ __global__ void __launch_bounds__(kThreads) rows_kernel(
         if (win < 0) break;
         ++count;
         // drop the winner and every candidate alias-related to it, either way
-        const double fc = __ddiv_rn(1.0, period[win]);
+        const double fc = freq[win];                  // RN(1/P), numpy's 1.0 / period
+        const bool fast = hmax <= AliasRound::kMaxH;
+        if (fast && tid == 0) s_alias.init(fc, tol, sep, hmax, offs);
+        __syncthreads();
         for (int64_t w = tid; w < nw; w += kThreads) {
             uint32_t bits = cand[w], keep = bits;
             while (bits) {
                 const int b = __ffs(bits) - 1;
                 bits &= bits - 1u;
                 const long long j = w * 32 + b;
-                const double fn = __ddiv_rn(1.0, period[j]);
-                if (j == win || alias_related(fn, fc, tol, hmax, sep, offs) ||
-                    alias_related(fc, fn, tol, hmax, sep, offs))
+                const double fn = freq[j];
+                if (j == win ||
+                    (fast ? s_alias.related(fn)
+                          : alias_related(fn, fc, tol, hmax, sep, offs) ||
+                                alias_related(fc, fn, tol, hmax, sep, offs)))
                     keep &= ~(1u << b);
             }
             cand[w] = keep;
@@ -1307,16 +1365,17 @@ cudaError_t launch_best(const double* power, int n_curves, int64_t n_periods, in
 }
 
 cudaError_t launch_rows(const double* out, int64_t out_stride, int n_curves, int64_t n_periods,
-                        const double* period, const double* sep, const double* tol, int n_best,
-                        int harmonic_max, int32_t* n_peaks, int64_t* index, double* fields,
-                        cudaStream_t stream) {
+                        const double* period, const double* freq, const double* sep,
+                        const double* tol, int n_best, int harmonic_max, int32_t* n_peaks,
+                        int64_t* index, double* fields, cudaStream_t stream) {
     if (n_curves <= 0) return cudaSuccess;
     const size_t smem = sizeof(uint32_t) * (size_t)((n_periods + 31) / 32);
     cudaError_t e = cudaFuncSetAttribute(rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    rows_kernel<<<n_curves, kThreads, smem, stream>>>(out, out_stride, n_periods, period, sep, tol,
-                                                      n_best, harmonic_max, n_peaks, index, fields);
+    rows_kernel<<<n_curves, kThreads, smem, stream>>>(out, out_stride, n_periods, period, freq,
+                                                      sep, tol, n_best, harmonic_max, n_peaks,
+                                                      index, fields);
     return cudaGetLastError();
 }
 

@@ -43,9 +43,9 @@ cudaError_t static_scratch_address(int device, void** ptr);
 // spectrum (grid index and 8 fields each: period, frequency, power, depth,
 // depth_snr, duration, t0, sde) and their count.
 cudaError_t launch_rows(const double* out, int64_t out_stride, int n_curves, int64_t n_periods,
-                        const double* period, const double* sep, const double* tol, int n_best,
-                        int harmonic_max, int32_t* n_peaks, int64_t* index, double* fields,
-                        cudaStream_t stream);
+                        const double* period, const double* freq, const double* sep,
+                        const double* tol, int n_best, int harmonic_max, int32_t* n_peaks,
+                        int64_t* index, double* fields, cudaStream_t stream);
 
 // Bytes of one period's histogram in the kernel's layout.
 size_t period_hist_bytes(int mode, int hl);
