@@ -13,9 +13,10 @@ from __future__ import annotations
 from .api import periodogram, to_input
 from .batch import BatchSummary, batch_periodograms, periodogram_to_row
 from .bls import BLSMethod, get_method, register
+from .columns import ColumnMap
 from .core import BLSPower, bls_power, bls_power_many, bls_power_segments
-from .errors import (BackendUnavailableError, CuPeriodError, EngineError, GridTooLargeError,
-                     InsufficientDataError, UnknownMethodError)
+from .errors import (BackendUnavailableError, ColumnResolutionError, CuPeriodError, EngineError,
+                     GridTooLargeError, InsufficientDataError, UnknownMethodError)
 from .grid import GridSpec, check_grid_size, log_period_grid
 from .lightcurve import Domain, LightCurve, MultiBandLightCurve
 from .multiband import bls_multiband_power
@@ -26,6 +27,7 @@ __version__ = "0.1.0"
 
 __all__ = [
     "BLSMethod", "BLSPower", "BLSSettings", "BackendUnavailableError", "BatchSummary",
+    "ColumnMap", "ColumnResolutionError",
     "CuPeriodError", "Domain", "EngineError", "GridSpec", "GridTooLargeError",
     "InsufficientDataError", "LightCurve", "MultiBandLightCurve", "Peak", "Periodogram", "UnknownMethodError",
     "batch_periodograms", "bls_multiband_power", "bls_power", "bls_power_many", "bls_power_segments",

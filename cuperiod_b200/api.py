@@ -14,29 +14,58 @@ from .result import Periodogram
 from .settings import BLSSettings
 
 
-def to_input(data: Any, *, domain: Domain | str | None = None) -> LightCurve | MultiBandLightCurve:
-    """A ``LightCurve`` from a LightCurve or a ``(t, y[, dy])`` tuple; a bare tuple
-    is read as magnitudes unless ``domain`` says otherwise.  A MultiBandLightCurve,
-    or a ``{band: LightCurve or (t, y[, dy])}`` mapping, gives a
-    MultiBandLightCurve (api.py:47-106)."""
-    if isinstance(data, MultiBandLightCurve):
-        if domain is None:
-            return data
-        return MultiBandLightCurve({k: to_input(lc, domain=domain) for k, lc in data.bands.items()},
-                                   data.meta)
-    if isinstance(data, Mapping):
-        return MultiBandLightCurve.from_light_curves(
-            {str(k): to_input(v, domain=domain) for k, v in data.items()})
+def _looks_like_arrays(data: Any) -> bool:
+    return isinstance(data, (tuple, list)) and len(data) in (2, 3) and all(
+        np.ndim(x) == 1 for x in data)
+
+
+def _check_bands(bands: Mapping[str, Any], domain: Domain | None) -> None:
+    """Every band a LightCurve, all in one domain unless ``domain`` converts them
+    (api.py:134-158)."""
+    for name, lc in bands.items():
+        if not isinstance(lc, LightCurve):
+            raise TypeError(f"band {name!r} is a {type(lc).__name__}, not a LightCurve")
+    if domain is None and len({lc.domain for lc in bands.values()}) > 1:
+        raise ValueError("bands are in different brightness domains; pass domain='magnitude' "
+                         "or domain='flux' to convert them all")
+
+
+def to_input(data: Any, *, columns: Any = None,
+             domain: Domain | str | None = None) -> LightCurve | MultiBandLightCurve:
+    """A LightCurve or MultiBandLightCurve from a user input (api.py:47-131): a
+    LightCurve/MultiBandLightCurve (converted when ``domain`` is given), a
+    ``(t, y[, dy])`` tuple (magnitudes unless ``domain`` says otherwise), a
+    ``{band: LightCurve}`` mapping, or a pandas/pyarrow/``{column: array}`` table
+    read with column detection -- split into bands when ``columns`` names a band
+    column."""
+    dom = None if domain is None else Domain(domain)
     if isinstance(data, LightCurve):
-        return data if domain is None else LightCurve(data.time, data.value, data.error,
-                                                      Domain(domain), data.meta)
-    if isinstance(data, (tuple, list)) and len(data) in (2, 3):
+        return data if dom is None else data.in_domain(dom)
+    if isinstance(data, MultiBandLightCurve):
+        _check_bands(data.bands, dom)
+        if dom is None:
+            return data
+        return MultiBandLightCurve({k: lc.in_domain(dom) for k, lc in data.bands.items()},
+                                   data.meta)
+    if _looks_like_arrays(data):
         t, y = data[0], data[1]
         dy = data[2] if len(data) == 3 else None
         return LightCurve.from_arrays(np.asarray(t), np.asarray(y),
                                       None if dy is None else np.asarray(dy),
-                                      domain=Domain(domain) if domain else Domain.MAGNITUDE)
-    raise TypeError("expected a LightCurve or a (t, y[, dy]) tuple")
+                                      domain=dom or Domain.MAGNITUDE)
+    band_split = columns is not None and getattr(columns, "band", None) is not None
+    if isinstance(data, Mapping):
+        values = list(data.values())
+        if values and all(isinstance(v, LightCurve) for v in values):
+            _check_bands(data, dom)
+            bands = data if dom is None else {k: lc.in_domain(dom) for k, lc in data.items()}
+            return MultiBandLightCurve.from_light_curves({str(k): v for k, v in bands.items()})
+    if band_split:
+        return MultiBandLightCurve.from_dataframe(data, columns=columns, domain=dom)
+    if isinstance(data, Mapping) or hasattr(data, "columns") or hasattr(data, "column_names"):
+        return LightCurve.from_dataframe(data, columns=columns, domain=dom)
+    raise TypeError("expected a LightCurve, a MultiBandLightCurve, a (t, y[, dy]) tuple, a "
+                    "{band: LightCurve} mapping or a table")
 
 
 def _settings(settings: Any) -> BLSSettings:
@@ -53,13 +82,13 @@ def _settings(settings: Any) -> BLSSettings:
 
 
 def periodogram(data: Any, method: str = "BLS", *, backend: str | None = "auto",
-                grid: GridSpec | None = None, settings: Any = None,
+                grid: GridSpec | None = None, settings: Any = None, columns: Any = None,
                 domain: Domain | str | None = None, engine=None) -> Periodogram:
     """The BLS periodogram of one light curve (api.py:204-307): flux domain
     (magnitudes converted), the default grid unless ``grid`` is given, peak
     defaults from the settings."""
     m = get_method(method)
-    lc = to_input(data, domain=domain)
+    lc = to_input(data, columns=columns, domain=domain)
     s = _settings(settings)
     m.resolve_backend(backend if backend not in (None, "auto") else s.backend)
     if isinstance(lc, MultiBandLightCurve):

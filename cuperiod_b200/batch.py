@@ -76,18 +76,96 @@ def _grid_key(grid: GridSpec) -> str:
     return h.hexdigest()
 
 
-def batch_periodograms(inputs: Iterable[tuple[str, Any]], method: str = "BLS", *,
+_TABLE_SUFFIXES = (".csv", ".ecsv", ".tsv", ".tab", ".dat", ".txt", ".parquet", ".pq")
+
+
+def _unique_keys(items: list[tuple[str, Any]]) -> list[tuple[str, Any]]:
+    """Repeated keys keep the first and get #2, #3, ... (io.py:147-193)."""
+    seen: dict[str, int] = {}
+    out = []
+    for key, src in items:
+        k = str(key)
+        n = seen.get(k, 0) + 1
+        seen[k] = n
+        out.append((k if n == 1 else f"{k}#{n}", src))
+    return out
+
+
+def resolve_inputs(inputs: Any, *, columns: Any = None, domain: Any = None,
+                   band_column: str | None = None) -> list[tuple[str, Any]]:
+    """``(key, source)`` pairs from ``(key, data)`` pairs, light curves, a
+    ``(DataFrame, group_column)`` tuple, or files (a path, a directory or a glob),
+    keyed by file stem (io.py:147-224)."""
+    import glob
+    import os
+    from pathlib import Path
+
+    from .lightcurve import LightCurve as _LC
+    if isinstance(inputs, tuple) and len(inputs) == 2 and hasattr(inputs[0], "groupby"):
+        df, group_col = inputs
+        multiband = band_column is not None or (columns is not None and
+                                                getattr(columns, "band", None) is not None)
+        items = []
+        for key, sub in df.groupby(group_col, sort=False):
+            lc = (MultiBandLightCurve.from_dataframe(sub, band_column=band_column,
+                                                     columns=columns, domain=domain)
+                  if multiband else _LC.from_dataframe(sub, columns=columns, domain=domain))
+            items.append((str(key), lc))
+        return _unique_keys(items)
+    if isinstance(inputs, (str, os.PathLike)):
+        p = Path(inputs)
+        if p.is_dir():
+            paths = sorted(q for q in p.iterdir() if q.is_file() and any(
+                str(q).lower().endswith(sfx) or str(q).lower().endswith(sfx + z)
+                for sfx in _TABLE_SUFFIXES for z in ("", ".gz", ".bz2", ".xz")))
+        elif p.exists():
+            paths = [p]
+        else:
+            paths = sorted(Path(x) for x in glob.glob(str(inputs)))
+            if not paths:
+                raise FileNotFoundError(f"no light-curve files match {str(inputs)!r}")
+        return _unique_keys([(q.name.split(".")[0], q) for q in paths])
+    items = []
+    for i, entry in enumerate(inputs):
+        if isinstance(entry, tuple) and len(entry) == 2 and isinstance(entry[0], (str, int)):
+            items.append((str(entry[0]), entry[1]))
+        elif isinstance(entry, (str, os.PathLike)):
+            items.append((Path(entry).name.split(".")[0], Path(entry)))
+        else:
+            meta = getattr(entry, "meta", {}) or {}
+            items.append((str(meta.get("id", i)), entry))
+    return _unique_keys(items)
+
+
+def _load(src: Any, columns: Any, domain: Any, band_column: str | None) -> Any:
+    """A path's light curve (split on a band column when one is named)."""
+    import os
+
+    from .lightcurve import LightCurve as _LC
+    if isinstance(src, (str, os.PathLike)):
+        if band_column is not None or (columns is not None and
+                                       getattr(columns, "band", None) is not None):
+            return MultiBandLightCurve.from_file(src, band_column=band_column, columns=columns,
+                                                 domain=domain)
+        return _LC.from_file(src, columns=columns, domain=domain)
+    return src
+
+
+def batch_periodograms(inputs: Any, method: str = "BLS", *,
                        grid: GridSpec | None = None, settings: Any = None,
-                       domain: Domain | str | None = None, n_best: int = 10,
+                       columns: Any = None, domain: Domain | str | None = None,
+                       band_column: str | None = None, n_best: int = 10,
                        chunk_size: int = 4096, sink: str | None = None,
                        engine: _lib.Engine | None = None) -> BatchSummary:
     """Search many light curves; one engine launch per chunk of curves that share
     a trial grid (the explicit ``grid``, or curves whose default grids coincide).
 
-    ``inputs`` yields ``(key, data)`` with ``data`` a LightCurve or a
-    ``(t, y[, dy])`` tuple.  A curve that cannot be searched (too few points,
-    no baseline) is recorded in ``errors`` like the reference's per-curve
-    failures (runner.py:248-249).  ``sink``: optional Parquet path for the rows.
+    ``inputs``: ``(key, data)`` pairs (``data`` a LightCurve, MultiBandLightCurve,
+    ``(t, y[, dy])`` tuple or table), light curves, files (a path, a directory, a
+    glob) or a ``(DataFrame, group_column)`` tuple (``resolve_inputs``).  A curve
+    that cannot be searched (too few points, no baseline, unreadable) is recorded
+    in ``errors`` like the reference's per-curve failures (runner.py:248-249).
+    ``sink``: optional Parquet path for the rows.
     """
     m = get_method(method)
     s = _settings(settings)
@@ -95,9 +173,11 @@ def batch_periodograms(inputs: Iterable[tuple[str, Any]], method: str = "BLS", *
     summary = BatchSummary()
     groups: dict[str, tuple[GridSpec, list[tuple[str, Any]]]] = {}
     fixed_key = _grid_key(grid) if grid is not None else None     # one grid: hash it once
-    for key, data in inputs:
+    for key, data in resolve_inputs(inputs, columns=columns, domain=domain,
+                                    band_column=band_column):
         try:
-            lc = to_input(data, domain=domain)
+            data = _load(data, columns, domain, band_column)
+            lc = to_input(data, columns=columns, domain=domain)
             if isinstance(lc, MultiBandLightCurve):
                 # one star's bands: one launch of its own, peaks ranked on the host
                 from .multiband import multiband_default_grid
@@ -111,7 +191,7 @@ def batch_periodograms(inputs: Iterable[tuple[str, Any]], method: str = "BLS", *
                 continue
             lc = lc.in_domain(m.natural_domain)
             g = grid or m.default_grid(lc, s)
-        except (CuPeriodError, ValueError) as exc:
+        except (CuPeriodError, ValueError, OSError) as exc:
             summary.errors[str(key)] = f"{type(exc).__name__}: {exc}"
             continue
         gk = fixed_key if fixed_key is not None else _grid_key(g)
@@ -142,4 +222,5 @@ def batch_periodograms(inputs: Iterable[tuple[str, Any]], method: str = "BLS", *
     return summary
 
 
-__all__ = ["BatchSummary", "PEAK_EXTRA_COLUMNS", "batch_periodograms", "periodogram_to_row"]
+__all__ = ["BatchSummary", "PEAK_EXTRA_COLUMNS", "batch_periodograms", "periodogram_to_row",
+           "resolve_inputs"]

@@ -25,12 +25,17 @@ class UnknownMethodError(CuPeriodError, KeyError):
     """A method name that is not registered."""
 
 
+class ColumnResolutionError(CuPeriodError, ValueError):
+    """A light-curve table's time, value or band column could not be resolved."""
+
+
 class EngineError(CuPeriodError, RuntimeError):
     """The CUDA engine failed at run time (a CUDA error or a device-side check)."""
 
 
 __all__ = [
     "BackendUnavailableError",
+    "ColumnResolutionError",
     "CuPeriodError",
     "EngineError",
     "GridTooLargeError",

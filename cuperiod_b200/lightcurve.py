@@ -47,6 +47,47 @@ class LightCurve:
                     meta: Mapping[str, Any] | None = None) -> "LightCurve":
         return cls(time, value, error, Domain(domain), dict(meta or {}))
 
+    @classmethod
+    def from_dataframe(cls, df: Any, *, columns: Any = None, domain: Domain | str | None = None,
+                       meta: Mapping[str, Any] | None = None) -> "LightCurve":
+        """From a pandas/pyarrow/``{column: array}`` table with column detection
+        (lightcurve.py:143-158)."""
+        from .tables import adapt_table
+        names, getter = adapt_table(df)
+        return cls._from_table(names, getter, columns, domain, meta)
+
+    @classmethod
+    def from_file(cls, path: Any, *, columns: Any = None, domain: Domain | str | None = None,
+                  meta: Mapping[str, Any] | None = None) -> "LightCurve":
+        """From a CSV/TSV/ECSV/text/Parquet file with column detection; the
+        format follows the extension (lightcurve.py:160-176)."""
+        from .tables import adapt_table, read_table_object
+        names, getter = adapt_table(read_table_object(path))
+        return cls._from_table(names, getter, columns, domain,
+                               {"source": str(path), **dict(meta or {})})
+
+    @classmethod
+    def _from_table(cls, names, getter, columns, domain, meta) -> "LightCurve":
+        import warnings
+        from .columns import ColumnMap
+        from .tables import band_codes
+        resolved = (columns or ColumnMap()).resolve(names, domain=domain)
+        if resolved.band is not None:
+            _, labels = band_codes(getter(resolved.band))
+            if len(labels) > 1:
+                warnings.warn(f"band column {resolved.band!r} holds {len(labels)} bands that "
+                              "are pooled into one light curve; read the table as a "
+                              "MultiBandLightCurve to keep them apart", UserWarning,
+                              stacklevel=3)
+        return cls._from_resolved(getter, resolved, meta)
+
+    @classmethod
+    def _from_resolved(cls, getter, resolved, meta) -> "LightCurve":
+        from .tables import as_float
+        return cls(as_float(getter(resolved.time)), as_float(getter(resolved.value)),
+                   None if resolved.error is None else as_float(getter(resolved.error)),
+                   resolved.domain, dict(meta or {}))
+
     @property
     def n(self) -> int:
         return int(self.time.size)
@@ -113,6 +154,61 @@ class MultiBandLightCurve:
     def from_light_curves(cls, bands: Mapping[str, LightCurve], *,
                           meta: Mapping[str, Any] | None = None) -> "MultiBandLightCurve":
         return cls(dict(bands), dict(meta or {}))
+
+    @classmethod
+    def from_dataframe(cls, df: Any, *, band_column: str | None = None, columns: Any = None,
+                       domain: Domain | str | None = None,
+                       meta: Mapping[str, Any] | None = None) -> "MultiBandLightCurve":
+        """From one long-format table split on its band column (lightcurve.py:389-425)."""
+        return cls._from_table_object(df, band_column, columns, domain, meta)
+
+    @classmethod
+    def from_file(cls, path: Any, *, band_column: str | None = None, columns: Any = None,
+                  domain: Domain | str | None = None,
+                  meta: Mapping[str, Any] | None = None) -> "MultiBandLightCurve":
+        """From one long-format table file split on its band column
+        (lightcurve.py:427-463)."""
+        from .tables import read_table_object
+        return cls._from_table_object(read_table_object(path), band_column, columns, domain,
+                                      {"source": str(path), **dict(meta or {})})
+
+    @classmethod
+    def _from_table_object(cls, table, band_column, columns, domain,
+                           meta) -> "MultiBandLightCurve":
+        """Rows without a band label are dropped; each band keeps its rows' order
+        (lightcurve.py:465-518)."""
+        import dataclasses
+        import warnings
+        from .columns import ColumnMap
+        from .errors import ColumnResolutionError
+        from .tables import adapt_table, band_codes
+        names, getter = adapt_table(table)
+        cmap = columns or ColumnMap(band=band_column)
+        if band_column is not None and cmap.band is None:
+            cmap = dataclasses.replace(cmap, band=band_column)
+        resolved = cmap.resolve(names, domain=domain)
+        if resolved.band is None:
+            raise ColumnResolutionError("could not resolve a band column; pass band_column=... "
+                                        f"or ColumnMap(band=...). Available columns: {names}")
+        codes, labels = band_codes(getter(resolved.band))
+        if not labels:
+            raise ColumnResolutionError(f"band column {resolved.band!r} holds no labels")
+        missing = int(np.count_nonzero(codes < 0))
+        if missing:
+            warnings.warn(f"{missing} of {codes.size} rows have no label in band column "
+                          f"{resolved.band!r} and were dropped", UserWarning, stacklevel=3)
+        whole = LightCurve._from_resolved(getter, resolved, None)
+        order = np.argsort(codes, kind="stable")
+        bounds = np.searchsorted(codes[order], np.arange(len(labels) + 1))
+        time, value = whole.time[order], whole.value[order]
+        error = None if whole.error is None else whole.error[order]
+        bands = {}
+        for k, label in enumerate(labels):
+            rows = slice(int(bounds[k]), int(bounds[k + 1]))
+            bands[label] = LightCurve(time[rows], value[rows],
+                                      None if error is None else error[rows], whole.domain,
+                                      {"band": label})
+        return cls(bands, dict(meta or {}))
 
     @property
     def band_names(self) -> tuple[str, ...]:
