@@ -197,3 +197,149 @@ int bls_oracle_search(const double* tau, const double* yw, const double* wv, int
     for (int i = 0; i < started; ++i) pthread_join(th[i], NULL);
     return atomic_load(&a.failed) ? 2 : 0;
 }
+
+/* ---- joint multi-band search ------------------------------------------------
+ * The joint-ephemeris sweep of src/cuperiod/multiband/_bls_joint.py:412-507: the
+ * bands of one star (points of band k in [starts[k], starts[k+1]), one time
+ * origin) are folded and binned each on its own, padded and accumulated over the
+ * full width, and one box (d, n) is scored by the sum over bands, in band order,
+ * of depth^2 / (1/iv_in + 1/iv_out) (obj 0) or 0.5 * iv_in * depth^2 (obj 1) of
+ * the bands that are admissible there and have yout >= yin; the first box in
+ * (duration, start) order with the largest strictly-improving total wins.
+ * Outputs per period: the box (start n, width d in bins), whether one was found,
+ * and each band's y_in and iv_in at it (n_bands x n_periods, band-major). */
+typedef struct {
+    const double *tau, *yw, *wv, *sum_y, *sum_ivar, *floors, *periods;
+    const int64_t *starts, *dur_bins;
+    int64_t n_bands, n_periods, n_dur, oversample, width;
+    double bin_duration;
+    int obj_flag;
+    int64_t *out_n, *out_d;
+    uint8_t* out_found;
+    double *out_yin, *out_ivin;
+    atomic_long next;
+    atomic_int failed;
+} joint_args;
+
+static void joint_period(const joint_args* a, int64_t pidx, double* my, double* mi)
+{
+    const int64_t K = a->n_bands, width = a->width;
+    const double period = a->periods[pidx];
+    const int64_t n_bins = period_bins(period, a->bin_duration, a->oversample, width);
+    for (int64_t k = 0; k < K; ++k) {
+        double* y = my + k * width;
+        double* w = mi + k * width;
+        memset(y, 0, sizeof(double) * (size_t)width);
+        memset(w, 0, sizeof(double) * (size_t)width);
+        for (int64_t j = a->starts[k]; j < a->starts[k + 1]; ++j) {
+            const int64_t ind = fold_bin(a->tau[j], period, a->bin_duration, width);
+            y[ind] += a->yw[j];
+            w[ind] += a->wv[j];
+        }
+        for (int64_t o = 0; o < a->oversample; ++o) {
+            int64_t dst = n_bins - a->oversample + o;
+            if (dst < 0) dst = 0;
+            else if (dst > width - 1) dst = width - 1;
+            y[dst] = y[1 + o];
+            w[dst] = w[1 + o];
+        }
+        double ay = 0.0, ai = 0.0;
+        for (int64_t i = 0; i < width; ++i) {
+            ay += y[i];
+            y[i] = ay;
+            ai += w[i];
+            w[i] = ai;
+        }
+    }
+    double best = -INFINITY;
+    int64_t bn = 0, bd = 0;
+    for (int64_t di = 0; di < a->n_dur; ++di) {
+        const int64_t d = a->dur_bins[di];
+        if (d >= width || d >= n_bins) continue;
+        for (int64_t n = 0; n <= n_bins - d; ++n) {
+            double total = 0.0;
+            int hit = 0;
+            for (int64_t k = 0; k < K; ++k) {
+                const double* y = my + k * width;
+                const double* w = mi + k * width;
+                const double y_in = y[n + d] - y[n];
+                const double iv_in = w[n + d] - w[n];
+                const double iv_out = a->sum_ivar[k] - iv_in;
+                if (iv_in < a->floors[k] || iv_out < a->floors[k]) continue;
+                const double yin = y_in / iv_in;
+                const double yout = (a->sum_y[k] - y_in) / iv_out;
+                if (!(yout >= yin)) continue;
+                const double depth = yout - yin;
+                hit = 1;
+                if (a->obj_flag == 0) total += depth * depth / (1.0 / iv_in + 1.0 / iv_out);
+                else total += 0.5 * iv_in * depth * depth;
+            }
+            if (hit && total > best) {
+                best = total;
+                bn = n;
+                bd = d;
+            }
+        }
+    }
+    const int found = best > -INFINITY;
+    a->out_found[pidx] = (uint8_t)found;
+    a->out_n[pidx] = found ? bn : 0;
+    a->out_d[pidx] = found ? bd : 0;
+    for (int64_t k = 0; k < K; ++k) {
+        const double* y = my + k * width;
+        const double* w = mi + k * width;
+        a->out_yin[k * a->n_periods + pidx] = found ? y[bn + bd] - y[bn] : 0.0;
+        a->out_ivin[k * a->n_periods + pidx] = found ? w[bn + bd] - w[bn] : 0.0;
+    }
+}
+
+static void* joint_worker(void* arg)
+{
+    joint_args* a = (joint_args*)arg;
+    const size_t cells = (size_t)a->n_bands * (size_t)a->width;
+    double* my = (double*)malloc(sizeof(double) * cells);
+    double* mi = (double*)malloc(sizeof(double) * cells);
+    if (!my || !mi) {
+        atomic_store(&a->failed, 1);
+    } else {
+        for (;;) {
+            const int64_t p = atomic_fetch_add(&a->next, 1);
+            if (p >= a->n_periods) break;
+            joint_period(a, p, my, mi);
+        }
+    }
+    free(my);
+    free(mi);
+    return NULL;
+}
+
+int bls_oracle_joint(const double* tau, const double* yw, const double* wv, const int64_t* starts,
+                     int64_t n_bands, const double* sum_y, const double* sum_ivar,
+                     const double* floors, const double* periods, int64_t n_periods,
+                     const int64_t* dur_bins, int64_t n_dur, double bin_duration,
+                     int64_t oversample, int64_t width, int obj_flag, int64_t* out_n,
+                     int64_t* out_d, uint8_t* out_found, double* out_yin, double* out_ivin,
+                     int n_threads)
+{
+    if (width < 2 || n_periods < 0 || n_bands < 1) return 1;
+    joint_args a = {
+        .tau = tau, .yw = yw, .wv = wv, .sum_y = sum_y, .sum_ivar = sum_ivar, .floors = floors,
+        .periods = periods, .starts = starts, .dur_bins = dur_bins, .n_bands = n_bands,
+        .n_periods = n_periods, .n_dur = n_dur, .oversample = oversample, .width = width,
+        .bin_duration = bin_duration, .obj_flag = obj_flag, .out_n = out_n, .out_d = out_d,
+        .out_found = out_found, .out_yin = out_yin, .out_ivin = out_ivin,
+    };
+    atomic_init(&a.next, 0);
+    atomic_init(&a.failed, 0);
+    if (n_threads < 1) n_threads = 1;
+    if (n_threads > 512) n_threads = 512;
+    pthread_t th[512];
+    int started = 0;
+    for (int i = 1; i < n_threads; ++i) {
+        if (pthread_create(&th[started], NULL, joint_worker, &a) != 0) break;
+        ++started;
+    }
+    joint_worker(&a);
+    for (int i = 0; i < started; ++i) pthread_join(th[i], NULL);
+    return atomic_load(&a.failed) ? 2 : 0;
+}

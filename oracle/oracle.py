@@ -52,6 +52,9 @@ def _load() -> ctypes.CDLL:
         lib.bls_oracle_search.restype = i32
         lib.bls_oracle_fold_bins.argtypes = [p, i64, d, d, i64, p]
         lib.bls_oracle_fold_bins.restype = i32
+        lib.bls_oracle_joint.argtypes = [p, p, p, p, i64, p, p, p, p, i64, p, i64, d, i64,
+                                         i64, i32, p, p, p, p, p, i32]
+        lib.bls_oracle_joint.restype = i32
         _lib = lib
     return _lib
 
@@ -314,13 +317,15 @@ def robust_scatter(flux: np.ndarray) -> float:
     return sigma
 
 
-def multiband_power(bands, periods, meta, s: Settings, n_threads: int | None = None):
-    """``bls_multiband_power`` in its independent mode (``multiband/bls_mb.py:120-275``)
-    on finite flux-domain bands ``[(name, t, flux, err or None), ...]``: bands with
-    at least 3 points are searched over the common segments, the per-period power
-    is the sum of the squared clipped depth-SNRs and the box comes from the band
-    with the largest.  Returns ``(frequency, power, extras, used_band_names,
-    n_samples, baseline)`` in ascending frequency."""
+def multiband_power(bands, periods, meta, s: Settings, n_threads: int | None = None,
+                    ephemeris: str = "independent"):
+    """``bls_multiband_power`` (``multiband/bls_mb.py:120-315``) on finite flux-domain
+    bands ``[(name, t, flux, err or None), ...]``: bands with at least 3 points are
+    searched over the common segments.  Independent: the per-period power is the
+    sum of the squared clipped depth-SNRs and the box comes from the band with the
+    largest.  Shared: one box for all bands (``joint_power``).  Returns
+    ``(frequency, power, extras, used_band_names, n_samples, baseline)`` in
+    ascending frequency."""
     used = [b for b in bands if len(b[1]) >= 3]
     n_total = sum(len(b[1]) for b in used)
     stacked = np.concatenate([np.asarray(b[1], dtype=np.float64) for b in used])
@@ -332,21 +337,34 @@ def multiband_power(bands, periods, meta, s: Settings, n_threads: int | None = N
                   for b in used]
     parts = {k: [] for k in ("period", "power", "depth", "depth_snr", "duration", "t0",
                              "band_index")}
-    for per, dur in grid_segments(periods, meta, s):
-        seg = [bls_power(np.asarray(b[1], dtype=np.float64), np.asarray(b[2], dtype=np.float64),
-                         e, per, dur, s.bins_per_duration, objective=s.objective,
-                         n_threads=n_threads) for b, e in zip(used, errors)]
-        dsnr = np.vstack([np.clip(o["depth_snr"], 0.0, None) for o in seg])
-        combined = np.sum(dsnr ** 2, axis=0)
-        best = np.argmax(dsnr, axis=0)
-        cols = np.arange(dsnr.shape[1])
-        parts["period"].append(per)
-        parts["power"].append(combined)
-        parts["depth_snr"].append(np.sqrt(combined))
-        parts["depth"].append(np.vstack([o["depth"] for o in seg])[best, cols])
-        parts["duration"].append(np.vstack([o["duration"] for o in seg])[best, cols])
-        parts["t0"].append(np.vstack([o["transit_time"] for o in seg])[best, cols])
-        parts["band_index"].append(best.astype(np.float64))
+    segments = grid_segments(periods, meta, s)
+    if ephemeris == "shared":
+        jb = joint_bands([np.asarray(b[1], dtype=np.float64) for b in used],
+                         [np.asarray(b[2], dtype=np.float64) for b in used], errors)
+        for per, dur in segments:
+            o = joint_power(jb, per, dur, s.bins_per_duration, objective_flag(s.objective),
+                            n_threads)
+            parts["period"].append(np.asarray(per, dtype=np.float64))
+            parts["t0"].append(o.pop("transit_time"))
+            for k, v in o.items():
+                parts[k].append(v)
+    else:
+        for per, dur in segments:
+            seg = [bls_power(np.asarray(b[1], dtype=np.float64),
+                             np.asarray(b[2], dtype=np.float64), e, per, dur,
+                             s.bins_per_duration, objective=s.objective, n_threads=n_threads)
+                   for b, e in zip(used, errors)]
+            dsnr = np.vstack([np.clip(o["depth_snr"], 0.0, None) for o in seg])
+            combined = np.sum(dsnr ** 2, axis=0)
+            best = np.argmax(dsnr, axis=0)
+            cols = np.arange(dsnr.shape[1])
+            parts["period"].append(per)
+            parts["power"].append(combined)
+            parts["depth_snr"].append(np.sqrt(combined))
+            parts["depth"].append(np.vstack([o["depth"] for o in seg])[best, cols])
+            parts["duration"].append(np.vstack([o["duration"] for o in seg])[best, cols])
+            parts["t0"].append(np.vstack([o["transit_time"] for o in seg])[best, cols])
+            parts["band_index"].append(best.astype(np.float64))
     joined = {k: np.concatenate(v) for k, v in parts.items()}
     period = joined.pop("period")
     power = np.nan_to_num(joined.pop("power"), nan=0.0, posinf=0.0)
@@ -359,6 +377,120 @@ def multiband_power(bands, periods, meta, s: Settings, n_threads: int | None = N
               "band_index": joined["band_index"]}
     return (frequency[order], power[order], {k: v[order] for k, v in extras.items()},
             [b[0] for b in used], n_total, baseline)
+
+
+@dataclass
+class JointBands:
+    """``JointBands``, ``multiband/_bls_joint.py:65-91``: every band of one star with
+    one time origin, concatenated; ``starts`` delimits the bands."""
+    tau: np.ndarray
+    yw: np.ndarray
+    ivar: np.ndarray
+    starts: np.ndarray
+    sum_y: np.ndarray
+    sum_ivar: np.ndarray
+    floor: np.ndarray
+    t_min: float
+
+
+def joint_bands(times, values, errors) -> JointBands:
+    """``joint_bands``, ``multiband/_bls_joint.py:94-135``: each band centred on its
+    own median, ``yw = y_c / dy^2``, the times of all bands from the earliest."""
+    t_min = float(min(float(np.min(t)) for t in times))
+    taus, yws, ivars, sum_y, sum_ivar, floors = [], [], [], [], [], []
+    for t, y, dy in zip(times, values, errors, strict=True):
+        y_c = np.asarray(y, dtype=np.float64)
+        y_c = y_c - float(np.median(y_c))
+        ivar = 1.0 / (np.asarray(dy, dtype=np.float64) ** 2)
+        yw = y_c * ivar
+        taus.append(np.asarray(t, dtype=np.float64) - t_min)
+        yws.append(yw)
+        ivars.append(ivar)
+        sum_y.append(float(yw.sum()))
+        sum_ivar.append(float(ivar.sum()))
+        floors.append(ivar_floor(int(yw.size), sum_ivar[-1]))
+    starts = np.concatenate([[0], np.cumsum([t.size for t in taus])]).astype(np.int64)
+    return JointBands(np.ascontiguousarray(np.concatenate(taus)),
+                      np.ascontiguousarray(np.concatenate(yws)),
+                      np.ascontiguousarray(np.concatenate(ivars)), starts,
+                      np.asarray(sum_y, dtype=np.float64), np.asarray(sum_ivar, dtype=np.float64),
+                      np.asarray(floors, dtype=np.float64), t_min)
+
+
+JOINT_FIELDS = ("power", "depth", "depth_snr", "duration", "transit_time", "band_index")
+
+
+def joint_sweep(jb: JointBands, periods, durations, oversample: int, obj_flag: int,
+                n_threads: int | None = None):
+    """The numba joint sweep, ``multiband/_bls_joint.py:412-507``, on one segment:
+    ``(best_n, best_d, found, y_in[K, P], iv_in[K, P], spec)``."""
+    lib = _load()
+    spec = search_spec(periods, durations, oversample)
+    per = np.ascontiguousarray(spec.periods, dtype=np.float64)
+    db = np.ascontiguousarray(spec.dur_bins, dtype=np.int64)
+    k = int(jb.starts.size - 1)
+    out_n = np.zeros(per.size, dtype=np.int64)
+    out_d = np.zeros(per.size, dtype=np.int64)
+    found = np.zeros(per.size, dtype=np.uint8)
+    yin = np.zeros((k, per.size), dtype=np.float64)
+    ivin = np.zeros((k, per.size), dtype=np.float64)
+    floors = np.ascontiguousarray(jb.floor, dtype=np.float64)
+    if n_threads is None:
+        n_threads = os.cpu_count() or 1
+    rc = lib.bls_oracle_joint(
+        _ptr(jb.tau), _ptr(jb.yw), _ptr(jb.ivar), _ptr(jb.starts), k, _ptr(jb.sum_y),
+        _ptr(jb.sum_ivar), _ptr(floors), _ptr(per), per.size, _ptr(db), db.size,
+        float(spec.bin_duration), int(oversample), int(spec.width), int(obj_flag),
+        _ptr(out_n), _ptr(out_d), _ptr(found), _ptr(yin), _ptr(ivin), int(n_threads))
+    if rc != 0:
+        raise RuntimeError(f"oracle joint search failed ({rc})")
+    return out_n, out_d, found.astype(bool), yin, ivin, spec
+
+
+def joint_finish(jb: JointBands, y_in, iv_in, best_n, best_d, found, periods,
+                 bin_duration: float) -> dict[str, np.ndarray]:
+    """``_finish``, ``multiband/_bls_joint.py:359-404``: each band's depth and SNR at
+    the chosen box; power = sum of squared SNRs in band order, the depth of the
+    band with the largest SNR, the box's duration and mid-transit time."""
+    k_bands = int(jb.starts.size - 1)
+    n_p = int(np.asarray(periods).size)
+    snr = np.zeros((k_bands, n_p))
+    depth = np.zeros((k_bands, n_p))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for k in range(k_bands):
+            floor = float(jb.floor[k])
+            iv_out = float(jb.sum_ivar[k]) - iv_in[k]
+            ok = (iv_in[k] >= floor) & (iv_out >= floor)
+            safe_in = np.where(ok, iv_in[k], 1.0)
+            safe_out = np.where(ok, iv_out, 1.0)
+            yin = y_in[k] / safe_in
+            yout = (float(jb.sum_y[k]) - y_in[k]) / safe_out
+            dip = ok & (yout >= yin)
+            d = yout - yin
+            depth[k] = np.where(dip, d, 0.0)
+            snr[k] = np.where(dip, d / np.sqrt(1.0 / safe_in + 1.0 / safe_out), 0.0)
+    power = np.zeros(n_p)
+    for k in range(k_bands):
+        power = power + snr[k] * snr[k]
+    band = np.argmax(snr, axis=0)
+    duration = best_d.astype(np.float64) * bin_duration
+    t0 = np.remainder(best_n.astype(np.float64) * bin_duration + 0.5 * duration,
+                      periods) + jb.t_min
+    cols = np.arange(n_p)
+    return {"power": np.where(found, power, 0.0),
+            "depth": np.where(found, depth[band, cols], 0.0),
+            "depth_snr": np.where(found, np.sqrt(power), 0.0),
+            "duration": np.where(found, duration, 0.0),
+            "transit_time": np.where(found, t0, 0.0),
+            "band_index": np.where(found, band.astype(np.float64), 0.0)}
+
+
+def joint_power(jb: JointBands, periods, durations, oversample: int, obj_flag: int,
+                n_threads: int | None = None) -> dict[str, np.ndarray]:
+    """One segment of ``joint_search`` (``multiband/_bls_joint.py:151-204``)."""
+    bn, bd, found, yin, ivin, spec = joint_sweep(jb, periods, durations, oversample,
+                                                 obj_flag, n_threads)
+    return joint_finish(jb, yin, ivin, bn, bd, found, spec.periods, spec.bin_duration)
 
 
 def best_index(power: np.ndarray) -> int:

@@ -63,8 +63,9 @@ def test_oracle_multiband_on_golden(case):
     meta, z = case
     k = meta["key"]
     freq, power, extras, used, n, baseline = oracle.multiband_power(
-        multiband_inputs(meta, z), z[f"{k}_periods"], meta["grid_meta"], oracle.Settings(),
-        n_threads=4)
+        multiband_inputs(meta, z), z[f"{k}_periods"], meta["grid_meta"],
+        oracle.Settings(objective=meta["objective"]), n_threads=4,
+        ephemeris=meta["ephemeris"])
     assert used == meta["used_bands"] and n == meta["n_samples"] and baseline == meta["baseline"]
     np.testing.assert_array_equal(freq, z[f"{k}_frequency"])
     np.testing.assert_array_equal(power, z[f"{k}_power"])
