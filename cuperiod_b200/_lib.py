@@ -23,6 +23,8 @@ BLS_OK, BLS_E_INVALID, BLS_E_CUDA, BLS_E_RESOURCE, BLS_E_NOMEM, BLS_E_DEVICE, BL
 N_FIELDS = 7
 FIELD_NAMES = ("power", "depth", "depth_err", "depth_snr", "duration", "transit_time",
                "log_likelihood")
+#: Fields of the joint-ephemeris search (``JOINT_FIELDS``, multiband/_bls_joint.py:52-54).
+JOINT_FIELD_NAMES = ("power", "depth", "depth_snr", "duration", "transit_time", "band_index")
 
 _i32, _i64, _dbl, _vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
@@ -81,13 +83,14 @@ def load() -> ctypes.CDLL:
         lib.bls_download_rows.argtypes = [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp]
         lib.bls_search.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_batch_info.argtypes = [_vp, P(BlsBatchInfo)]
+        lib.bls_search_joint.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_debug_fold_bins.argtypes = [_vp, _vp, _i64, _dbl, _dbl, _i32, _vp, _vp]
         lib.bls_debug_prefix.argtypes = [_vp, _vp, _vp, _vp, _i64, _dbl, _vp, _i32, _i32, _vp, _vp,
                                          _vp]
         for name in ("bls_engine_create", "bls_engine_destroy", "bls_prepare", "bls_launch",
                      "bls_download", "bls_device_output", "bls_download_best", "bls_search",
                      "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix",
-                     "bls_launch_best_noalloc", "bls_download_rows"):
+                     "bls_launch_best_noalloc", "bls_download_rows", "bls_search_joint"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib
@@ -274,6 +277,16 @@ class Engine:
         self.prepare(grid, curves, stream)
         self.launch(stream)
         return self.download(stream)
+
+    def search_joint(self, grid: PackedGrid, bands: PackedCurves,
+                     stream: int | None = None) -> np.ndarray:
+        """The joint-ephemeris search of one star whose bands are ``bands``:
+        ``(len(JOINT_FIELD_NAMES), n_periods)`` in grid order."""
+        out = np.empty((len(JOINT_FIELD_NAMES), grid.n_periods), dtype=np.float64)
+        g, c = grid.struct(), bands.struct()
+        _check(self._lib.bls_search_joint(self._h, ctypes.byref(g), ctypes.byref(c),
+                                          out.ctypes.data, stream))
+        return out
 
     def prefix_sums(self, t, y, dy, period: float, durations, oversample: int):
         """Debug view: the device's padded cumulative sums of y*ivar and ivar over

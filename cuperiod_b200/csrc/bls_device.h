@@ -121,4 +121,57 @@ struct BatchArgs {
     int32_t obj_flag;           // 0 snr, 1 log-likelihood
 };
 
+// ---- joint-ephemeris multi-band search --------------------------------------
+// One star's bands share one box per trial period (cuPeriod
+// src/cuperiod/multiband/_bls_joint.py).  Each band's centred flux*weight and
+// weight are quantised to 64-bit fixed point with a power-of-two scale per band
+// (|sum of the band's values| < 2^62), so every bin and prefix sum is an exact
+// integer and a box's sums are exact differences.
+
+constexpr int kJointFields = 6;     // power, depth, depth_snr, duration, t0, band_index
+constexpr int kMaxJointBands = 64;
+
+struct JointBand {
+    int64_t point_off;      // first point of the band in tau / qy / qi
+    int32_t n_points;
+    int32_t pad;
+    double sum_y;           // the reference's float sums of y*ivar and ivar
+    double sum_ivar;
+    double ivar_floor;      // admissibility floor of either side of a box
+    double y_unit;          // reference units of one quantum of y*ivar (2^-e)
+    double i_unit;          // reference units of one quantum of ivar
+};
+
+struct JointSegment {
+    int64_t period_off;     // first period of the segment
+    int32_t n_periods;
+    int32_t width;          // ceil(max P / bin) + oversample + 1
+    double bin_duration;
+    int32_t dur_off;        // into dur_bins
+    int32_t n_dur;
+    int32_t oversample;
+    int32_t hist_len;       // max n_bins + 1 over the segment
+};
+
+struct JointArgs {
+    const double* tau;          // per point: t - t_min over all bands
+    const long long* qy;        // per point: quantised (y - median) * ivar
+    const long long* qi;        // per point: quantised ivar
+    const JointBand* bands;
+    const JointSegment* segments;
+    const double* period;       // per grid period
+    const int32_t* nbins;       // the reference's n_bins per period
+    const int32_t* dur_bins;    // per segment, box widths in bins (first-seen order)
+    double* out;                // kJointFields x n_periods, field-major
+    int64_t n_periods;
+    long long* scratch;         // global histograms when they exceed shared memory
+    int64_t hist_stride;        // int64 entries of one band array (max hist_len)
+    int32_t* work_counter;      // next unclaimed period
+    int32_t* error_flag;
+    double t_min;
+    int32_t n_bands;
+    int32_t n_segments;
+    int32_t obj_flag;           // 0 snr, 1 log-likelihood
+};
+
 }  // namespace blsb200

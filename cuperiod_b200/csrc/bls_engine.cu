@@ -199,9 +199,9 @@ struct BlsEngine {
 
     // device buffers
     DevBuf d_tau, d_pay_r, d_r64, d_iv64, d_period, d_freq, d_scale, d_nbins, d_dur, d_curves,
-        d_segments, d_rows, d_out, d_ctl, d_best;
+        d_segments, d_rows, d_out, d_ctl, d_best, d_joint;
     // pinned staging
-    HostBuf h_tau, h_pay_r, h_r64, h_iv64, h_grid, h_meta, h_ctl, h_best, h_rows;
+    HostBuf h_tau, h_pay_r, h_r64, h_iv64, h_grid, h_meta, h_ctl, h_best, h_rows, h_joint;
 
     // the prepared batch
     bool prepared = false;
@@ -220,10 +220,11 @@ struct BlsEngine {
     ~BlsEngine() {
         if (graph) cudaGraphExecDestroy(graph);
         for (DevBuf* b : {&d_tau, &d_pay_r, &d_r64, &d_iv64, &d_period, &d_freq, &d_scale, &d_nbins,
-                          &d_dur, &d_curves, &d_segments, &d_rows, &d_out, &d_ctl, &d_best})
+                          &d_dur, &d_curves, &d_segments, &d_rows, &d_out, &d_ctl, &d_best,
+                          &d_joint})
             b->release();
         for (HostBuf* b : {&h_tau, &h_pay_r, &h_r64, &h_iv64, &h_grid, &h_meta, &h_ctl, &h_best,
-                           &h_rows})
+                           &h_rows, &h_joint})
             b->release();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -251,6 +252,19 @@ inline int64_t point_slot(int64_t j, int64_t n) {
     if (j >= full) return j;
     const int64_t c = j / kChunk, w = j % kChunk;
     return c * kChunk + (w % kChunkPts) * kChunkThreads + w / kChunkPts;
+}
+
+// np.median of n >= 1 values: the mean of the two middle values for even n.
+double median_of(const double* y, int64_t n, std::vector<double>& scratch) {
+    scratch.assign(y, y + n);
+    const int64_t mid = n / 2;
+    std::nth_element(scratch.begin(), scratch.begin() + mid, scratch.end());
+    double med = scratch[mid];
+    if (n % 2 == 0) {
+        const double lo = *std::max_element(scratch.begin(), scratch.begin() + mid);
+        med = (lo + med) / 2.0;
+    }
+    return med;
 }
 
 // Pack one curve: the reference's host inputs, then the fixed-point words.
@@ -287,15 +301,7 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
         }
         t_min = std::min(t_min, t[j]);
     }
-    // y - median(y) (np.median: the mean of the two middle values for even n)
-    scratch.assign(y, y + n);
-    const int64_t mid = n / 2;
-    std::nth_element(scratch.begin(), scratch.begin() + mid, scratch.end());
-    double med = scratch[mid];
-    if (n % 2 == 0) {
-        const double lo = *std::max_element(scratch.begin(), scratch.begin() + mid);
-        med = (lo + med) / 2.0;
-    }
+    const double med = median_of(y, n, scratch);
     // yw, ivar (reference units); sums with numpy's pairwise order
     scratch.resize(3 * (size_t)n);
     double* yw = scratch.data();
@@ -799,6 +805,228 @@ int check_device_flag(BlsEngine* e, cudaStream_t st) {
     return BLS_OK;
 }
 
+// ---- joint-ephemeris multi-band search ----------------------------------------
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// One star's bands, prepared as joint_bands does (_bls_joint.py:94-135): one time
+// origin for every band, each band centred on its own median, y*ivar and ivar
+// quantised to 64-bit fixed point with one power-of-two scale per band.
+int pack_joint_bands(const BlsCurves* bv, double* tau, long long* qy, long long* qi,
+                     JointBand* jb, double* t_min_out) {
+    const int K = bv->n_curves;
+    double t_min = INFINITY;
+    for (int k = 0; k < K; ++k) {
+        const int64_t b = bv->offsets[k], e = bv->offsets[k + 1];
+        if (e - b < 1) return fail(BLS_E_INVALID, "band %d has no points", k);
+        if (e - b > INT32_MAX) return fail(BLS_E_INVALID, "band %d has too many points", k);
+        for (int64_t j = b; j < e; ++j) {
+            if (!std::isfinite(bv->t[j]) || !std::isfinite(bv->y[j]) ||
+                (bv->dy && !(std::isfinite(bv->dy[j]) && bv->dy[j] > 0.0)))
+                return fail(BLS_E_INVALID,
+                            "band %d: times, fluxes and errors must be finite (errors > 0)", k);
+            t_min = std::min(t_min, bv->t[j]);
+        }
+    }
+    std::vector<double> scratch, yw, iv;
+    for (int k = 0; k < K; ++k) {
+        const int64_t b = bv->offsets[k], n = bv->offsets[k + 1] - b;
+        const double med = median_of(bv->y + b, n, scratch);
+        yw.resize(n);
+        iv.resize(n);
+        double abs_y = 0.0, abs_i = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            tau[b + j] = bv->t[b + j] - t_min;
+            iv[j] = bv->dy ? 1.0 / (bv->dy[b + j] * bv->dy[b + j]) : 1.0;
+            yw[j] = (bv->y[b + j] - med) * iv[j];
+            abs_y += std::fabs(yw[j]);
+            abs_i += iv[j];
+        }
+        // scale so that the sum of magnitudes stays below 2^61: the wrap pad at
+        // most doubles a prefix sum, so every prefix sum and box sum fits an int64
+        auto exponent = [](double total) {
+            if (!(total > 0.0) || !std::isfinite(total)) return 0;
+            int x = 0;
+            std::frexp(total * (1.0 + 1e-12), &x);          // total < 2^x
+            return std::max(-1000, std::min(1000, 61 - x));
+        };
+        const int e_y = exponent(abs_y), e_i = exponent(abs_i);
+        for (int64_t j = 0; j < n; ++j) {
+            qy[b + j] = std::llrint(std::ldexp(yw[j], e_y));
+            qi[b + j] = std::llrint(std::ldexp(iv[j], e_i));
+        }
+        JointBand& d = jb[k];
+        std::memset(&d, 0, sizeof(d));
+        d.point_off = b;
+        d.n_points = (int32_t)n;
+        d.sum_y = pairwise_sum(yw.data(), n);
+        d.sum_ivar = pairwise_sum(iv.data(), n);
+        double floor_v = 4.0 * (double)n * DBL_EPSILON * d.sum_ivar;   // _ivar_floor
+        if (!(floor_v > 0.0)) floor_v = DBL_MIN;
+        d.ivar_floor = floor_v;
+        d.y_unit = std::ldexp(1.0, -e_y);
+        d.i_unit = std::ldexp(1.0, -e_i);
+    }
+    *t_min_out = t_min;
+    return BLS_OK;
+}
+
+int do_search_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, double* out,
+                    cudaStream_t st) {
+    if (!g || !bv) return fail(BLS_E_INVALID, "grid and bands are required");
+    if (g->n_segments < 0 || (g->n_segments > 0 && (!g->seg_offsets || !g->dur_offsets)))
+        return fail(BLS_E_INVALID, "bad segment table");
+    if (g->oversample < 1) return fail(BLS_E_INVALID, "oversample must be >= 1");
+    if (g->objective != 0 && g->objective != 1)
+        return fail(BLS_E_INVALID, "objective must be 'snr' or 'likelihood'");
+    const int K = bv->n_curves;
+    if (K < 1 || !bv->offsets || !bv->t || !bv->y)
+        return fail(BLS_E_INVALID, "at least one band is required");
+    if (K > kMaxJointBands)
+        return fail(BLS_E_INVALID, "at most %d bands per star", kMaxJointBands);
+    if (bv->offsets[0] != 0) return fail(BLS_E_INVALID, "offsets[0] must be 0");
+    const int ns = g->n_segments;
+    const int o = g->oversample;
+    if (ns > 0 && g->seg_offsets[0] != 0) return fail(BLS_E_INVALID, "seg_offsets[0] must be 0");
+    const int64_t P_total = ns > 0 ? g->seg_offsets[ns] : 0;
+    const int64_t n_pts = bv->offsets[K];
+    if (P_total > INT32_MAX - (1 << 22)) return fail(BLS_E_RESOURCE, "too many trial periods");
+
+    // ---- segments (_segment, _bls_joint.py:138-144; _duration_bins) -------------
+    std::vector<JointSegment> segs(std::max(ns, 1));
+    std::vector<int32_t> nbins(P_total), dur_all;
+    int64_t hist_stride = 2;
+    for (int s = 0; s < ns; ++s) {
+        const int64_t p0 = g->seg_offsets[s], p1 = g->seg_offsets[s + 1];
+        const int64_t d0 = g->dur_offsets[s], d1 = g->dur_offsets[s + 1];
+        if (p1 < p0 || d1 < d0) return fail(BLS_E_INVALID, "segment %d: bad offsets", s);
+        JointSegment& sd = segs[s];
+        std::memset(&sd, 0, sizeof(sd));
+        sd.period_off = p0;
+        sd.n_periods = (int32_t)(p1 - p0);
+        sd.oversample = o;
+        sd.dur_off = (int32_t)dur_all.size();
+        if (p1 == p0) continue;
+        if (d1 == d0) return fail(BLS_E_INVALID, "segment %d has no durations", s);
+        double dmin = INFINITY, pmax = 0.0;
+        for (int64_t i = d0; i < d1; ++i) {
+            const double d = g->durations[i];
+            if (!(std::isfinite(d) && d > 0.0))
+                return fail(BLS_E_INVALID, "segment %d: durations must be finite and > 0", s);
+            dmin = std::min(dmin, d);
+        }
+        for (int64_t i = p0; i < p1; ++i) {
+            const double P = g->periods[i];
+            if (!(std::isfinite(P) && P > 0.0))
+                return fail(BLS_E_INVALID,
+                            "BLS: trial periods must be finite and > 0 (segment %d)", s);
+            pmax = std::max(pmax, P);
+        }
+        const double bin = dmin / (double)o;
+        std::vector<int32_t> dur;
+        for (int64_t i = d0; i < d1; ++i) {
+            const double kd = std::floor(g->durations[i] / bin + 0.5);
+            if (kd >= 1.0 && kd < 2147483647.0) {
+                const int32_t k = (int32_t)kd;
+                if (std::find(dur.begin(), dur.end(), k) == dur.end()) dur.push_back(k);
+            }
+        }
+        if ((int)dur.size() > kMaxDur)
+            return fail(BLS_E_INVALID, "segment %d: more than %d distinct box widths", s, kMaxDur);
+        const double wmax = std::ceil(pmax / bin) + (double)o + 1.0;
+        if (!(wmax < 1073741824.0))
+            return fail(BLS_E_RESOURCE, "segment %d: %.3g phase bins per period", s, wmax);
+        const int64_t width = (int64_t)wmax;
+        int64_t hl = 2;
+        for (int64_t i = p0; i < p1; ++i) {
+            const int64_t nb = period_bins(g->periods[i], bin, o, width);
+            nbins[i] = (int32_t)nb;
+            hl = std::max(hl, nb + 1);
+        }
+        sd.width = (int32_t)width;
+        sd.bin_duration = bin;
+        sd.n_dur = (int32_t)dur.size();
+        sd.hist_len = (int32_t)hl;
+        hist_stride = std::max(hist_stride, hl);
+        dur_all.insert(dur_all.end(), dur.begin(), dur.end());
+    }
+    if (P_total == 0) return BLS_OK;
+
+    // ---- where the histograms live ---------------------------------------------
+    const size_t hist_bytes = (size_t)2 * K * hist_stride * sizeof(long long);
+    const bool in_smem = hist_bytes + joint_static_smem() + 1024 <= e->smem_optin;
+    if (in_smem) CUDA_TRY(configure_joint(hist_bytes), "shared-memory opt-in");
+    const int per_sm = std::max(1, joint_resident_ctas(in_smem, in_smem ? hist_bytes : 0));
+    int ctas = (int)std::min<int64_t>(P_total, (int64_t)e->n_sm * (in_smem ? per_sm : 2));
+
+    // ---- stage and upload (one copy) -------------------------------------------
+    const size_t o_tau = 0;
+    const size_t o_qy = o_tau + align256(8 * (size_t)n_pts);
+    const size_t o_qi = o_qy + align256(8 * (size_t)n_pts);
+    const size_t o_band = o_qi + align256(8 * (size_t)n_pts);
+    const size_t o_seg = o_band + align256(sizeof(JointBand) * K);
+    const size_t o_per = o_seg + align256(sizeof(JointSegment) * segs.size());
+    const size_t o_nb = o_per + align256(8 * (size_t)P_total);
+    const size_t o_dur = o_nb + align256(4 * (size_t)P_total);
+    const size_t staged = o_dur + align256(4 * std::max<size_t>(dur_all.size(), 1));
+    const size_t o_out = staged;
+    const size_t o_ctl = o_out + align256(8 * (size_t)kJointFields * P_total);
+    const size_t o_scr = o_ctl + 256;
+    const size_t total = o_scr + (in_smem ? 0 : (size_t)ctas * hist_bytes);
+    int rc;
+    if ((rc = e->h_joint.ensure(std::max(staged, (size_t)8 * kJointFields * P_total)))) return rc;
+    char* h = e->h_joint.as<char>();
+    double t_min = 0.0;
+    if ((rc = pack_joint_bands(bv, reinterpret_cast<double*>(h + o_tau),
+                               reinterpret_cast<long long*>(h + o_qy),
+                               reinterpret_cast<long long*>(h + o_qi),
+                               reinterpret_cast<JointBand*>(h + o_band), &t_min)))
+        return rc;
+    std::memcpy(h + o_seg, segs.data(), sizeof(JointSegment) * segs.size());
+    std::memcpy(h + o_per, g->periods, 8 * (size_t)P_total);
+    std::memcpy(h + o_nb, nbins.data(), 4 * (size_t)P_total);
+    if (!dur_all.empty()) std::memcpy(h + o_dur, dur_all.data(), 4 * dur_all.size());
+    if ((rc = e->d_joint.ensure(total))) return rc;
+    char* d = e->d_joint.as<char>();
+    CUDA_TRY(cudaMemcpyAsync(d, h, staged, cudaMemcpyHostToDevice, st), "upload bands");
+    CUDA_TRY(cudaMemsetAsync(d + o_ctl, 0, 256, st), "reset control words");
+
+    JointArgs a{};
+    a.tau = reinterpret_cast<const double*>(d + o_tau);
+    a.qy = reinterpret_cast<const long long*>(d + o_qy);
+    a.qi = reinterpret_cast<const long long*>(d + o_qi);
+    a.bands = reinterpret_cast<const JointBand*>(d + o_band);
+    a.segments = reinterpret_cast<const JointSegment*>(d + o_seg);
+    a.period = reinterpret_cast<const double*>(d + o_per);
+    a.nbins = reinterpret_cast<const int32_t*>(d + o_nb);
+    a.dur_bins = reinterpret_cast<const int32_t*>(d + o_dur);
+    a.out = reinterpret_cast<double*>(d + o_out);
+    a.n_periods = P_total;
+    a.scratch = in_smem ? nullptr : reinterpret_cast<long long*>(d + o_scr);
+    a.hist_stride = hist_stride;
+    a.work_counter = reinterpret_cast<int32_t*>(d + o_ctl);
+    a.error_flag = reinterpret_cast<int32_t*>(d + o_ctl) + 8;
+    a.t_min = t_min;
+    a.n_bands = K;
+    a.n_segments = ns;
+    a.obj_flag = g->objective;
+    CUDA_TRY(launch_joint(a, in_smem, in_smem ? hist_bytes : 0, ctas, st), "joint search launch");
+    int32_t* hflag = nullptr;
+    if ((rc = e->h_ctl.ensure(64))) return rc;
+    hflag = e->h_ctl.as<int32_t>();
+    CUDA_TRY(cudaMemcpyAsync(h, d + o_out, 8 * (size_t)kJointFields * P_total,
+                             cudaMemcpyDeviceToHost, st),
+             "download joint fields");
+    CUDA_TRY(cudaMemcpyAsync(hflag, a.error_flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
+             "read error flag");
+    CUDA_TRY(cudaStreamSynchronize(st), "synchronize");
+    if (hflag[0] != 0)
+        return fail(BLS_E_DEVICE, "the joint search met an impossible descriptor (flag %d)",
+                    hflag[0]);
+    std::memcpy(out, h, 8 * (size_t)kJointFields * P_total);
+    return BLS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1033,6 +1261,13 @@ int bls_search(BlsEngine* e, const BlsGrid* grid, const BlsCurves* curves, doubl
     if ((rc = bls_prepare(e, grid, curves, stream))) return rc;
     if ((rc = bls_launch(e, stream))) return rc;
     return bls_download(e, out, stream);
+}
+
+int bls_search_joint(BlsEngine* e, const BlsGrid* grid, const BlsCurves* bands, double* out,
+                     void* stream) {
+    if (!e) return fail(BLS_E_INVALID, "engine is NULL");
+    if (!out) return fail(BLS_E_INVALID, "output pointer is NULL");
+    return do_search_joint(e, grid, bands, out, pick(e, stream));
 }
 
 int bls_batch_info(BlsEngine* e, BlsBatchInfo* info) {

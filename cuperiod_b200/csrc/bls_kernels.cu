@@ -35,6 +35,7 @@
 #include <mutex>
 
 #include "bls_device.h"
+#include "bls_fold.cuh"
 #include "bls_launch.h"
 
 namespace blsb200 {
@@ -76,16 +77,6 @@ struct TileShared {
     int next;
     uint32_t thr_bits;              // the sweep's shared threshold (bits of a float >= 0)
 };
-
-// The reference's IEEE fold (no contraction): the fallback of the fast path.
-__device__ __forceinline__ int fold_exact(double x, double P, double bin, int width) {
-    const double q = __ddiv_rn(x, P);
-    const double w = __dsub_rn(x, __dmul_rn(P, floor(q)));
-    int ind = (int)__ddiv_rn(w, bin) + 1;
-    ind = ind < 0 ? 0 : ind;
-    ind = ind > width - 1 ? width - 1 : ind;
-    return ind;
-}
 
 // Fast fold.  Returns the reference's bin when the scaled phase is provably away
 // from every edge, else -1.

@@ -50,6 +50,15 @@ cudaError_t launch_rows(const double* out, int64_t out_stride, int n_curves, int
 // Bytes of one period's histogram in the kernel's layout.
 size_t period_hist_bytes(int mode, int hl);
 
+// Joint-ephemeris multi-band search (bls_joint.cu): static shared memory of one
+// CTA, CTAs resident per SM (histograms in `smem` bytes of dynamic shared memory,
+// or in global scratch), and the persistent launch over every trial period.
+size_t joint_static_smem();
+cudaError_t configure_joint(size_t smem);
+int joint_resident_ctas(bool in_smem, size_t smem);
+cudaError_t launch_joint(const JointArgs& args, bool in_smem, size_t smem, int n_ctas,
+                         cudaStream_t stream);
+
 int search_threads();
 int max_resident_ctas(int mode, size_t smem);
 

@@ -1,15 +1,16 @@
-"""Multi-band BLS (cuPeriod src/cuperiod/multiband/bls_mb.py:1-275).
+"""Multi-band BLS (cuPeriod src/cuperiod/multiband/bls_mb.py:1-315).
 
 Bands of one star share the trial period grid.  In the "independent" statistic
 each band is box-searched on its own -- here all bands of the star are curves of
 one engine launch -- and the per-period power is the quadrature stack of the
 bands' clipped depth-SNRs, sum_k max(SNR_k, 0)^2, with the box (depth, duration,
-mid-transit time) of the band detecting it most strongly.  A band's errors are
-used only when every contributing band has them; otherwise every band is
-searched with a constant error equal to its own robust scatter (1.4826 x MAD).
-
-The "shared" statistic (one box placed in every band at once,
-multiband/_bls_joint.py) is a different kernel and is not built on this engine.
+mid-transit time) of the band detecting it most strongly.  In the "shared"
+statistic (multiband/_bls_joint.py) one box -- one duration and one phase from
+one time origin -- is placed in every band at once and chosen by the summed
+per-band objective of the bands that dip in it (the engine's joint kernel); the
+power is the same quadrature stack at that box.  A band's errors are used only
+when every contributing band has them; otherwise every band is searched with a
+constant error equal to its own robust scatter (1.4826 x MAD).
 """
 
 from __future__ import annotations
@@ -19,7 +20,7 @@ from typing import Any, Final
 import numpy as np
 
 from . import _lib
-from .errors import BackendUnavailableError, InsufficientDataError
+from .errors import InsufficientDataError
 from .grid import GridSpec
 from .lightcurve import Domain, LightCurve, MultiBandLightCurve
 from .result import Periodogram
@@ -72,14 +73,10 @@ def multiband_default_grid(method: Any, mblc: MultiBandLightCurve, settings: Any
 def bls_multiband_power(grid: GridSpec, mblc: MultiBandLightCurve, settings: Any, *,
                         ephemeris: str | None = None,
                         engine: _lib.Engine | None = None) -> Periodogram:
-    """The multi-band BLS periodogram on a shared period grid (bls_mb.py:120-237)."""
+    """The multi-band BLS periodogram on a shared period grid (bls_mb.py:120-315)."""
     from .bls import BACKEND_NAME, _grid_segments
     from .core import _objective_flag
     mode = resolve_ephemeris(settings, ephemeris)
-    if mode == "shared":
-        raise BackendUnavailableError(
-            "BLS multiband: ephemeris='shared' (one box across all bands) is not built on "
-            "the b200 engine; use ephemeris='independent'")
     finite = mblc.finite()
     used = [(name, lc.in_domain(Domain.FLUX)) for name, lc in finite.bands.items()
             if lc.n >= MIN_BAND_POINTS]
@@ -104,22 +101,33 @@ def bls_multiband_power(grid: GridSpec, mblc: MultiBandLightCurve, settings: Any
                                                 _objective_flag(settings.objective))
     curves = _lib.PackedCurves.from_arrays([(lc.time, lc.value, e)
                                             for lc, e in zip(bands, errors)])
-    out = (engine or _lib.default_engine()).search(packed_grid, curves)
-    names = _lib.FIELD_NAMES
-    dsnr = np.clip(out[names.index("depth_snr")], 0.0, None)
-    combined = np.sum(dsnr ** 2, axis=0)
-    best = np.argmax(dsnr, axis=0)
-    cols = np.arange(dsnr.shape[1])
+    eng = engine or _lib.default_engine()
     period = np.concatenate([np.asarray(p, dtype=np.float64) for p, _ in segments])
+    if mode == "shared":
+        # one box for every band (bls_mb.py:278-312): the joint kernel's fields
+        joint = dict(zip(_lib.JOINT_FIELD_NAMES, eng.search_joint(packed_grid, curves)))
+        combined = joint["power"]
+        fields = {"depth": joint["depth"], "depth_snr": joint["depth_snr"],
+                  "duration": joint["duration"], "t0": joint["transit_time"],
+                  "band_index": joint["band_index"]}
+    else:
+        out = eng.search(packed_grid, curves)
+        names = _lib.FIELD_NAMES
+        dsnr = np.clip(out[names.index("depth_snr")], 0.0, None)
+        combined = np.sum(dsnr ** 2, axis=0)
+        best = np.argmax(dsnr, axis=0)
+        cols = np.arange(dsnr.shape[1])
+        fields = {"depth": out[names.index("depth")][best, cols],
+                  "depth_snr": np.sqrt(combined),
+                  "duration": out[names.index("duration")][best, cols],
+                  "t0": out[names.index("transit_time")][best, cols],
+                  "band_index": best.astype(np.float64)}
     power = np.nan_to_num(combined, nan=0.0, posinf=0.0)
     mean, std = float(power.mean()), float(power.std())
     sde = (power - mean) / std if std > 0.0 else np.zeros_like(power)
-    extras = {"depth": out[names.index("depth")][best, cols],
-              "depth_snr": np.sqrt(combined),
-              "duration": out[names.index("duration")][best, cols],
-              "t0": out[names.index("transit_time")][best, cols],
-              "sde": sde,
-              "band_index": best.astype(np.float64)}
+    extras = {"depth": fields["depth"], "depth_snr": fields["depth_snr"],
+              "duration": fields["duration"], "t0": fields["t0"], "sde": sde,
+              "band_index": fields["band_index"]}
     meta = {**dict(finite.meta), "bands": tuple(name for name, _ in used),
             "mb_ephemeris": mode}
     return Periodogram.from_spectrum(method="BLS", backend=BACKEND_NAME, frequency=1.0 / period,

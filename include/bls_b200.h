@@ -175,6 +175,26 @@ int bls_search(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* curves, 
 
 int bls_batch_info(BlsEngine* engine, BlsBatchInfo* info);
 
+/* Joint-ephemeris fields (JOINT_FIELDS, src/cuperiod/multiband/_bls_joint.py:52-54). */
+enum {
+    BLS_J_POWER = 0, BLS_J_DEPTH, BLS_J_DEPTH_SNR, BLS_J_DURATION, BLS_J_TRANSIT_TIME,
+    BLS_J_BAND_INDEX, BLS_J_N_FIELDS
+};
+
+/* The joint-ephemeris ("shared") multi-band search of one star: one box -- one
+ * duration and one phase on a phase grid binned from one time origin -- placed
+ * in every band at once, chosen per trial period by the summed per-band
+ * objective of the bands that dip in it.  Replaces joint_search with the
+ * 'cupy' backend (src/cuperiod/multiband/_bls_joint.py:151-204, the launch of
+ * _joint_cuda, 703-796) together with joint_bands (94-135) and _finish
+ * (359-404).  `bands` holds the star's bands as curves (1 to 64; each band's
+ * fluxes are centred on its own median here; dy may be NULL for unit errors).
+ * out receives BLS_J_N_FIELDS x n_periods values, field-major, in grid order: a
+ * period where no band dips in any admissible box has every field 0.  Waits for
+ * the stream. */
+int bls_search_joint(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* bands, double* out,
+                     void* stream);
+
 /* Phase bin of every point of one curve (times t, n points; t_min removed as the
  * reference does) at one period of a segment whose shortest duration and
  * oversample give the bin width, as the search kernel computes it.  used_fast[j]

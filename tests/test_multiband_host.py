@@ -58,12 +58,16 @@ def test_band_rules():
         MultiBandLightCurve({"g": a, "m": LightCurve(np.arange(3.0), np.ones(3))})
 
 
-def test_shared_ephemeris_is_refused_before_the_device():
-    from cuperiod_b200.errors import BackendUnavailableError
+@pytest.mark.parametrize("ephemeris", ["independent", "shared"])
+def test_band_selection_fails_before_the_device(ephemeris):
+    from cuperiod_b200.errors import InsufficientDataError
     from cuperiod_b200.grid import GridSpec
+    from cuperiod_b200.lightcurve import Domain, LightCurve, MultiBandLightCurve
     from cuperiod_b200.multiband import bls_multiband_power
     from cuperiod_b200.settings import BLSSettings
-    meta, z = _cases()[0]
-    with pytest.raises(BackendUnavailableError, match="shared"):
-        bls_multiband_power(GridSpec(kind="period", values=np.array([1.0, 2.0])),
-                            mblc_of(meta, z), BLSSettings(), ephemeris="shared")
+    short = MultiBandLightCurve.from_light_curves({
+        "g": LightCurve(np.arange(2.0), np.ones(2), None, Domain.FLUX),
+        "r": LightCurve(np.arange(2.0) + 0.5, np.ones(2), None, Domain.FLUX)})
+    with pytest.raises(InsufficientDataError, match="no band has enough"):
+        bls_multiband_power(GridSpec(kind="period", values=np.array([1.0, 2.0])), short,
+                            BLSSettings(), ephemeris=ephemeris)
