@@ -63,6 +63,10 @@ def parse_args():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target duration of the CPU-baseline sample")
+    p.add_argument("--workload", choices=("batch", "multiband-shared"), default="batch",
+                   help="batch: the headline batched search; multiband-shared: the "
+                        "joint-ephemeris multi-band search of --stars six-band stars")
+    p.add_argument("--stars", type=int, default=64, help="multiband-shared: stars per rank")
     return p.parse_args()
 
 
@@ -309,9 +313,214 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+# ---- the joint-ephemeris multi-band search ------------------------------------
+
+JOINT_METRIC = "multi-band BLS (shared ephemeris) stars/s on 1 B200"
+JOINT_UNIT = "stars/s"
+JOINT_WORKLOAD = ("joint-ephemeris multi-band BLS: six-band stars (u/g/r/i/z/y share "
+                  "6/9/26/26/17/16%), N~U[600,3000] points over 90 d, default grid of the "
+                  "stacked baseline (~17,800 periods, 8 segments), snr objective")
+# FP64 divisions per SM clock on a B200 (profiles/pipe_rates.txt)
+DDIV_PER_SM_CLOCK = 7.163
+
+
+def joint_workload(n_stars: int, seed: int):
+    """Per star: the light curves, the packed grid and bands, the segments."""
+    from cuperiod_b200 import _lib
+    from cuperiod_b200.bls import BLSMethod, _grid_segments
+    from cuperiod_b200.lightcurve import Domain, LightCurve, MultiBandLightCurve
+    from cuperiod_b200.multiband import band_errors, multiband_default_grid
+    from cuperiod_b200.settings import BLSSettings
+    from cuperiod_b200.synthetic import multiband_stars
+
+    settings = BLSSettings(mb_ephemeris="shared")
+    out = []
+    for star in multiband_stars(n_stars, seed=seed):
+        mblc = MultiBandLightCurve.from_light_curves(
+            {k: LightCurve(c.t, c.y, c.dy, Domain.FLUX) for k, c in star.items()})
+        grid = multiband_default_grid(BLSMethod(), mblc, settings)
+        segments = _grid_segments(grid, settings)
+        bands = list(mblc.finite().bands.values())
+        errors = band_errors(bands)
+        packed = _lib.PackedCurves.from_arrays([(lc.time, lc.value, e)
+                                                for lc, e in zip(bands, errors)])
+        pgrid = _lib.PackedGrid.from_segments(segments, settings.bins_per_duration, 0)
+        out.append({"mblc": mblc, "grid": grid, "segments": segments, "packed": packed,
+                    "pgrid": pgrid, "settings": settings,
+                    "bands": [(lc.time, lc.value, e) for lc, e in zip(bands, errors)]})
+    return out
+
+
+def joint_box_bands(star) -> float:
+    """Box evaluations x bands of one star's joint search (the reference's sweep
+    visits every (duration, start) box of every period once per band)."""
+    from oracle import oracle
+    total = 0.0
+    for periods, durations in star["segments"]:
+        spec = oracle.search_spec(periods, durations, 10)
+        nb = np.minimum(np.ceil(spec.periods / spec.bin_duration) + 10, spec.width - 1)
+        for k in spec.dur_bins:
+            total += float(np.where(k < nb, nb - k + 1, 0).sum())
+    return total * len(star["bands"])
+
+
+def joint_cpu_sample(stars, seconds: float) -> dict:
+    """The reference's joint sweep (the oracle's C port of its numba kernel, all
+    host cores) on stars of the workload until ``seconds`` have passed."""
+    from oracle import oracle
+    cores = os.cpu_count() or 1
+    done, t0 = 0, time.perf_counter()
+    for star in stars:
+        jb = oracle.joint_bands(*[list(x) for x in zip(*star["bands"])])
+        for periods, durations in star["segments"]:
+            oracle.joint_power(jb, periods, durations, 10, 0, n_threads=cores)
+        done += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": JOINT_UNIT, "cores": cores, "kind": "port",
+            "sample": f"the first {done} stars of the workload in {dt:.1f} s"}
+
+
+def run_joint_reference(args) -> None:
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    stars = joint_workload(args.stars, args.seed)
+    for _ in range(args.warmup):
+        joint_cpu_sample(stars[:1], 0.0)
+    vals = [joint_cpu_sample(stars, args.cpu_seconds) for _ in range(args.steps)]
+    value = statistics.mean(v["value"] for v in vals)
+    print(json.dumps({
+        "impl": "reference", "metric": JOINT_METRIC, "value": value, "unit": JOINT_UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * args.stars / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": JOINT_WORKLOAD, "stars_per_rank": args.stars, "cpu": "host cores"},
+        "cpu_baseline": dict(vals[-1], value=value),
+        "e2e": {"value": value, "unit": JOINT_UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_joint_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from cuperiod_b200 import _lib
+    from cuperiod_b200.multiband import bls_multiband_power
+    from cuperiod_b200.sharding import max_over_ranks
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    stars = joint_workload(args.stars, args.seed + rank)
+    stream = torch.cuda.Stream(device=local)
+    handle = stream.cuda_stream
+    assert handle != 0
+    # one engine per star, each holding its prepared star on the device
+    engines = [_lib.Engine(device=local) for _ in stars]
+    for eng, st in zip(engines, stars):
+        eng.joint_prepare(st["pgrid"], st["packed"], stream=handle)
+    for _ in range(args.warmup):
+        for eng in engines:
+            eng.joint_launch(handle)
+    torch.cuda.synchronize()
+
+    # ---- device-resident: every star's launch, K times --------------------------
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as sampler:
+        for i in range(args.steps):
+            starts[i].record(stream)
+            for eng in engines:
+                eng.joint_launch(handle)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.summary()
+    total_ms = starts[0].elapsed_time(ends[-1])
+    ms_per_step = max_over_ranks(total_ms / args.steps)
+    value = world * args.stars / (ms_per_step / 1000.0)
+
+    # ---- end to end: the public multi-band entry with host arrays ---------------
+    e2e_ms = []
+    for i in range(args.steps):
+        barrier()
+        torch.cuda.synchronize()
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for st in stars:
+            pg = bls_multiband_power(st["grid"], st["mblc"], st["settings"], engine=engines[0])
+            pg.best_period()
+        e.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(s.elapsed_time(e))
+    e2e_step = max_over_ranks(statistics.mean(e2e_ms))
+    e2e_value = world * args.stars / (e2e_step / 1000.0)
+
+    if rank == 0:
+        n_pts = sum(st["packed"].t.size for st in stars)
+        n_per = sum(st["pgrid"].n_periods for st in stars)
+        box_bands = sum(joint_box_bands(st) for st in stars)
+        f_clk = (clocks.get("sm_mhz") or 1900.0) * 1e6
+        n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+        # FP64 division pipe: the two quotients (inside and outside means) that
+        # decide the dip of every box-band, at the probe's rate
+        t_div = box_bands * 2 / (DDIV_PER_SM_CLOCK * n_sm * f_clk)
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        alg_bytes = n_pts * 24 + n_per * 12 + n_per * 6 * 8
+        achieved = alg_bytes / (ms_per_step / 1000.0) / 1e9
+        out = {
+            "metric": JOINT_METRIC, "value": value, "unit": JOINT_UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": JOINT_WORKLOAD, "stars_per_rank": args.stars,
+                       "periods_per_step": n_per, "box_bands_per_step": box_bands,
+                       "l2": "a star's bands and histograms live in L2 and shared memory; "
+                             "no flush (the bound is the SM pipes)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "note": "SM-bound (FP64 box arithmetic); see sm_roofline"},
+            "sm_roofline": {"bound": "fp64_div", "model_ms": 1000.0 * t_div,
+                            "kernel_ms": ms_per_step, "frac": 1000.0 * t_div / ms_per_step},
+            "clocks": clocks,
+            "gpu_launches": args.steps * len(stars),
+            "e2e": {"value": e2e_value, "unit": JOINT_UNIT,
+                    "h2d_bytes_per_step": n_pts * 25 + n_per * 12,
+                    "d2h_bytes_per_step": n_per * 6 * 8},
+        }
+        if world == 1:
+            out["cpu_baseline"] = joint_cpu_sample(stars, args.cpu_seconds)
+        print(json.dumps(out), flush=True)
+    for eng in engines:
+        eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main() -> None:
     args = parse_args()
-    if args.impl == "reference":
+    if args.workload == "multiband-shared":
+        run_joint_reference(args) if args.impl == "reference" else run_joint_ours(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

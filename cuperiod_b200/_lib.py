@@ -84,13 +84,17 @@ def load() -> ctypes.CDLL:
         lib.bls_search.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_batch_info.argtypes = [_vp, P(BlsBatchInfo)]
         lib.bls_search_joint.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
+        lib.bls_joint_prepare.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp]
+        lib.bls_joint_launch.argtypes = [_vp, _vp]
+        lib.bls_joint_download.argtypes = [_vp, _vp, _vp]
         lib.bls_debug_fold_bins.argtypes = [_vp, _vp, _i64, _dbl, _dbl, _i32, _vp, _vp]
         lib.bls_debug_prefix.argtypes = [_vp, _vp, _vp, _vp, _i64, _dbl, _vp, _i32, _i32, _vp, _vp,
                                          _vp]
         for name in ("bls_engine_create", "bls_engine_destroy", "bls_prepare", "bls_launch",
                      "bls_download", "bls_device_output", "bls_download_best", "bls_search",
                      "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix",
-                     "bls_launch_best_noalloc", "bls_download_rows", "bls_search_joint"):
+                     "bls_launch_best_noalloc", "bls_download_rows", "bls_search_joint",
+                     "bls_joint_prepare", "bls_joint_launch", "bls_joint_download"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib
@@ -198,6 +202,7 @@ class Engine:
         self._h = handle
         self._grid: PackedGrid | None = None
         self._curves: PackedCurves | None = None
+        self._joint_periods = 0
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -286,6 +291,20 @@ class Engine:
         g, c = grid.struct(), bands.struct()
         _check(self._lib.bls_search_joint(self._h, ctypes.byref(g), ctypes.byref(c),
                                           out.ctypes.data, stream))
+        return out
+
+    def joint_prepare(self, grid: PackedGrid, bands: PackedCurves,
+                      stream: int | None = None) -> None:
+        g, c = grid.struct(), bands.struct()
+        _check(self._lib.bls_joint_prepare(self._h, ctypes.byref(g), ctypes.byref(c), stream))
+        self._joint_periods = grid.n_periods
+
+    def joint_launch(self, stream: int | None = None) -> None:
+        _check(self._lib.bls_joint_launch(self._h, stream))
+
+    def joint_download(self, stream: int | None = None) -> np.ndarray:
+        out = np.empty((len(JOINT_FIELD_NAMES), self._joint_periods), dtype=np.float64)
+        _check(self._lib.bls_joint_download(self._h, out.ctypes.data, stream))
         return out
 
     def prefix_sums(self, t, y, dy, period: float, durations, oversample: int):

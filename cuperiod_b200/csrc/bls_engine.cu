@@ -217,6 +217,14 @@ struct BlsEngine {
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
 
+    // the prepared joint (multi-band, shared box) search
+    bool joint_prepared = false;
+    JointArgs jargs{};
+    bool joint_in_smem = false;
+    size_t joint_smem = 0;
+    int joint_ctas = 0;
+    int64_t joint_periods = 0;
+
     ~BlsEngine() {
         if (graph) cudaGraphExecDestroy(graph);
         for (DevBuf* b : {&d_tau, &d_pay_r, &d_r64, &d_iv64, &d_period, &d_freq, &d_scale, &d_nbins,
@@ -871,9 +879,9 @@ int pack_joint_bands(const BlsCurves* bv, double* tau, long long* qy, long long*
     return BLS_OK;
 }
 
-int do_search_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, double* out,
-                    cudaStream_t st) {
+int do_prepare_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, cudaStream_t st) {
     if (!g || !bv) return fail(BLS_E_INVALID, "grid and bands are required");
+    e->joint_prepared = false;
     if (g->n_segments < 0 || (g->n_segments > 0 && (!g->seg_offsets || !g->dur_offsets)))
         return fail(BLS_E_INVALID, "bad segment table");
     if (g->oversample < 1) return fail(BLS_E_INVALID, "oversample must be >= 1");
@@ -950,7 +958,11 @@ int do_search_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, double*
         hist_stride = std::max(hist_stride, hl);
         dur_all.insert(dur_all.end(), dur.begin(), dur.end());
     }
-    if (P_total == 0) return BLS_OK;
+    if (P_total == 0) {
+        e->joint_periods = 0;
+        e->joint_prepared = true;
+        return BLS_OK;
+    }
 
     // ---- where the histograms live ---------------------------------------------
     const size_t hist_bytes = (size_t)2 * K * hist_stride * sizeof(long long);
@@ -1010,20 +1022,44 @@ int do_search_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, double*
     a.n_bands = K;
     a.n_segments = ns;
     a.obj_flag = g->objective;
-    CUDA_TRY(launch_joint(a, in_smem, in_smem ? hist_bytes : 0, ctas, st), "joint search launch");
-    int32_t* hflag = nullptr;
+    e->jargs = a;
+    e->joint_in_smem = in_smem;
+    e->joint_smem = in_smem ? hist_bytes : 0;
+    e->joint_ctas = ctas;
+    e->joint_periods = P_total;
+    e->joint_prepared = true;
+    return BLS_OK;
+}
+
+int do_launch_joint(BlsEngine* e, cudaStream_t st) {
+    if (!e->joint_prepared) return fail(BLS_E_STATE, "bls_joint_launch before bls_joint_prepare");
+    if (e->joint_periods == 0) return BLS_OK;
+    CUDA_TRY(cudaMemsetAsync(e->jargs.work_counter, 0, 64, st), "reset control words");
+    CUDA_TRY(launch_joint(e->jargs, e->joint_in_smem, e->joint_smem, e->joint_ctas, st),
+             "joint search launch");
+    return BLS_OK;
+}
+
+int do_download_joint(BlsEngine* e, double* out, cudaStream_t st) {
+    if (!e->joint_prepared) return fail(BLS_E_STATE, "bls_joint_download before bls_joint_prepare");
+    const int64_t P = e->joint_periods;
+    if (P == 0) return BLS_OK;
+    int rc;
     if ((rc = e->h_ctl.ensure(64))) return rc;
-    hflag = e->h_ctl.as<int32_t>();
-    CUDA_TRY(cudaMemcpyAsync(h, d + o_out, 8 * (size_t)kJointFields * P_total,
-                             cudaMemcpyDeviceToHost, st),
+    int32_t* hflag = e->h_ctl.as<int32_t>();
+    const size_t bytes = 8 * (size_t)kJointFields * P;
+    // the staging buffer holds at least this much (do_prepare_joint)
+    char* h = e->h_joint.as<char>();
+    CUDA_TRY(cudaMemcpyAsync(h, e->jargs.out, bytes, cudaMemcpyDeviceToHost, st),
              "download joint fields");
-    CUDA_TRY(cudaMemcpyAsync(hflag, a.error_flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
+    CUDA_TRY(cudaMemcpyAsync(hflag, e->jargs.error_flag, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             st),
              "read error flag");
     CUDA_TRY(cudaStreamSynchronize(st), "synchronize");
     if (hflag[0] != 0)
         return fail(BLS_E_DEVICE, "the joint search met an impossible descriptor (flag %d)",
                     hflag[0]);
-    std::memcpy(out, h, 8 * (size_t)kJointFields * P_total);
+    std::memcpy(out, h, bytes);
     return BLS_OK;
 }
 
@@ -1263,11 +1299,28 @@ int bls_search(BlsEngine* e, const BlsGrid* grid, const BlsCurves* curves, doubl
     return bls_download(e, out, stream);
 }
 
-int bls_search_joint(BlsEngine* e, const BlsGrid* grid, const BlsCurves* bands, double* out,
-                     void* stream) {
+int bls_joint_prepare(BlsEngine* e, const BlsGrid* grid, const BlsCurves* bands, void* stream) {
+    if (!e) return fail(BLS_E_INVALID, "engine is NULL");
+    return do_prepare_joint(e, grid, bands, pick(e, stream));
+}
+
+int bls_joint_launch(BlsEngine* e, void* stream) {
+    if (!e) return fail(BLS_E_INVALID, "engine is NULL");
+    return do_launch_joint(e, pick(e, stream));
+}
+
+int bls_joint_download(BlsEngine* e, double* out, void* stream) {
     if (!e) return fail(BLS_E_INVALID, "engine is NULL");
     if (!out) return fail(BLS_E_INVALID, "output pointer is NULL");
-    return do_search_joint(e, grid, bands, out, pick(e, stream));
+    return do_download_joint(e, out, pick(e, stream));
+}
+
+int bls_search_joint(BlsEngine* e, const BlsGrid* grid, const BlsCurves* bands, double* out,
+                     void* stream) {
+    int rc;
+    if ((rc = bls_joint_prepare(e, grid, bands, stream))) return rc;
+    if ((rc = bls_joint_launch(e, stream))) return rc;
+    return bls_joint_download(e, out, stream);
 }
 
 int bls_batch_info(BlsEngine* e, BlsBatchInfo* info) {

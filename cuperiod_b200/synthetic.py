@@ -15,6 +15,14 @@ cadences, lengths and value distributions:
 * :func:`long_baseline_curves` -- 60,000 points at 30-minute cadence over four
   years with times offset by ~1.4e3 d, depths down to 5e-5; 200,000 log periods
   in [0.5, 400] d with 12 durations per segment.
+* :func:`multiband_stars` -- stars observed in six bands (u, g, r, i, z, y; the
+  points of a star split 6/9/26/26/17/16% between them) at random night-time
+  epochs over 90 d, N ~ U[600, 3000] points per star; per band a flux level
+  log-uniform in [0.3, 3], noise sigma log-uniform in [1e-3, 1e-2] with errors
+  of sigma x U[0.8, 1.2]; half the stars carry a chromatic box transit (depth
+  log-uniform [1e-3, 1e-2] scaled 0.7-1.3x from u to y, period log-uniform
+  [0.5, 20] d, duration U[0.04, 0.3] d).  Searched with the shared box over the
+  default grid of the stacked baseline.
 """
 
 from __future__ import annotations
@@ -104,5 +112,40 @@ def long_baseline_periods() -> np.ndarray:
     return np.geomspace(0.5, 400.0, 200000)
 
 
-__all__ = ["Curve", "batched_curves", "batched_periods", "long_baseline_curves",
-           "long_baseline_periods", "single_curve"]
+MULTIBAND_BANDS = ("u", "g", "r", "i", "z", "y")
+MULTIBAND_SHARE = (0.06, 0.09, 0.26, 0.26, 0.17, 0.16)
+
+
+def multiband_stars(n_stars: int, *, seed: int = 0, span: float = 90.0,
+                    n_range=(600, 3000)) -> list[dict[str, Curve]]:
+    """The multi-band workload's stars, ``{band: Curve}`` each (see the module
+    docstring)."""
+    rng = np.random.default_rng(seed)
+    stars = []
+    for _ in range(n_stars):
+        n_total = int(rng.integers(n_range[0], n_range[1] + 1))
+        transit = None
+        if rng.random() < 0.5:
+            transit = (10.0 ** rng.uniform(np.log10(0.5), np.log10(20.0)),
+                       rng.uniform(0.04, 0.3), 10.0 ** rng.uniform(-3.0, -2.0))
+            t0 = rng.uniform(0.0, transit[0])
+        bands = {}
+        for b, (name, share) in enumerate(zip(MULTIBAND_BANDS, MULTIBAND_SHARE)):
+            n = max(3, int(round(n_total * share)))
+            nights = rng.integers(0, int(span), size=n)
+            t = np.sort(nights + rng.uniform(0.05, 0.45, size=n)) + 2460000.0
+            level = 10.0 ** rng.uniform(np.log10(0.3), np.log10(3.0))
+            sigma = 10.0 ** rng.uniform(-3.0, -2.0)
+            y = level * (1.0 + rng.normal(0.0, sigma, n))
+            if transit is not None:
+                scale = 0.7 + 0.6 * b / (len(MULTIBAND_BANDS) - 1)
+                y[np.mod(t - 2460000.0 - t0, transit[0]) < transit[1]] -= \
+                    level * transit[2] * scale
+            dy = level * sigma * rng.uniform(0.8, 1.2, n)
+            bands[name] = Curve(t, y, dy, transit)
+        stars.append(bands)
+    return stars
+
+
+__all__ = ["Curve", "MULTIBAND_BANDS", "batched_curves", "batched_periods",
+           "long_baseline_curves", "long_baseline_periods", "multiband_stars", "single_curve"]

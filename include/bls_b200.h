@@ -195,6 +195,16 @@ enum {
 int bls_search_joint(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* bands, double* out,
                      void* stream);
 
+/* bls_search_joint in its three phases, as _joint_cuda runs them: the uploads
+ * (joint_bands and the segment tables, 703-760), the launch (one persistent
+ * launch for every segment) and the download of the fields (784-796).  A
+ * prepared star stays on the device: bls_joint_launch may run again; the next
+ * bls_joint_prepare replaces it.  bls_joint_download waits for the stream. */
+int bls_joint_prepare(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* bands,
+                      void* stream);
+int bls_joint_launch(BlsEngine* engine, void* stream);
+int bls_joint_download(BlsEngine* engine, double* out, void* stream);
+
 /* Phase bin of every point of one curve (times t, n points; t_min removed as the
  * reference does) at one period of a segment whose shortest duration and
  * oversample give the bin width, as the search kernel computes it.  used_fast[j]
