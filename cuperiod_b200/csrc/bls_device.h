@@ -125,8 +125,9 @@ struct BatchArgs {
 // One star's bands share one box per trial period (cuPeriod
 // src/cuperiod/multiband/_bls_joint.py).  Each band's centred flux*weight and
 // weight are quantised to 64-bit fixed point with a power-of-two scale per band
-// (|sum of the band's values| < 2^62), so every bin and prefix sum is an exact
-// integer and a box's sums are exact differences.
+// (the band's magnitudes sum below 2^61, so even wrap-padded prefix sums fit
+// an int64), so every bin and prefix sum is an exact integer and a box's sums
+// are exact differences.  One bin of one band is a 16-byte record {Y, I}.
 
 constexpr int kJointFields = 6;     // power, depth, depth_snr, duration, t0, band_index
 constexpr int kMaxJointBands = 64;
@@ -134,12 +135,20 @@ constexpr int kMaxJointBands = 64;
 struct JointBand {
     int64_t point_off;      // first point of the band in tau / qy / qi
     int32_t n_points;
-    int32_t pad;
+    // FP32 screen, box sums in units of 2^61 quanta (|y'|, i' <= 1):
+    float ybar_n;           // (sum_y / sum_ivar) * i_unit / y_unit
+    float s_n;              // sum_ivar / (i_unit * 2^61)
+    float c_n;              // 2^61 * y_unit^2 / i_unit: the objective per unit of
+                            // the normalised one
+    float floor_n;          // ivar_floor / (i_unit * 2^61), rounded up
     double sum_y;           // the reference's float sums of y*ivar and ivar
     double sum_ivar;
     double ivar_floor;      // admissibility floor of either side of a box
     double y_unit;          // reference units of one quantum of y*ivar (2^-e)
     double i_unit;          // reference units of one quantum of ivar
+    long long qi_total;     // sum of the band's quantised weights
+    int32_t full_skip;      // 1: a box holding qi_total fails the floor test
+    int32_t pad;
 };
 
 struct JointSegment {
@@ -151,15 +160,22 @@ struct JointSegment {
     int32_t n_dur;
     int32_t oversample;
     int32_t hist_len;       // max n_bins + 1 over the segment
+    int32_t frac_bits;      // fast fold (fold_fast): fraction bits of the scaled phase
+    uint32_t margin_u;      // fast fold: bin-edge margin, units of 2^-frac_bits bins
+    uint32_t margin_phi;    // fast fold: cycle-edge margin, units of 2^-32 cycles
+    int32_t fast_fold;      // 1: the fast fold's error bound holds for the star
 };
 
 struct JointArgs {
     const double* tau;          // per point: t - t_min over all bands
     const long long* qy;        // per point: quantised (y - median) * ivar
     const long long* qi;        // per point: quantised ivar
+    const uint8_t* band_of;     // per point: its band
     const JointBand* bands;
     const JointSegment* segments;
     const double* period;       // per grid period
+    const double* freq;         // RN(1/P)
+    const uint32_t* scale;      // round(P/bin * 2^frac_bits) (fast-fold segments)
     const int32_t* nbins;       // the reference's n_bins per period
     const int32_t* dur_bins;    // per segment, box widths in bins (first-seen order)
     double* out;                // kJointFields x n_periods, field-major
@@ -169,6 +185,8 @@ struct JointArgs {
     int32_t* work_counter;      // next unclaimed period
     int32_t* error_flag;
     double t_min;
+    int32_t n_points;           // points of the star (all bands)
+    int32_t screen;             // 1: the FP32 screen's constants are in range
     int32_t n_bands;
     int32_t n_segments;
     int32_t obj_flag;           // 0 snr, 1 log-likelihood

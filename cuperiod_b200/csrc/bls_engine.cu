@@ -821,7 +821,7 @@ size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 // origin for every band, each band centred on its own median, y*ivar and ivar
 // quantised to 64-bit fixed point with one power-of-two scale per band.
 int pack_joint_bands(const BlsCurves* bv, double* tau, long long* qy, long long* qi,
-                     JointBand* jb, double* t_min_out) {
+                     uint8_t* band_of, JointBand* jb, double* t_min_out) {
     const int K = bv->n_curves;
     double t_min = INFINITY;
     for (int k = 0; k < K; ++k) {
@@ -859,9 +859,12 @@ int pack_joint_bands(const BlsCurves* bv, double* tau, long long* qy, long long*
             return std::max(-1000, std::min(1000, 61 - x));
         };
         const int e_y = exponent(abs_y), e_i = exponent(abs_i);
+        long long qi_total = 0;
         for (int64_t j = 0; j < n; ++j) {
             qy[b + j] = std::llrint(std::ldexp(yw[j], e_y));
             qi[b + j] = std::llrint(std::ldexp(iv[j], e_i));
+            qi_total += qi[b + j];
+            band_of[b + j] = (uint8_t)k;
         }
         JointBand& d = jb[k];
         std::memset(&d, 0, sizeof(d));
@@ -874,9 +877,33 @@ int pack_joint_bands(const BlsCurves* bv, double* tau, long long* qy, long long*
         d.ivar_floor = floor_v;
         d.y_unit = std::ldexp(1.0, -e_y);
         d.i_unit = std::ldexp(1.0, -e_i);
+        // a box holding every quantum of the band's weight: the kernel's FP64
+        // floor test on it, operation for operation (the product is exact)
+        d.qi_total = qi_total;
+        const double iv_all = (double)qi_total * d.i_unit;
+        const double out_all = d.sum_ivar - iv_all;
+        d.full_skip = (iv_all < d.ivar_floor || out_all < d.ivar_floor) ? 1 : 0;
+        // screen constants (the kernel's joint_screen); out of range or NaN
+        // turns the screen off for the star
+        const double ybar = d.sum_ivar > 0.0 ? d.sum_y / d.sum_ivar : NAN;
+        d.ybar_n = (float)(ybar * d.i_unit / d.y_unit);
+        d.s_n = (float)(d.sum_ivar / std::ldexp(d.i_unit, 61));
+        d.c_n = (float)std::ldexp(d.y_unit * d.y_unit / d.i_unit, 61);
+        d.floor_n = std::nextafter((float)(d.ivar_floor / std::ldexp(d.i_unit, 61)), INFINITY);
     }
     *t_min_out = t_min;
     return BLS_OK;
+}
+
+// The FP32 screen needs every band's constants well inside FP32's range.
+bool joint_screen_ok(const JointBand* jb, int K) {
+    for (int k = 0; k < K; ++k) {
+        const double ybar = jb[k].ybar_n, sn = jb[k].s_n, cn = jb[k].c_n;
+        if (!std::isfinite(ybar) || std::fabs(ybar) > 1e30) return false;
+        if (!(sn > 1e-30 && sn <= 2.0)) return false;
+        if (!(cn > 1e-30 && cn < 1e30)) return false;
+    }
+    return true;
 }
 
 int do_prepare_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, cudaStream_t st) {
@@ -899,10 +926,21 @@ int do_prepare_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, cudaSt
     const int64_t P_total = ns > 0 ? g->seg_offsets[ns] : 0;
     const int64_t n_pts = bv->offsets[K];
     if (P_total > INT32_MAX - (1 << 22)) return fail(BLS_E_RESOURCE, "too many trial periods");
+    if (n_pts > INT32_MAX - (1 << 22)) return fail(BLS_E_INVALID, "too many points in one star");
+
+    // the star's largest time offset bounds the fast fold's error
+    double t_lo = INFINITY, t_hi = -INFINITY;
+    for (int64_t j = 0; j < n_pts; ++j) {
+        t_lo = std::min(t_lo, bv->t[j]);
+        t_hi = std::max(t_hi, bv->t[j]);
+    }
+    const double tau_max = n_pts > 0 && std::isfinite(t_hi - t_lo) ? t_hi - t_lo : 0.0;
 
     // ---- segments (_segment, _bls_joint.py:138-144; _duration_bins) -------------
     std::vector<JointSegment> segs(std::max(ns, 1));
     std::vector<int32_t> nbins(P_total), dur_all;
+    std::vector<double> freq(P_total);
+    std::vector<uint32_t> scale(P_total, 0u);
     int64_t hist_stride = 2;
     for (int s = 0; s < ns; ++s) {
         const int64_t p0 = g->seg_offsets[s], p1 = g->seg_offsets[s + 1];
@@ -957,6 +995,28 @@ int do_prepare_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, cudaSt
         sd.hist_len = (int32_t)hl;
         hist_stride = std::max(hist_stride, hl);
         dur_all.insert(dur_all.end(), dur.begin(), dur.end());
+        // fast fold, with the single-band search's margins and checks
+        double fmax = 0.0, smax = 0.0;
+        for (int64_t i = p0; i < p1; ++i) {
+            fmax = std::max(fmax, 1.0 / g->periods[i]);
+            smax = std::max(smax, g->periods[i] / bin);
+        }
+        FoldParams fp = fold_params(width, bin, tau_max, fmax, smax);
+        const double sc_unit = std::ldexp(1.0, fp.fb);
+        for (int64_t i = p0; i < p1 && fp.fast; ++i) {
+            const double sc = std::nearbyint((g->periods[i] / bin) * sc_unit);
+            if (!(sc >= 1.0 && sc < 4294967296.0)) { fp.fast = false; break; }
+            // the fast fold's largest bin, ((S - 1) >> fb) + 1, must stay inside n_bins
+            if ((int64_t)(((uint32_t)sc - 1u) >> fp.fb) + 1 > nbins[i]) { fp.fast = false; break; }
+        }
+        for (int64_t i = p0; i < p1; ++i) {
+            freq[i] = 1.0 / g->periods[i];
+            scale[i] = fp.fast ? (uint32_t)std::nearbyint((g->periods[i] / bin) * sc_unit) : 0u;
+        }
+        sd.fast_fold = fp.fast ? 1 : 0;
+        sd.frac_bits = fp.fast ? fp.fb : 0;
+        sd.margin_u = fp.mu;
+        sd.margin_phi = fp.mphi;
     }
     if (P_total == 0) {
         e->joint_periods = 0;
@@ -969,16 +1029,19 @@ int do_prepare_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, cudaSt
     const bool in_smem = hist_bytes + joint_static_smem() + 1024 <= e->smem_optin;
     if (in_smem) CUDA_TRY(configure_joint(hist_bytes), "shared-memory opt-in");
     const int per_sm = std::max(1, joint_resident_ctas(in_smem, in_smem ? hist_bytes : 0));
-    int ctas = (int)std::min<int64_t>(P_total, (int64_t)e->n_sm * (in_smem ? per_sm : 2));
+    int ctas = (int)std::min<int64_t>(P_total, (int64_t)e->n_sm * per_sm);
 
     // ---- stage and upload (one copy) -------------------------------------------
     const size_t o_tau = 0;
     const size_t o_qy = o_tau + align256(8 * (size_t)n_pts);
     const size_t o_qi = o_qy + align256(8 * (size_t)n_pts);
-    const size_t o_band = o_qi + align256(8 * (size_t)n_pts);
+    const size_t o_bof = o_qi + align256(8 * (size_t)n_pts);
+    const size_t o_band = o_bof + align256((size_t)n_pts);
     const size_t o_seg = o_band + align256(sizeof(JointBand) * K);
     const size_t o_per = o_seg + align256(sizeof(JointSegment) * segs.size());
-    const size_t o_nb = o_per + align256(8 * (size_t)P_total);
+    const size_t o_freq = o_per + align256(8 * (size_t)P_total);
+    const size_t o_scale = o_freq + align256(8 * (size_t)P_total);
+    const size_t o_nb = o_scale + align256(4 * (size_t)P_total);
     const size_t o_dur = o_nb + align256(4 * (size_t)P_total);
     const size_t staged = o_dur + align256(4 * std::max<size_t>(dur_all.size(), 1));
     const size_t o_out = staged;
@@ -992,10 +1055,13 @@ int do_prepare_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, cudaSt
     if ((rc = pack_joint_bands(bv, reinterpret_cast<double*>(h + o_tau),
                                reinterpret_cast<long long*>(h + o_qy),
                                reinterpret_cast<long long*>(h + o_qi),
+                               reinterpret_cast<uint8_t*>(h + o_bof),
                                reinterpret_cast<JointBand*>(h + o_band), &t_min)))
         return rc;
     std::memcpy(h + o_seg, segs.data(), sizeof(JointSegment) * segs.size());
     std::memcpy(h + o_per, g->periods, 8 * (size_t)P_total);
+    std::memcpy(h + o_freq, freq.data(), 8 * (size_t)P_total);
+    std::memcpy(h + o_scale, scale.data(), 4 * (size_t)P_total);
     std::memcpy(h + o_nb, nbins.data(), 4 * (size_t)P_total);
     if (!dur_all.empty()) std::memcpy(h + o_dur, dur_all.data(), 4 * dur_all.size());
     if ((rc = e->d_joint.ensure(total))) return rc;
@@ -1007,9 +1073,12 @@ int do_prepare_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, cudaSt
     a.tau = reinterpret_cast<const double*>(d + o_tau);
     a.qy = reinterpret_cast<const long long*>(d + o_qy);
     a.qi = reinterpret_cast<const long long*>(d + o_qi);
+    a.band_of = reinterpret_cast<const uint8_t*>(d + o_bof);
     a.bands = reinterpret_cast<const JointBand*>(d + o_band);
     a.segments = reinterpret_cast<const JointSegment*>(d + o_seg);
     a.period = reinterpret_cast<const double*>(d + o_per);
+    a.freq = reinterpret_cast<const double*>(d + o_freq);
+    a.scale = reinterpret_cast<const uint32_t*>(d + o_scale);
     a.nbins = reinterpret_cast<const int32_t*>(d + o_nb);
     a.dur_bins = reinterpret_cast<const int32_t*>(d + o_dur);
     a.out = reinterpret_cast<double*>(d + o_out);
@@ -1019,6 +1088,8 @@ int do_prepare_joint(BlsEngine* e, const BlsGrid* g, const BlsCurves* bv, cudaSt
     a.work_counter = reinterpret_cast<int32_t*>(d + o_ctl);
     a.error_flag = reinterpret_cast<int32_t*>(d + o_ctl) + 8;
     a.t_min = t_min;
+    a.n_points = (int32_t)n_pts;
+    a.screen = joint_screen_ok(reinterpret_cast<const JointBand*>(h + o_band), K) ? 1 : 0;
     a.n_bands = K;
     a.n_segments = ns;
     a.obj_flag = g->objective;

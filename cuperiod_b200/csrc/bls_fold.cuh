@@ -1,9 +1,11 @@
-// The reference's phase bin of one point, in its own IEEE operations:
+// The reference's phase bin of one point.  fold_exact runs its own IEEE
+// operations:
 //   w = x - P*floor(x/P); ind = int(w/bin) + 1, clipped to [0, width-1]
 // (cuPeriod src/cuperiod/methods/_bls_core.py:369-376 / 536-538,
 // src/cuperiod/multiband/_bls_joint.py:442-449).  Every operation is rounded on
 // its own (no contraction), as the reference's compiled loop does.
 #pragma once
+#include <stdint.h>
 
 namespace blsb200 {
 
@@ -14,6 +16,22 @@ __device__ __forceinline__ int fold_exact(double x, double P, double bin, int wi
     ind = ind < 0 ? 0 : ind;
     ind = ind > width - 1 ? width - 1 : ind;
     return ind;
+}
+
+// Fast fold: q = x * RN(1/P) rounded onto a 2^-32 grid, then one 32-bit
+// multiply-high by S = round(P/bin * 2^fb).  Returns the reference's bin when
+// the scaled phase is provably away from every cycle and bin edge (margins mu
+// and mphi, derived on the host from the batch's largest time offset), else -1.
+__device__ __forceinline__ int fold_fast(double x, double f, uint32_t S, int fb, uint32_t fmask,
+                                         uint32_t mu, uint32_t fr_span, uint32_t mphi,
+                                         uint32_t phi_span) {
+    // x*f + 1.5*2^20 in one rounding: the ulp there is 2^-32, so the low word is
+    // round(frac(x*f) * 2^32)
+    const double qm = __fma_rn(x, f, 1572864.0);
+    const uint32_t phi = (uint32_t)__double2loint(qm);
+    const uint32_t v = __umulhi(phi, S);                 // phase * P/bin * 2^fb
+    const bool ok = ((phi - mphi) < phi_span) & (((v & fmask) - mu) < fr_span);
+    return ok ? (int)(v >> fb) + 1 : -1;
 }
 
 }  // namespace blsb200

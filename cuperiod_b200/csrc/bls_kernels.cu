@@ -78,20 +78,6 @@ struct TileShared {
     uint32_t thr_bits;              // the sweep's shared threshold (bits of a float >= 0)
 };
 
-// Fast fold.  Returns the reference's bin when the scaled phase is provably away
-// from every edge, else -1.
-__device__ __forceinline__ int fold_fast(double x, double f, uint32_t S, int fb, uint32_t fmask,
-                                         uint32_t mu, uint32_t fr_span, uint32_t mphi,
-                                         uint32_t phi_span) {
-    // x*f + 1.5*2^20 in one rounding: the ulp there is 2^-32, so the low word is
-    // round(frac(x*f) * 2^32)
-    const double qm = __fma_rn(x, f, 1572864.0);
-    const uint32_t phi = (uint32_t)__double2loint(qm);
-    const uint32_t v = __umulhi(phi, S);                 // phase * P/bin * 2^fb
-    const bool ok = ((phi - mphi) < phi_span) & (((v & fmask) - mu) < fr_span);
-    return ok ? (int)(v >> fb) + 1 : -1;
-}
-
 // Shared-memory accesses by 32-bit shared-space address (the hot loops compute
 // addresses in 32-bit arithmetic instead of converting generic pointers).
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
