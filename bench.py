@@ -322,6 +322,9 @@ JOINT_WORKLOAD = ("joint-ephemeris multi-band BLS: six-band stars (u/g/r/i/z/y s
                   "stacked baseline (~17,800 periods, 8 segments), snr objective")
 # FP64 divisions per SM clock on a B200 (profiles/pipe_rates.txt)
 DDIV_PER_SM_CLOCK = 7.163
+# DRAM bytes (read + write) of one joint launch over one star of this workload,
+# from one ncu capture (profiles/joint_kernel_6band_star.txt)
+JOINT_TRAFFIC_PER_STAR = 572416
 
 
 def joint_workload(n_stars: int, seed: int):
@@ -485,6 +488,7 @@ def run_joint_ours(args) -> None:
         except (OSError, ValueError):
             pass
         hbm = float(peaks.get("hbm_gbs", 6650.0))
+        hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
         alg_bytes = n_pts * 24 + n_per * 12 + n_per * 6 * 8
         achieved = alg_bytes / (ms_per_step / 1000.0) / 1e9
         out = {
@@ -497,8 +501,10 @@ def run_joint_ours(args) -> None:
                        "l2": "a star's bands and histograms live in L2 and shared memory; "
                              "no flush (the bound is the SM pipes)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None,
-                         "note": "SM-bound (FP64 box arithmetic); see sm_roofline"},
+                         "frac": achieved / hbm, "peak_source": hbm_src,
+                         "traffic": JOINT_TRAFFIC_PER_STAR * args.stars,
+                         "note": "SM-bound (FP32 screen, barriers, shared atomics); see "
+                                 "sm_roofline for the reference's FP64 division count"},
             "sm_roofline": {"bound": "fp64_div", "model_ms": 1000.0 * t_div,
                             "kernel_ms": ms_per_step, "frac": 1000.0 * t_div / ms_per_step},
             "clocks": clocks,

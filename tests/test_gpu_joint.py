@@ -6,8 +6,7 @@ is admissible.
 
 The engine's box sums are exact 64-bit fixed-point sums; the reference's are
 sequential FP64 sums.  Values therefore agree to rounding (relative 1e-6 is
-asserted, the observed differences are near 1e-12) and the chosen box agrees
-except where two boxes tie to rounding."""
+asserted) and the chosen box agrees except where two boxes tie to rounding."""
 
 from __future__ import annotations
 
