@@ -6,6 +6,7 @@ of ``periodogram_to_row`` (src/cuperiod/batch/io.py:507-571)."""
 from __future__ import annotations
 
 import hashlib
+import os
 from dataclasses import dataclass, field
 from typing import Any, Iterable, Sequence
 
@@ -155,7 +156,7 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                        grid: GridSpec | None = None, settings: Any = None,
                        columns: Any = None, domain: Domain | str | None = None,
                        band_column: str | None = None, n_best: int = 10,
-                       chunk_size: int = 4096, sink: str | None = None,
+                       chunk_size: int = 4096, sink: str | os.PathLike | None = None,
                        engine: _lib.Engine | None = None) -> BatchSummary:
     """Search many light curves; one engine launch per chunk of curves that share
     a trial grid (the explicit ``grid``, or curves whose default grids coincide).
@@ -165,7 +166,7 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
     glob) or a ``(DataFrame, group_column)`` tuple (``resolve_inputs``).  A curve
     that cannot be searched (too few points, no baseline, unreadable) is recorded
     in ``errors`` like the reference's per-curve failures (runner.py:248-249).
-    ``sink``: optional Parquet path for the rows.
+    ``sink``: optional ``.parquet`` or ``.csv`` path for the rows (``write_rows``).
     """
     m = get_method(method)
     s = _settings(settings)
@@ -216,9 +217,8 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                                             extra_keys=PEAK_EXTRA_COLUMNS, engine=eng))
             summary.launches += 1
     if sink is not None and summary.rows:
-        import pyarrow as pa
-        import pyarrow.parquet as pq
-        pq.write_table(pa.Table.from_pylist(summary.rows), sink)
+        from .sinks import write_rows
+        write_rows(summary.rows, sink)
     return summary
 
 
