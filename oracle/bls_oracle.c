@@ -343,3 +343,141 @@ int bls_oracle_joint(const double* tau, const double* yw, const double* wv, cons
     for (int i = 0; i < started; ++i) pthread_join(th[i], NULL);
     return atomic_load(&a.failed) ? 2 : 0;
 }
+
+/* ---- transit least squares (limb-darkened matched filter) --------------------
+ * The numba TLS kernel of src/cuperiod/methods/tls.py:516-593: per trial period
+ * the points are folded into n_bins phase bins (q = tau/P, ph = q - floor(q),
+ * bin = int(ph * n_bins) clipped), sums of yw and w in point order, the bins
+ * circularly padded by max_width - 1; each template g (widths dur_bins, samples
+ * at tmpl + tmpl_off) is slid over every start s with num = sum g a, cwg = sum
+ * g b, den = sum g^2 b accumulated in k order; a start counts when num < 0 and
+ * den > w_eps, and de = den - cwg^2 / w_total > den_rel * den; the first
+ * largest sr = num^2 / de in (width, start) order wins.  Outputs per period:
+ * sr, depth = -num/de, duration = width / n_bins * P, t0 = frac(centre) * P. */
+typedef struct {
+    const double *tau, *yw, *wv, *periods, *tmpl;
+    const int64_t *dur_bins, *tmpl_off;
+    int64_t n_points, n_periods, n_dur, n_bins, max_width;
+    double w_eps, w_total, den_rel;
+    double *o_sr, *o_depth, *o_duration, *o_t0;
+    atomic_long next;
+    atomic_int failed;
+} tls_args;
+
+static void tls_period(const tls_args* a, int64_t pidx, double* ab, double* acc)
+{
+    const int64_t nb = a->n_bins, n_ext = nb + a->max_width - 1;
+    double* A = ab;
+    double* B = ab + n_ext;
+    double* num = acc;
+    double* cwg = acc + nb;
+    double* den = acc + 2 * nb;
+    const double period = a->periods[pidx];
+    memset(ab, 0, sizeof(double) * 2 * (size_t)n_ext);
+    for (int64_t j = 0; j < a->n_points; ++j) {
+        const double q = a->tau[j] / period;
+        const double ph = q - floor(q);
+        int64_t bb = (int64_t)(ph * (double)nb);
+        if (bb > nb - 1) bb = nb - 1;
+        else if (bb < 0) bb = 0;
+        A[bb] += a->yw[j];
+        B[bb] += a->wv[j];
+    }
+    for (int64_t j = 0; j < a->max_width - 1; ++j) {
+        A[nb + j] = A[j];
+        B[nb + j] = B[j];
+    }
+    double loc_sr = 0.0, loc_depth = 0.0;
+    int64_t loc_start = 0, loc_width = 0;
+    for (int64_t di = 0; di < a->n_dur; ++di) {
+        const int64_t width = a->dur_bins[di];
+        const double* g = a->tmpl + a->tmpl_off[di];
+        const double g0 = g[0], g00 = g0 * g0;
+        for (int64_t s = 0; s < nb; ++s) {
+            num[s] = g0 * A[s];
+            cwg[s] = g0 * B[s];
+            den[s] = g00 * B[s];
+        }
+        for (int64_t k = 1; k < width; ++k) {
+            const double gk = g[k], gkk = gk * gk;
+            for (int64_t s = 0; s < nb; ++s) {
+                num[s] += gk * A[k + s];
+                cwg[s] += gk * B[k + s];
+                den[s] += gkk * B[k + s];
+            }
+        }
+        for (int64_t s = 0; s < nb; ++s) {
+            const double nm = num[s], dn = den[s];
+            if (nm < 0.0 && dn > a->w_eps) {
+                const double de = dn - cwg[s] * cwg[s] / a->w_total;
+                if (de > a->den_rel * dn) {
+                    const double sr = nm * nm / de;
+                    if (sr > loc_sr) {
+                        loc_sr = sr;
+                        loc_start = s;
+                        loc_width = width;
+                        loc_depth = -nm / de;
+                    }
+                }
+            }
+        }
+    }
+    a->o_sr[pidx] = loc_sr;
+    a->o_depth[pidx] = loc_depth;
+    a->o_duration[pidx] = (double)loc_width / (double)nb * period;
+    const double centre = ((double)loc_start + (double)loc_width / 2.0) / (double)nb;
+    a->o_t0[pidx] = (centre - floor(centre)) * period;
+}
+
+static void* tls_worker(void* arg)
+{
+    tls_args* a = (tls_args*)arg;
+    const int64_t n_ext = a->n_bins + a->max_width - 1;
+    double* ab = (double*)malloc(sizeof(double) * 2 * (size_t)n_ext);
+    double* acc = (double*)malloc(sizeof(double) * 3 * (size_t)a->n_bins);
+    if (!ab || !acc) {
+        atomic_store(&a->failed, 1);
+    } else {
+        for (;;) {
+            const int64_t p = atomic_fetch_add(&a->next, 1);
+            if (p >= a->n_periods) break;
+            tls_period(a, p, ab, acc);
+        }
+    }
+    free(ab);
+    free(acc);
+    return NULL;
+}
+
+int tls_oracle_search(const double* tau, const double* yw, const double* wv, int64_t n_points,
+                      const double* periods, int64_t n_periods, const int64_t* dur_bins,
+                      const int64_t* tmpl_off, const double* tmpl, int64_t n_dur,
+                      int64_t n_bins, double w_eps, double w_total, double den_rel,
+                      double* o_sr, double* o_depth, double* o_duration, double* o_t0,
+                      int n_threads)
+{
+    if (n_bins < 1 || n_dur < 1 || n_periods < 0) return 1;
+    int64_t max_width = 1;
+    for (int64_t di = 0; di < n_dur; ++di)
+        if (dur_bins[di] > max_width) max_width = dur_bins[di];
+    tls_args a = {
+        .tau = tau, .yw = yw, .wv = wv, .periods = periods, .tmpl = tmpl,
+        .dur_bins = dur_bins, .tmpl_off = tmpl_off, .n_points = n_points,
+        .n_periods = n_periods, .n_dur = n_dur, .n_bins = n_bins, .max_width = max_width,
+        .w_eps = w_eps, .w_total = w_total, .den_rel = den_rel, .o_sr = o_sr,
+        .o_depth = o_depth, .o_duration = o_duration, .o_t0 = o_t0,
+    };
+    atomic_init(&a.next, 0);
+    atomic_init(&a.failed, 0);
+    if (n_threads < 1) n_threads = 1;
+    if (n_threads > 512) n_threads = 512;
+    pthread_t th[512];
+    int started = 0;
+    for (int i = 1; i < n_threads; ++i) {
+        if (pthread_create(&th[started], NULL, tls_worker, &a) != 0) break;
+        ++started;
+    }
+    tls_worker(&a);
+    for (int i = 0; i < started; ++i) pthread_join(th[i], NULL);
+    return atomic_load(&a.failed) ? 2 : 0;
+}

@@ -55,6 +55,9 @@ def _load() -> ctypes.CDLL:
         lib.bls_oracle_joint.argtypes = [p, p, p, p, i64, p, p, p, p, i64, p, i64, d, i64,
                                          i64, i32, p, p, p, p, p, i32]
         lib.bls_oracle_joint.restype = i32
+        lib.tls_oracle_search.argtypes = [p, p, p, i64, p, i64, p, p, p, i64, i64, d, d, d,
+                                          p, p, p, p, i32]
+        lib.tls_oracle_search.restype = i32
         _lib = lib
     return _lib
 
@@ -491,6 +494,126 @@ def joint_power(jb: JointBands, periods, durations, oversample: int, obj_flag: i
     bn, bd, found, yin, ivin, spec = joint_sweep(jb, periods, durations, oversample,
                                                  obj_flag, n_threads)
     return joint_finish(jb, yin, ivin, bn, bd, found, spec.periods, spec.bin_duration)
+
+
+# --- transit least squares (methods/tls.py) -------------------------------------
+
+TLS_W_EPS = 1e-300          # tls.py:57
+TLS_DEN_REL = 1e-9          # tls.py:63
+TLS_CONSTANT_ULPS = 64.0    # tls.py:68
+TLS_OUTPUTS = ("sde", "sr", "depth", "duration", "t0")
+
+
+def tls_template(n: int, u1: float, u2: float) -> np.ndarray:
+    """``limb_darkened_template``, tls.py:84-111."""
+    if n <= 1:
+        return np.ones(max(n, 1), dtype=np.float64)
+    x = (np.arange(n, dtype=np.float64) + 0.5) / n - 0.5
+    z = np.clip(2.0 * np.abs(x), 0.0, 1.0)
+    mu = np.sqrt(1.0 - z * z)
+    g = 1.0 - u1 * (1.0 - mu) - u2 * (1.0 - mu) ** 2
+    g = np.where(z < 1.0, g, 0.0)
+    peak = float(g.max())
+    return g / peak if peak > 0.0 else g
+
+
+def tls_duration_bins(n_bins: int, dmin: float, dmax: float, n_dur: int) -> list[int]:
+    """``_duration_bins``, tls.py:114-126."""
+    fracs = np.geomspace(dmin, dmax, n_dur)
+    return sorted({min(max(int(round(f * n_bins)), 1), n_bins - 1) for f in fracs})
+
+
+def tls_period_grid(baseline: float, *, min_period: float, max_period: float, min_transits: int,
+                    grid_duration_frac: float, duration_min_frac: float,
+                    oversample: int) -> np.ndarray:
+    """``_period_grid`` (tls.py:141-170) without its size check."""
+    pmax = min(max_period, baseline / min_transits)
+    if pmax <= min_period:
+        return np.zeros(0, dtype=np.float64)
+    step = min(grid_duration_frac, 2.0 * duration_min_frac)        # _grid_duration_frac
+    df = step / (oversample * baseline)
+    freq = np.arange(1.0 / pmax, 1.0 / min_period, df)
+    if freq.size == 0:
+        return np.zeros(0, dtype=np.float64)
+    return np.ascontiguousarray(1.0 / freq[::-1], dtype=np.float64)
+
+
+def tls_kernel(tau, yw, w, periods, *, n_bins: int, dur_bins, templates, w_total: float,
+               den_rel: float = TLS_DEN_REL, n_threads: int | None = None):
+    """The numba kernel (tls.py:516-593) through the C restatement: sr, depth,
+    duration, t0 (t0 relative to tau's origin)."""
+    lib = _load()
+    tau = np.ascontiguousarray(tau, dtype=np.float64)
+    yw = np.ascontiguousarray(yw, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    per = np.ascontiguousarray(periods, dtype=np.float64)
+    tmpl = np.ascontiguousarray(np.concatenate([templates[wd] for wd in dur_bins]),
+                                dtype=np.float64)
+    widths = [len(templates[wd]) for wd in dur_bins]
+    off = np.zeros(len(dur_bins), dtype=np.int64)
+    if len(widths) > 1:
+        off[1:] = np.cumsum(widths[:-1])
+    db = np.ascontiguousarray(dur_bins, dtype=np.int64)
+    out = np.zeros((4, per.size), dtype=np.float64)
+    if n_threads is None:
+        n_threads = os.cpu_count() or 1
+    rc = lib.tls_oracle_search(_ptr(tau), _ptr(yw), _ptr(w), tau.size, _ptr(per), per.size,
+                               _ptr(db), _ptr(off), _ptr(tmpl), db.size, int(n_bins),
+                               TLS_W_EPS, float(w_total), float(den_rel), _ptr(out[0]),
+                               _ptr(out[1]), _ptr(out[2]), _ptr(out[3]), int(n_threads))
+    if rc != 0:
+        raise RuntimeError(f"oracle TLS search failed ({rc})")
+    return dict(zip(("sr", "depth", "duration", "t0"), out))
+
+
+def tls_host_inputs(t, y, dy):
+    """``tls_power``'s host steps (tls.py:680-699): t_ref, flux scale, weights,
+    weighted-mean-subtracted y*w; None when the flux is constant."""
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    t_ref = float(t.min())
+    scale_y = float(np.max(np.abs(y))) if y.size else 0.0
+    if y.size == 0 or float(np.ptp(y)) <= TLS_CONSTANT_ULPS * F64_EPS * scale_y:
+        return None, t_ref, 1.0
+    sc = float(np.std(y)) if dy is None else float(np.median(np.abs(dy)))
+    scale = 1.0 if not (math.isfinite(sc) and sc > 0.0) else \
+        2.0 ** min(max(round(math.log2(sc)), -1000), 1000)
+    y = y / scale
+    w = np.ones_like(y) if dy is None else \
+        1.0 / (np.ascontiguousarray(dy, dtype=np.float64) / scale) ** 2
+    w_total = float(w.sum())
+    y_mean = float(np.dot(w, y) / w_total)
+    yw = w * (y - y_mean)
+    return (t - t_ref, yw, w, w_total), t_ref, scale
+
+
+def tls_power(t, y, dy, periods, *, n_bins: int = 256, duration_min_frac: float = 0.01,
+              duration_max_frac: float = 0.10, n_durations: int = 5, u1: float = 0.4,
+              u2: float = 0.3, n_threads: int | None = None) -> dict[str, np.ndarray]:
+    """``tls_power`` (tls.py:624-755) with the numba kernel: sde, sr, depth,
+    duration and absolute t0 per period."""
+    periods = np.ascontiguousarray(periods, dtype=np.float64)
+    n_p = int(periods.size)
+    if n_p == 0:
+        return {k: np.zeros(0) for k in TLS_OUTPUTS}
+    prep, t_ref, scale = tls_host_inputs(t, y, dy)
+    dur = tls_duration_bins(n_bins, duration_min_frac, duration_max_frac, n_durations)
+    if prep is None or not dur:
+        out = {k: np.zeros(n_p) for k in TLS_OUTPUTS}
+        out["t0"] = np.full(n_p, t_ref)
+        return out
+    tau, yw, w, w_total = prep
+    templates = {wd: tls_template(wd, u1, u2) for wd in dur}
+    res = tls_kernel(tau, yw, w, periods, n_bins=n_bins, dur_bins=dur, templates=templates,
+                     w_total=w_total, n_threads=n_threads)
+    sr = res["sr"]
+    mean, std = float(sr.mean()), float(sr.std())
+    res["sde"] = (sr - mean) / std if std > 0.0 else np.zeros_like(sr)
+    res["depth"] = res["depth"] * scale
+    if dy is None:
+        res["sr"] = sr * (scale * scale)
+    res["t0"] = res["t0"] + t_ref
+    return res
 
 
 def best_index(power: np.ndarray) -> int:
