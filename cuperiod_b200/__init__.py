@@ -3,7 +3,9 @@
 A drop-in for cuPeriod's BLS path (``method="bls"`` through ``periodogram`` and
 ``batch_periodograms``): the same trial grids, objective, result object and best
 period, computed by hand-written sm_100a kernels behind a C ABI
-(``include/bls_b200.h``, ``libbls_b200.so``).  There is no CPU fallback: without
+(``include/bls_b200.h``, ``libbls_b200.so``).  Multi-band BLS (both
+statistics) and the transit least squares search (``method="tls"``) run on the
+same engine.  There is no CPU fallback: without
 the built library or a CUDA device the entry points raise
 ``BackendUnavailableError``.
 """
@@ -21,7 +23,8 @@ from .grid import GridSpec, check_grid_size, log_period_grid
 from .lightcurve import Domain, LightCurve, MultiBandLightCurve
 from .multiband import bls_multiband_power
 from .result import Peak, Periodogram
-from .settings import BLSSettings
+from .settings import BLSSettings, TLSSettings
+from .tls import TLSMethod, tls_power
 
 __version__ = "0.1.0"
 
@@ -32,5 +35,5 @@ __all__ = [
     "InsufficientDataError", "LightCurve", "MultiBandLightCurve", "Peak", "Periodogram", "UnknownMethodError",
     "batch_periodograms", "bls_multiband_power", "bls_power", "bls_power_many", "bls_power_segments",
     "check_grid_size", "get_method", "log_period_grid", "periodogram", "periodogram_to_row",
-    "register", "to_input",
+    "register", "to_input", "TLSMethod", "TLSSettings", "tls_power",
 ]

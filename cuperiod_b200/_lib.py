@@ -44,6 +44,16 @@ class BlsCurves(ctypes.Structure):
     _fields_ = [("n_curves", _i32), ("offsets", _vp), ("t", _vp), ("y", _vp), ("dy", _vp)]
 
 
+class BlsTlsInputs(ctypes.Structure):
+    _fields_ = [("n_curves", _i32), ("offsets", _vp), ("tau", _vp), ("yw", _vp), ("w", _vp),
+                ("w_total", _vp), ("n_bins", _i32), ("n_dur", _i32), ("dur_bins", _vp),
+                ("templates", _vp), ("den_rel", _dbl)]
+
+
+#: Per-period outputs of the TLS kernel, in the C ABI's order.
+TLS_FIELD_NAMES = ("sr", "depth", "duration", "t0")
+
+
 class BlsBatchInfo(ctypes.Structure):
     _fields_ = [("n_curves", _i32), ("n_segments", _i32), ("n_periods", _i64),
                 ("n_items", _i64), ("n_points", _i64), ("folds", _dbl), ("boxes", _dbl),
@@ -84,6 +94,7 @@ def load() -> ctypes.CDLL:
         lib.bls_search.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_batch_info.argtypes = [_vp, P(BlsBatchInfo)]
         lib.bls_search_joint.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
+        lib.bls_tls_search.argtypes = [_vp, P(BlsTlsInputs), _vp, _i64, _vp, _vp]
         lib.bls_joint_prepare.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp]
         lib.bls_joint_launch.argtypes = [_vp, _vp]
         lib.bls_joint_download.argtypes = [_vp, _vp, _vp]
@@ -94,7 +105,8 @@ def load() -> ctypes.CDLL:
                      "bls_download", "bls_device_output", "bls_download_best", "bls_search",
                      "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix",
                      "bls_launch_best_noalloc", "bls_download_rows", "bls_search_joint",
-                     "bls_joint_prepare", "bls_joint_launch", "bls_joint_download"):
+                     "bls_joint_prepare", "bls_joint_launch", "bls_joint_download",
+                     "bls_tls_search"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib
@@ -291,6 +303,32 @@ class Engine:
         g, c = grid.struct(), bands.struct()
         _check(self._lib.bls_search_joint(self._h, ctypes.byref(g), ctypes.byref(c),
                                           out.ctypes.data, stream))
+        return out
+
+    def tls_search(self, curves, periods, *, n_bins: int, dur_bins, templates,
+                   den_rel: float, stream: int | None = None) -> np.ndarray:
+        """The TLS matched filter of curves ``[(tau, yw, w, w_total), ...]`` over
+        ``periods``: ``(4, n_curves, n_periods)`` (``TLS_FIELD_NAMES``)."""
+        taus = [_f64(c[0]).ravel() for c in curves]
+        off = np.zeros(len(curves) + 1, dtype=np.int64)
+        off[1:] = np.cumsum([x.size for x in taus])
+        cat = lambda xs: _f64(np.concatenate(xs)) if xs else np.empty(0)
+        tau = cat(taus)
+        yw = cat([_f64(c[1]).ravel() for c in curves])
+        w = cat([_f64(c[2]).ravel() for c in curves])
+        if yw.size != tau.size or w.size != tau.size:
+            raise ValueError("tau, yw and w must have the same length")
+        w_total = _f64([float(c[3]) for c in curves])
+        db = np.ascontiguousarray(dur_bins, dtype=np.int32)
+        tmpl = _f64(np.concatenate([np.asarray(templates[int(d)], dtype=np.float64)
+                                    for d in db])) if db.size else np.empty(0)
+        per = _f64(periods).ravel()
+        inp = BlsTlsInputs(len(curves), _addr(off), _addr(tau), _addr(yw), _addr(w),
+                           _addr(w_total), int(n_bins), int(db.size), _addr(db), _addr(tmpl),
+                           float(den_rel))
+        out = np.empty((len(TLS_FIELD_NAMES), len(curves), per.size), dtype=np.float64)
+        _check(self._lib.bls_tls_search(self._h, ctypes.byref(inp), _addr(per), per.size,
+                                        out.ctypes.data, stream))
         return out
 
     def joint_prepare(self, grid: PackedGrid, bands: PackedCurves,

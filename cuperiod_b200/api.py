@@ -68,30 +68,36 @@ def to_input(data: Any, *, columns: Any = None,
                     "{band: LightCurve} mapping or a table")
 
 
-def _settings(settings: Any) -> BLSSettings:
+def _settings(settings: Any, cls: type = BLSSettings) -> Any:
+    """A settings object of the method's class: None gives the defaults, a mapping
+    is read directly or under the method's name (``{"TLS": {...}}``)."""
     if settings is None:
-        return BLSSettings()
-    if isinstance(settings, BLSSettings):
+        return cls()
+    if isinstance(settings, cls):
         return settings
     if isinstance(settings, Mapping):
-        if "BLS" in settings or "bls" in settings:
-            inner = settings.get("BLS", settings.get("bls"))
-            return _settings(inner)
-        return BLSSettings(**settings)
-    raise TypeError(f"settings must be BLSSettings or a mapping, got {type(settings).__name__}")
+        name = cls.__name__[:-len("Settings")]
+        for key in (name, name.lower()):
+            if key in settings:
+                return _settings(settings[key], cls)
+        return cls(**settings)
+    raise TypeError(f"settings must be {cls.__name__} or a mapping, "
+                    f"got {type(settings).__name__}")
 
 
 def periodogram(data: Any, method: str = "BLS", *, backend: str | None = "auto",
                 grid: GridSpec | None = None, settings: Any = None, columns: Any = None,
                 domain: Domain | str | None = None, engine=None) -> Periodogram:
-    """The BLS periodogram of one light curve (api.py:204-307): flux domain
+    """The BLS or TLS periodogram of one light curve (api.py:204-307): flux domain
     (magnitudes converted), the default grid unless ``grid`` is given, peak
     defaults from the settings."""
     m = get_method(method)
     lc = to_input(data, columns=columns, domain=domain)
-    s = _settings(settings)
+    s = _settings(settings, m.settings_cls)
     m.resolve_backend(backend if backend not in (None, "auto") else s.backend)
     if isinstance(lc, MultiBandLightCurve):
+        if not m.supports_multiband:
+            raise ValueError(f"{m.name} does not support multi-band input")
         from .multiband import multiband_default_grid
         g = grid or multiband_default_grid(m, lc, s)
         return m.multiband_power(g, lc, s, engine=engine).with_peak_defaults(s)

@@ -149,7 +149,7 @@ class BLSMethod:
 
     name: ClassVar[str] = "BLS"
     objective_sense: ClassVar[Literal["max", "min"]] = "max"
-    supports_multiband: ClassVar[bool] = False
+    supports_multiband: ClassVar[bool] = True
     natural_domain: ClassVar[Domain] = Domain.FLUX
     settings_cls: ClassVar[type] = BLSSettings
     gpu_backend: ClassVar[str] = BACKEND_NAME
@@ -307,7 +307,8 @@ def get_method(name: str) -> BLSMethod:
     from .errors import UnknownMethodError
     key = "".join(ch for ch in str(name) if ch.isalnum()).upper()
     if key not in _REGISTRY:
-        raise UnknownMethodError(f"unknown method {name!r}; this engine provides BLS")
+        raise UnknownMethodError(f"unknown method {name!r}; this engine provides "
+                                 f"{', '.join(sorted(_REGISTRY))}")
     return _REGISTRY[key]
 
 

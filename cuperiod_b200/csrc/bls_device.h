@@ -192,4 +192,49 @@ struct JointArgs {
     int32_t obj_flag;           // 0 snr, 1 log-likelihood
 };
 
+// ---- transit least squares (limb-darkened matched filter) --------------------
+// cuPeriod src/cuperiod/methods/tls.py.  Per curve the weighted residuals yw and
+// the weights w are quantised to 64-bit fixed point (a power-of-two scale each,
+// magnitudes summing below 2^61), stored in the same chunked point layout as
+// the BLS curves (kChunk), so a phase bin's sums are exact integers.
+
+constexpr int kTlsFields = 4;       // sr, depth, duration, t0 (from tau's origin)
+constexpr int kTlsMaxTile = 8;      // periods per work item
+constexpr int kTlsMaxDur = 64;
+
+struct TlsCurveDesc {
+    int64_t point_off;      // first point slot
+    int32_t n_points;
+    int32_t pad;
+    double w_total;         // the reference's float sum of w
+    double y_unit;          // reference units of one quantum of yw (2^-e)
+    double w_unit;          // reference units of one quantum of w
+};
+
+struct TlsArgs {
+    const TlsCurveDesc* curves;
+    const double* tau;          // per point slot: t - t_ref
+    const long long* qy;        // per point slot: quantised yw
+    const long long* qw;        // per point slot: quantised w
+    const double* period;       // the shared trial periods
+    const int32_t* dur_bins;    // template widths in bins
+    const int32_t* tmpl_off;    // offsets of the templates in tmpl
+    const double* tmpl;         // the templates, concatenated
+    double* out;                // kTlsFields x out_stride, field-major; curve c at c * P
+    int64_t out_stride;         // n_curves * n_periods
+    int64_t n_periods;
+    int32_t* work_counter;
+    int32_t* error_flag;
+    double w_eps;               // smallest admissible template energy (1e-300)
+    double den_rel;             // relative floor of the level-corrected energy
+    int32_t n_curves;
+    int32_t n_bins;
+    int32_t n_dur;
+    int32_t n_tmpl;             // samples of all templates
+    int32_t max_width;
+    int32_t tile;               // periods per work item (<= kTlsMaxTile)
+    int32_t tiles_per_curve;
+    int32_t n_items;
+};
+
 }  // namespace blsb200

@@ -199,9 +199,10 @@ struct BlsEngine {
 
     // device buffers
     DevBuf d_tau, d_pay_r, d_r64, d_iv64, d_period, d_freq, d_scale, d_nbins, d_dur, d_curves,
-        d_segments, d_rows, d_out, d_ctl, d_best, d_joint;
+        d_segments, d_rows, d_out, d_ctl, d_best, d_joint, d_tls;
     // pinned staging
-    HostBuf h_tau, h_pay_r, h_r64, h_iv64, h_grid, h_meta, h_ctl, h_best, h_rows, h_joint;
+    HostBuf h_tau, h_pay_r, h_r64, h_iv64, h_grid, h_meta, h_ctl, h_best, h_rows, h_joint,
+        h_tls;
 
     // the prepared batch
     bool prepared = false;
@@ -229,10 +230,10 @@ struct BlsEngine {
         if (graph) cudaGraphExecDestroy(graph);
         for (DevBuf* b : {&d_tau, &d_pay_r, &d_r64, &d_iv64, &d_period, &d_freq, &d_scale, &d_nbins,
                           &d_dur, &d_curves, &d_segments, &d_rows, &d_out, &d_ctl, &d_best,
-                          &d_joint})
+                          &d_joint, &d_tls})
             b->release();
         for (HostBuf* b : {&h_tau, &h_pay_r, &h_r64, &h_iv64, &h_grid, &h_meta, &h_ctl, &h_best,
-                           &h_rows, &h_joint})
+                           &h_rows, &h_joint, &h_tls})
             b->release();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -1134,6 +1135,168 @@ int do_download_joint(BlsEngine* e, double* out, cudaStream_t st) {
     return BLS_OK;
 }
 
+// ---- transit least squares ----------------------------------------------------
+
+// The largest power-of-two exponent e with total * 2^e below 2^61 (0 for an
+// all-zero or non-finite total).
+int fixed_exponent(double total) {
+    if (!(total > 0.0) || !std::isfinite(total)) return 0;
+    int x = 0;
+    std::frexp(total * (1.0 + 1e-12), &x);                  // total < 2^x
+    return std::max(-1000, std::min(1000, 61 - x));
+}
+
+int do_tls_search(BlsEngine* e, const BlsTlsInputs* in, const double* periods, int64_t P,
+                  double* out, cudaStream_t st) {
+    if (!in || (P > 0 && !periods) || !out) return fail(BLS_E_INVALID, "inputs are required");
+    const int nc = in->n_curves;
+    if (nc < 1 || !in->offsets || !in->tau || !in->yw || !in->w || !in->w_total)
+        return fail(BLS_E_INVALID, "at least one light curve is required");
+    if (in->offsets[0] != 0) return fail(BLS_E_INVALID, "offsets[0] must be 0");
+    const int nb = in->n_bins, nd = in->n_dur;
+    if (nb < 2 || nb > (1 << 20)) return fail(BLS_E_INVALID, "n_bins must be in [2, 2^20]");
+    if (nd < 1 || nd > kTlsMaxDur || !in->dur_bins || !in->templates)
+        return fail(BLS_E_INVALID, "1 to %d template widths are required", kTlsMaxDur);
+    int max_w = 1, n_tmpl = 0;
+    for (int d = 0; d < nd; ++d) {
+        const int w = in->dur_bins[d];
+        if (w < 1 || w > nb - 1)
+            return fail(BLS_E_INVALID, "template width %d outside [1, n_bins - 1]", w);
+        max_w = std::max(max_w, w);
+        n_tmpl += w;
+    }
+    for (int i = 0; i < n_tmpl; ++i)
+        if (!std::isfinite(in->templates[i]))
+            return fail(BLS_E_INVALID, "templates must be finite");
+    if (!(in->den_rel >= 0.0) || !std::isfinite(in->den_rel))
+        return fail(BLS_E_INVALID, "den_rel must be finite and >= 0");
+    for (int64_t i = 0; i < P; ++i)
+        if (!(std::isfinite(periods[i]) && periods[i] > 0.0))
+            return fail(BLS_E_INVALID, "TLS: trial periods must be finite and > 0");
+    if (P > INT32_MAX - (1 << 22)) return fail(BLS_E_RESOURCE, "too many trial periods");
+    const int64_t n_pts = in->offsets[nc];
+    for (int c = 0; c < nc; ++c) {
+        const int64_t b = in->offsets[c], en = in->offsets[c + 1];
+        if (en - b < 1 || en - b > INT32_MAX)
+            return fail(BLS_E_INVALID, "light curve %d has no points or too many", c);
+        if (!(std::isfinite(in->w_total[c]) && in->w_total[c] > 0.0))
+            return fail(BLS_E_INVALID, "light curve %d: w_total must be finite and > 0", c);
+        for (int64_t j = b; j < en; ++j)
+            if (!std::isfinite(in->tau[j]) || !std::isfinite(in->yw[j]) ||
+                !(std::isfinite(in->w[j]) && in->w[j] >= 0.0))
+                return fail(BLS_E_INVALID,
+                            "light curve %d: tau, yw and w must be finite (w >= 0)", c);
+    }
+    if (P == 0) return BLS_OK;
+
+    // one work item: a tile of periods, each one histogram of n_bins + max_w - 1 bins
+    const int ext = nb + max_w - 1;
+    int tile = (int)std::max<int64_t>(1, (48 * 1024 - 8 * (int64_t)n_tmpl) / (16 * (int64_t)ext));
+    tile = std::min<int>(tile, kTlsMaxTile);
+    const size_t smem = tls_smem_bytes(nb, max_w, tile, n_tmpl);
+    if (smem + 1024 > e->smem_optin)
+        return fail(BLS_E_RESOURCE,
+                    "TLS: %zu bytes of shared memory per period exceed the device's %zu; "
+                    "lower n_phase_bins", smem, e->smem_optin);
+    const int64_t tiles = (P + tile - 1) / tile;
+    if (tiles * nc > INT32_MAX - (1 << 22))
+        return fail(BLS_E_RESOURCE, "too many work items; split the batch");
+
+    // staging: descriptors, points (chunked layout), grid, templates
+    const size_t o_cur = 0;
+    const size_t o_tau = o_cur + align256(sizeof(TlsCurveDesc) * nc);
+    const size_t o_qy = o_tau + align256(8 * (size_t)n_pts);
+    const size_t o_qw = o_qy + align256(8 * (size_t)n_pts);
+    const size_t o_per = o_qw + align256(8 * (size_t)n_pts);
+    const size_t o_dur = o_per + align256(8 * (size_t)P);
+    const size_t o_off = o_dur + align256(4 * (size_t)nd);
+    const size_t o_tmpl = o_off + align256(4 * (size_t)nd);
+    const size_t staged = o_tmpl + align256(8 * (size_t)n_tmpl);
+    const size_t out_bytes = 8 * (size_t)kTlsFields * nc * P;
+    const size_t o_out = staged;
+    const size_t o_ctl = o_out + align256(out_bytes);
+    int rc;
+    if ((rc = e->h_tls.ensure(std::max(staged, out_bytes)))) return rc;
+    char* h = e->h_tls.as<char>();
+    TlsCurveDesc* cd = reinterpret_cast<TlsCurveDesc*>(h + o_cur);
+    double* htau = reinterpret_cast<double*>(h + o_tau);
+    long long* hqy = reinterpret_cast<long long*>(h + o_qy);
+    long long* hqw = reinterpret_cast<long long*>(h + o_qw);
+    parallel_for(nc, [&](int c, int) {
+        const int64_t b = in->offsets[c], n = in->offsets[c + 1] - b;
+        double abs_y = 0.0, sum_w = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            abs_y += std::fabs(in->yw[b + j]);
+            sum_w += in->w[b + j];
+        }
+        const int e_y = fixed_exponent(abs_y), e_w = fixed_exponent(sum_w);
+        for (int64_t j = 0; j < n; ++j) {
+            const int64_t m = b + point_slot(j, n);
+            htau[m] = in->tau[b + j];
+            hqy[m] = std::llrint(std::ldexp(in->yw[b + j], e_y));
+            hqw[m] = std::llrint(std::ldexp(in->w[b + j], e_w));
+        }
+        TlsCurveDesc& d = cd[c];
+        std::memset(&d, 0, sizeof(d));
+        d.point_off = b;
+        d.n_points = (int32_t)n;
+        d.w_total = in->w_total[c];
+        d.y_unit = std::ldexp(1.0, -e_y);
+        d.w_unit = std::ldexp(1.0, -e_w);
+    });
+    std::memcpy(h + o_per, periods, 8 * (size_t)P);
+    int32_t* hoff = reinterpret_cast<int32_t*>(h + o_off);
+    for (int d = 0, acc = 0; d < nd; ++d) {
+        reinterpret_cast<int32_t*>(h + o_dur)[d] = in->dur_bins[d];
+        hoff[d] = acc;
+        acc += in->dur_bins[d];
+    }
+    std::memcpy(h + o_tmpl, in->templates, 8 * (size_t)n_tmpl);
+    if ((rc = e->d_tls.ensure(o_ctl + 256))) return rc;
+    char* d = e->d_tls.as<char>();
+    CUDA_TRY(cudaMemcpyAsync(d, h, staged, cudaMemcpyHostToDevice, st), "upload TLS inputs");
+    CUDA_TRY(cudaMemsetAsync(d + o_ctl, 0, 256, st), "reset control words");
+
+    TlsArgs a{};
+    a.curves = reinterpret_cast<const TlsCurveDesc*>(d + o_cur);
+    a.tau = reinterpret_cast<const double*>(d + o_tau);
+    a.qy = reinterpret_cast<const long long*>(d + o_qy);
+    a.qw = reinterpret_cast<const long long*>(d + o_qw);
+    a.period = reinterpret_cast<const double*>(d + o_per);
+    a.dur_bins = reinterpret_cast<const int32_t*>(d + o_dur);
+    a.tmpl_off = reinterpret_cast<const int32_t*>(d + o_off);
+    a.tmpl = reinterpret_cast<const double*>(d + o_tmpl);
+    a.out = reinterpret_cast<double*>(d + o_out);
+    a.out_stride = (int64_t)nc * P;
+    a.n_periods = P;
+    a.work_counter = reinterpret_cast<int32_t*>(d + o_ctl);
+    a.error_flag = reinterpret_cast<int32_t*>(d + o_ctl) + 8;
+    a.w_eps = 1e-300;
+    a.den_rel = in->den_rel;
+    a.n_curves = nc;
+    a.n_bins = nb;
+    a.n_dur = nd;
+    a.n_tmpl = n_tmpl;
+    a.max_width = max_w;
+    a.tile = tile;
+    a.tiles_per_curve = (int32_t)tiles;
+    a.n_items = (int32_t)(tiles * nc);
+    CUDA_TRY(configure_tls(smem), "shared-memory opt-in");
+    const int per_sm = std::max(1, tls_resident_ctas(smem));
+    const int ctas = (int)std::min<int64_t>(a.n_items, (int64_t)e->n_sm * per_sm);
+    CUDA_TRY(launch_tls(a, ctas, smem, st), "TLS launch");
+    if ((rc = e->h_ctl.ensure(64))) return rc;
+    int32_t* hflag = e->h_ctl.as<int32_t>();
+    CUDA_TRY(cudaMemcpyAsync(h, d + o_out, out_bytes, cudaMemcpyDeviceToHost, st),
+             "download TLS fields");
+    CUDA_TRY(cudaMemcpyAsync(hflag, a.error_flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
+             "read error flag");
+    CUDA_TRY(cudaStreamSynchronize(st), "synchronize");
+    if (hflag[0] != 0) return fail(BLS_E_DEVICE, "the TLS kernel met an impossible descriptor");
+    std::memcpy(out, h, out_bytes);
+    return BLS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1392,6 +1555,13 @@ int bls_search_joint(BlsEngine* e, const BlsGrid* grid, const BlsCurves* bands, 
     if ((rc = bls_joint_prepare(e, grid, bands, stream))) return rc;
     if ((rc = bls_joint_launch(e, stream))) return rc;
     return bls_joint_download(e, out, stream);
+}
+
+int bls_tls_search(BlsEngine* e, const BlsTlsInputs* inputs, const double* periods,
+                   int64_t n_periods, double* out, void* stream) {
+    if (!e) return fail(BLS_E_INVALID, "engine is NULL");
+    if (n_periods < 0) return fail(BLS_E_INVALID, "n_periods must be >= 0");
+    return do_tls_search(e, inputs, periods, n_periods, out, pick(e, stream));
 }
 
 int bls_batch_info(BlsEngine* e, BlsBatchInfo* info) {

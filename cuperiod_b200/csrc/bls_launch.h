@@ -59,6 +59,13 @@ int joint_resident_ctas(bool in_smem, size_t smem);
 cudaError_t launch_joint(const JointArgs& args, bool in_smem, size_t smem, int n_ctas,
                          cudaStream_t stream);
 
+// Transit least squares (tls_kernels.cu): shared memory of one work item, the
+// opt-in, CTAs resident per SM and the persistent launch over every item.
+size_t tls_smem_bytes(int n_bins, int max_width, int tile, int n_tmpl);
+cudaError_t configure_tls(size_t smem);
+int tls_resident_ctas(size_t smem);
+cudaError_t launch_tls(const TlsArgs& args, int n_ctas, size_t smem, cudaStream_t stream);
+
 int search_threads();
 int max_resident_ctas(int mode, size_t smem);
 

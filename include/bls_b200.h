@@ -195,6 +195,39 @@ enum {
 int bls_search_joint(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* bands, double* out,
                      void* stream);
 
+/* A batch of light curves for the TLS matched filter, as the reference's kernel
+ * receives one (_tls_cuda / _tls_numba, src/cuperiod/methods/tls.py:428-491,
+ * 596-621): per point the time offset tau = t - t_ref, the weighted
+ * mean-subtracted flux yw = w (y - y_mean) and the weight w, per curve the
+ * float sum of w; per batch the phase-bin count, the template widths and the
+ * templates themselves (limb_darkened_template, concatenated in width order)
+ * and the relative floor of the level-corrected template energy.  The host
+ * steps of tls_power before the kernel (flux scale, weights, mean) stay with
+ * the caller, as in the reference.  All host pointers. */
+typedef struct {
+    int32_t n_curves;
+    const int64_t* offsets;       /* n_curves+1 offsets into tau / yw / w */
+    const double* tau;
+    const double* yw;
+    const double* w;
+    const double* w_total;        /* per curve */
+    int32_t n_bins;               /* phase bins (TLSSettings.n_phase_bins) */
+    int32_t n_dur;                /* template widths, 1 .. 64 */
+    const int32_t* dur_bins;      /* widths in bins, each in [1, n_bins - 1] */
+    const double* templates;      /* sum(dur_bins) samples */
+    double den_rel;               /* 1e-9 in float64 (_DEN_REL_EPS) */
+} BlsTlsInputs;
+
+/* The TLS matched filter of every curve over one period grid: the reference's
+ * per-period fold into n_bins phase bins, circular pad, sliding template
+ * correlation and joint level + depth fit, keeping the first largest signal
+ * residue (tls.py:516-593; the CUDA tls_block of tls.py:323-414).  out receives
+ * 4 x n_curves x n_periods values, field-major (sr, depth, duration, t0; t0
+ * measured from tau's origin, in [0, P)); the SDE normalisation and the unit
+ * conversions of tls_power stay with the caller.  Waits for the stream. */
+int bls_tls_search(BlsEngine* engine, const BlsTlsInputs* inputs, const double* periods,
+                   int64_t n_periods, double* out, void* stream);
+
 /* bls_search_joint in its three phases, as _joint_cuda runs them: the uploads
  * (joint_bands and the segment tables, 703-760), the launch (one persistent
  * launch for every segment) and the download of the fields (784-796).  A
