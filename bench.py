@@ -63,9 +63,11 @@ def parse_args():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target duration of the CPU-baseline sample")
-    p.add_argument("--workload", choices=("batch", "multiband-shared"), default="batch",
+    p.add_argument("--workload", choices=("batch", "multiband-shared", "tls"), default="batch",
                    help="batch: the headline batched search; multiband-shared: the "
-                        "joint-ephemeris multi-band search of --stars six-band stars")
+                        "joint-ephemeris multi-band search of --stars six-band stars; tls: "
+                        "the transit least squares search of --tls-curves curves")
+    p.add_argument("--tls-curves", type=int, default=32, help="tls: light curves per rank")
     p.add_argument("--stars", type=int, default=64, help="multiband-shared: stars per rank")
     return p.parse_args()
 
@@ -522,8 +524,194 @@ def run_joint_ours(args) -> None:
         dist.destroy_process_group()
 
 
+# ---- the transit least squares search ------------------------------------------
+
+TLS_METRIC = "TLS light curves/s on 1 B200"
+TLS_WORKLOAD = ("transit least squares: Kepler-like curves at 30-min cadence over 625 d, "
+                "N~U[10000,30000], default TLS grid over 0.5-12 d (119,788 periods), "
+                "256 phase bins, 5 limb-darkened templates")
+
+
+def tls_workload(n_curves: int, seed: int):
+    from cuperiod_b200.lightcurve import Domain, LightCurve
+    from cuperiod_b200.settings import TLSSettings
+    from cuperiod_b200.synthetic import tls_curves
+    from cuperiod_b200.tls import TLSMethod
+
+    settings = TLSSettings(min_period_days=0.5, max_period_days=12.0)
+    lcs = [LightCurve(c.t, c.y, c.dy, Domain.FLUX) for c in tls_curves(n_curves, seed=seed)]
+    grid = TLSMethod().default_grid(lcs[0], settings)
+    return lcs, grid, settings
+
+
+def tls_cpu_sample(lcs, periods, settings, seconds: float) -> dict:
+    """The reference's TLS kernel (the oracle's C port of its numba kernel, all
+    host cores) on curves of the workload until ``seconds`` have passed."""
+    from oracle import oracle
+    cores = os.cpu_count() or 1
+    done, t0, npts = 0, time.perf_counter(), 0
+    for lc in lcs:
+        oracle.tls_power(lc.time, lc.value, lc.error, periods, n_bins=settings.n_phase_bins,
+                         n_threads=cores)
+        done += 1
+        npts += lc.time.size
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    mean_n = float(np.mean([lc.time.size for lc in lcs]))
+    return {"value": done / dt * (npts / done) / mean_n, "unit": UNIT, "cores": cores,
+            "kind": "port",
+            "sample": f"{done} curves of the workload (mean N {npts / done:.0f}, rescaled to "
+                      f"the workload mean N {mean_n:.0f}) in {dt:.1f} s"}
+
+
+def run_tls_reference(args) -> None:
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    lcs, grid, settings = tls_workload(args.tls_curves, args.seed)
+    vals = [tls_cpu_sample(lcs, grid.period, settings, args.cpu_seconds)
+            for _ in range(args.steps)]
+    value = statistics.mean(v["value"] for v in vals)
+    print(json.dumps({
+        "impl": "reference", "metric": TLS_METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * args.tls_curves / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": TLS_WORKLOAD, "curves_per_rank": args.tls_curves,
+                   "cpu": "host cores"},
+        "cpu_baseline": dict(vals[-1], value=value),
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_tls_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from cuperiod_b200 import _lib
+    from cuperiod_b200.sharding import max_over_ranks
+    from cuperiod_b200.tls import (DEN_REL_EPS, TLSMethod, _prepare, duration_bins,
+                                   limb_darkened_template)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    lcs, grid, settings = tls_workload(args.tls_curves, args.seed + rank)
+    periods = grid.period
+    dur = duration_bins(settings)
+    templates = {w: limb_darkened_template(w, settings.limb_dark_u1, settings.limb_dark_u2)
+                 for w in dur}
+    inputs = [_prepare(lc.time, lc.value, lc.error)[0] for lc in lcs]
+    engine = _lib.Engine(device=local)
+    stream = torch.cuda.Stream(device=local)
+    handle = stream.cuda_stream
+    assert handle != 0
+    engine.tls_prepare(inputs, periods, n_bins=settings.n_phase_bins, dur_bins=dur,
+                       templates=templates, den_rel=DEN_REL_EPS, stream=handle)
+    for _ in range(args.warmup):
+        engine.tls_launch(handle)
+    engine.tls_download(handle)
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as sampler:
+        for i in range(args.steps):
+            starts[i].record(stream)
+            engine.tls_launch(handle)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.summary()
+    ms_per_step = max_over_ranks(starts[0].elapsed_time(ends[-1]) / args.steps)
+    kernel_ms = max_over_ranks(statistics.mean(s.elapsed_time(e) for s, e in zip(starts, ends)))
+    value = world * args.tls_curves / (ms_per_step / 1000.0)
+
+    # end to end: the public method on host arrays (host steps, upload, launch,
+    # download, SDE) for every curve of the step
+    e2e_ms = []
+    method = TLSMethod()
+    for i in range(args.steps):
+        barrier()
+        torch.cuda.synchronize()
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        pgs = method.power_many(grid, lcs, settings, engine=engine)
+        [pg.best_period() for pg in pgs]
+        e.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(s.elapsed_time(e))
+    e2e_value = world * args.tls_curves / (max_over_ranks(statistics.mean(e2e_ms)) / 1000.0)
+
+    if rank == 0:
+        n_pts = sum(lc.time.size for lc in lcs)
+        P = int(periods.size)
+        folds = float(n_pts) * P
+        corr = 6.0 * settings.n_phase_bins * sum(dur) * P * len(lcs)
+        f_clk = (clocks.get("sm_mhz") or 1900.0) * 1e6
+        n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+        # SM-pipe model: the fold's IEEE division per point-period at the probe's
+        # rate; the correlation's FP64 multiplies and adds at the DADD/DMUL rate
+        t_div = folds / (DDIV_PER_SM_CLOCK * n_sm * f_clk)
+        t_fp64 = corr / (108.0 * n_sm * f_clk)
+        t_model = max(t_div, t_fp64)
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        alg_bytes = n_pts * 24 + P * 8 + 4 * 8 * P * len(lcs)
+        achieved = alg_bytes / (kernel_ms / 1000.0) / 1e9
+        out = {
+            "metric": TLS_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": TLS_WORKLOAD, "curves_per_rank": args.tls_curves,
+                       "periods": P, "point_folds_per_step": folds * world,
+                       "l2": "a curve's points (~0.5 MB) are re-read from L2 per period tile; "
+                             "no flush (the bound is the SM pipes)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_source": hbm_src, "traffic": None,
+                         "note": "SM-bound (the fold's FP64 division and shared atomics, the "
+                                 "FP64 correlation); see sm_roofline"},
+            "sm_roofline": {"bound": "fp64_div" if t_div >= t_fp64 else "fp64",
+                            "model_ms": 1000.0 * t_model, "kernel_ms": kernel_ms,
+                            "frac": 1000.0 * t_model / kernel_ms},
+            "clocks": clocks,
+            "gpu_launches": args.steps,
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": n_pts * 24 + P * 8,
+                    "d2h_bytes_per_step": 4 * 8 * P * len(lcs)},
+        }
+        if world == 1:
+            out["cpu_baseline"] = tls_cpu_sample(lcs, periods, settings, args.cpu_seconds)
+        print(json.dumps(out), flush=True)
+    engine.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main() -> None:
     args = parse_args()
+    if args.workload == "tls":
+        run_tls_reference(args) if args.impl == "reference" else run_tls_ours(args)
+        return
     if args.workload == "multiband-shared":
         run_joint_reference(args) if args.impl == "reference" else run_joint_ours(args)
     elif args.impl == "reference":

@@ -95,6 +95,9 @@ def load() -> ctypes.CDLL:
         lib.bls_batch_info.argtypes = [_vp, P(BlsBatchInfo)]
         lib.bls_search_joint.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_tls_search.argtypes = [_vp, P(BlsTlsInputs), _vp, _i64, _vp, _vp]
+        lib.bls_tls_prepare.argtypes = [_vp, P(BlsTlsInputs), _vp, _i64, _vp]
+        lib.bls_tls_launch.argtypes = [_vp, _vp]
+        lib.bls_tls_download.argtypes = [_vp, _vp, _vp]
         lib.bls_joint_prepare.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp]
         lib.bls_joint_launch.argtypes = [_vp, _vp]
         lib.bls_joint_download.argtypes = [_vp, _vp, _vp]
@@ -106,7 +109,8 @@ def load() -> ctypes.CDLL:
                      "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix",
                      "bls_launch_best_noalloc", "bls_download_rows", "bls_search_joint",
                      "bls_joint_prepare", "bls_joint_launch", "bls_joint_download",
-                     "bls_tls_search"):
+                     "bls_tls_search", "bls_tls_prepare", "bls_tls_launch",
+                     "bls_tls_download"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib
@@ -215,6 +219,7 @@ class Engine:
         self._grid: PackedGrid | None = None
         self._curves: PackedCurves | None = None
         self._joint_periods = 0
+        self._tls_shape = (0, 0)
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -305,10 +310,10 @@ class Engine:
                                           out.ctypes.data, stream))
         return out
 
-    def tls_search(self, curves, periods, *, n_bins: int, dur_bins, templates,
-                   den_rel: float, stream: int | None = None) -> np.ndarray:
-        """The TLS matched filter of curves ``[(tau, yw, w, w_total), ...]`` over
-        ``periods``: ``(4, n_curves, n_periods)`` (``TLS_FIELD_NAMES``)."""
+    def tls_prepare(self, curves, periods, *, n_bins: int, dur_bins, templates,
+                    den_rel: float, stream: int | None = None) -> None:
+        """Upload curves ``[(tau, yw, w, w_total), ...]`` and ``periods`` for the
+        TLS matched filter (``bls_tls_prepare``)."""
         taus = [_f64(c[0]).ravel() for c in curves]
         off = np.zeros(len(curves) + 1, dtype=np.int64)
         off[1:] = np.cumsum([x.size for x in taus])
@@ -326,10 +331,27 @@ class Engine:
         inp = BlsTlsInputs(len(curves), _addr(off), _addr(tau), _addr(yw), _addr(w),
                            _addr(w_total), int(n_bins), int(db.size), _addr(db), _addr(tmpl),
                            float(den_rel))
-        out = np.empty((len(TLS_FIELD_NAMES), len(curves), per.size), dtype=np.float64)
-        _check(self._lib.bls_tls_search(self._h, ctypes.byref(inp), _addr(per), per.size,
-                                        out.ctypes.data, stream))
+        _check(self._lib.bls_tls_prepare(self._h, ctypes.byref(inp), _addr(per), per.size,
+                                         stream))
+        self._tls_shape = (len(curves), per.size)
+
+    def tls_launch(self, stream: int | None = None) -> None:
+        _check(self._lib.bls_tls_launch(self._h, stream))
+
+    def tls_download(self, stream: int | None = None) -> np.ndarray:
+        """``(4, n_curves, n_periods)`` (``TLS_FIELD_NAMES``)."""
+        out = np.empty((len(TLS_FIELD_NAMES),) + self._tls_shape, dtype=np.float64)
+        _check(self._lib.bls_tls_download(self._h, out.ctypes.data, stream))
         return out
+
+    def tls_search(self, curves, periods, *, n_bins: int, dur_bins, templates,
+                   den_rel: float, stream: int | None = None) -> np.ndarray:
+        """The TLS matched filter of curves ``[(tau, yw, w, w_total), ...]`` over
+        ``periods``: ``(4, n_curves, n_periods)`` (``TLS_FIELD_NAMES``)."""
+        self.tls_prepare(curves, periods, n_bins=n_bins, dur_bins=dur_bins,
+                         templates=templates, den_rel=den_rel, stream=stream)
+        self.tls_launch(stream)
+        return self.tls_download(stream)
 
     def joint_prepare(self, grid: PackedGrid, bands: PackedCurves,
                       stream: int | None = None) -> None:

@@ -218,6 +218,13 @@ struct BlsEngine {
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
 
+    // the prepared TLS search
+    bool tls_prepared = false;
+    TlsArgs targs{};
+    size_t tls_smem = 0;
+    int tls_ctas = 0;
+    size_t tls_out_bytes = 0;
+
     // the prepared joint (multi-band, shared box) search
     bool joint_prepared = false;
     JointArgs jargs{};
@@ -1146,9 +1153,10 @@ int fixed_exponent(double total) {
     return std::max(-1000, std::min(1000, 61 - x));
 }
 
-int do_tls_search(BlsEngine* e, const BlsTlsInputs* in, const double* periods, int64_t P,
-                  double* out, cudaStream_t st) {
-    if (!in || (P > 0 && !periods) || !out) return fail(BLS_E_INVALID, "inputs are required");
+int do_prepare_tls(BlsEngine* e, const BlsTlsInputs* in, const double* periods, int64_t P,
+                   cudaStream_t st) {
+    e->tls_prepared = false;
+    if (!in || (P > 0 && !periods)) return fail(BLS_E_INVALID, "inputs are required");
     const int nc = in->n_curves;
     if (nc < 1 || !in->offsets || !in->tau || !in->yw || !in->w || !in->w_total)
         return fail(BLS_E_INVALID, "at least one light curve is required");
@@ -1187,7 +1195,11 @@ int do_tls_search(BlsEngine* e, const BlsTlsInputs* in, const double* periods, i
                 return fail(BLS_E_INVALID,
                             "light curve %d: tau, yw and w must be finite (w >= 0)", c);
     }
-    if (P == 0) return BLS_OK;
+    if (P == 0) {
+        e->tls_out_bytes = 0;
+        e->tls_prepared = true;
+        return BLS_OK;
+    }
 
     // one work item: a tile of periods, each one histogram of n_bins + max_w - 1 bins
     const int ext = nb + max_w - 1;
@@ -1283,17 +1295,38 @@ int do_tls_search(BlsEngine* e, const BlsTlsInputs* in, const double* periods, i
     a.n_items = (int32_t)(tiles * nc);
     CUDA_TRY(configure_tls(smem), "shared-memory opt-in");
     const int per_sm = std::max(1, tls_resident_ctas(smem));
-    const int ctas = (int)std::min<int64_t>(a.n_items, (int64_t)e->n_sm * per_sm);
-    CUDA_TRY(launch_tls(a, ctas, smem, st), "TLS launch");
+    e->targs = a;
+    e->tls_smem = smem;
+    e->tls_ctas = (int)std::min<int64_t>(a.n_items, (int64_t)e->n_sm * per_sm);
+    e->tls_out_bytes = out_bytes;
+    e->tls_prepared = true;
+    return BLS_OK;
+}
+
+int do_launch_tls(BlsEngine* e, cudaStream_t st) {
+    if (!e->tls_prepared) return fail(BLS_E_STATE, "bls_tls_launch before bls_tls_prepare");
+    if (e->tls_out_bytes == 0) return BLS_OK;
+    CUDA_TRY(cudaMemsetAsync(e->targs.work_counter, 0, 64, st), "reset control words");
+    CUDA_TRY(launch_tls(e->targs, e->tls_ctas, e->tls_smem, st), "TLS launch");
+    return BLS_OK;
+}
+
+int do_download_tls(BlsEngine* e, double* out, cudaStream_t st) {
+    if (!e->tls_prepared) return fail(BLS_E_STATE, "bls_tls_download before bls_tls_prepare");
+    if (e->tls_out_bytes == 0) return BLS_OK;
+    int rc;
     if ((rc = e->h_ctl.ensure(64))) return rc;
     int32_t* hflag = e->h_ctl.as<int32_t>();
-    CUDA_TRY(cudaMemcpyAsync(h, d + o_out, out_bytes, cudaMemcpyDeviceToHost, st),
+    // the staging buffer holds at least the output (do_prepare_tls)
+    char* h = e->h_tls.as<char>();
+    CUDA_TRY(cudaMemcpyAsync(h, e->targs.out, e->tls_out_bytes, cudaMemcpyDeviceToHost, st),
              "download TLS fields");
-    CUDA_TRY(cudaMemcpyAsync(hflag, a.error_flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
+    CUDA_TRY(cudaMemcpyAsync(hflag, e->targs.error_flag, sizeof(int32_t),
+                             cudaMemcpyDeviceToHost, st),
              "read error flag");
     CUDA_TRY(cudaStreamSynchronize(st), "synchronize");
     if (hflag[0] != 0) return fail(BLS_E_DEVICE, "the TLS kernel met an impossible descriptor");
-    std::memcpy(out, h, out_bytes);
+    std::memcpy(out, h, e->tls_out_bytes);
     return BLS_OK;
 }
 
@@ -1557,11 +1590,31 @@ int bls_search_joint(BlsEngine* e, const BlsGrid* grid, const BlsCurves* bands, 
     return bls_joint_download(e, out, stream);
 }
 
-int bls_tls_search(BlsEngine* e, const BlsTlsInputs* inputs, const double* periods,
-                   int64_t n_periods, double* out, void* stream) {
+int bls_tls_prepare(BlsEngine* e, const BlsTlsInputs* inputs, const double* periods,
+                    int64_t n_periods, void* stream) {
     if (!e) return fail(BLS_E_INVALID, "engine is NULL");
     if (n_periods < 0) return fail(BLS_E_INVALID, "n_periods must be >= 0");
-    return do_tls_search(e, inputs, periods, n_periods, out, pick(e, stream));
+    return do_prepare_tls(e, inputs, periods, n_periods, pick(e, stream));
+}
+
+int bls_tls_launch(BlsEngine* e, void* stream) {
+    if (!e) return fail(BLS_E_INVALID, "engine is NULL");
+    return do_launch_tls(e, pick(e, stream));
+}
+
+int bls_tls_download(BlsEngine* e, double* out, void* stream) {
+    if (!e) return fail(BLS_E_INVALID, "engine is NULL");
+    if (!out) return fail(BLS_E_INVALID, "output pointer is NULL");
+    return do_download_tls(e, out, pick(e, stream));
+}
+
+int bls_tls_search(BlsEngine* e, const BlsTlsInputs* inputs, const double* periods,
+                   int64_t n_periods, double* out, void* stream) {
+    int rc;
+    if (!out) return fail(BLS_E_INVALID, "output pointer is NULL");
+    if ((rc = bls_tls_prepare(e, inputs, periods, n_periods, stream))) return rc;
+    if ((rc = bls_tls_launch(e, stream))) return rc;
+    return bls_tls_download(e, out, stream);
 }
 
 int bls_batch_info(BlsEngine* e, BlsBatchInfo* info) {

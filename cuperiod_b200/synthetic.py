@@ -23,6 +23,13 @@ cadences, lengths and value distributions:
   log-uniform [1e-3, 1e-2] scaled 0.7-1.3x from u to y, period log-uniform
   [0.5, 20] d, duration U[0.04, 0.3] d).  Searched with the shared box over the
   default grid of the stacked baseline.
+* :func:`tls_curves` -- Kepler-like long-cadence light curves for the TLS
+  search: a 30-minute cadence over 625 d, N ~ U[10000, 30000] points kept at
+  random (the first and last always, so every curve has the same baseline and
+  default grid), flux 1 + N(0, sigma), sigma log-uniform in [1e-4, 1e-3], errors
+  sigma x U[0.9, 1.1]; half carry a box transit (period log-uniform [0.5, 12] d,
+  duration U[0.05, 0.3] d, depth log-uniform [1e-4, 3e-3]).  Searched over
+  0.5-12 d on the default TLS grid.
 """
 
 from __future__ import annotations
@@ -147,5 +154,28 @@ def multiband_stars(n_stars: int, *, seed: int = 0, span: float = 90.0,
     return stars
 
 
+def tls_curves(n_curves: int, *, seed: int = 0, n_range=(10000, 30000)) -> list[Curve]:
+    """The TLS workload's light curves (see the module docstring)."""
+    rng = np.random.default_rng(seed)
+    base = np.arange(30000) * (30.0 / 1440.0)               # 625 d at 30-minute cadence
+    out = []
+    for _ in range(n_curves):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        inner = rng.choice(np.arange(1, base.size - 1), n - 2, replace=False)
+        t = base[np.sort(np.concatenate([[0, base.size - 1], inner]))] + 2454964.5
+        sigma = 10.0 ** rng.uniform(-4.0, -3.0)
+        y = 1.0 + rng.normal(0.0, sigma, t.size)
+        transit = None
+        if rng.random() < 0.5:
+            period = 10.0 ** rng.uniform(np.log10(0.5), np.log10(12.0))
+            duration = rng.uniform(0.05, 0.3)
+            depth = 10.0 ** rng.uniform(-4.0, np.log10(3e-3))
+            _box(t, rng, period, duration, depth, y)
+            transit = (period, duration, depth)
+        out.append(Curve(t, y, sigma * rng.uniform(0.9, 1.1, t.size), transit))
+    return out
+
+
 __all__ = ["Curve", "MULTIBAND_BANDS", "batched_curves", "batched_periods",
-           "long_baseline_curves", "long_baseline_periods", "multiband_stars", "single_curve"]
+           "long_baseline_curves", "long_baseline_periods", "multiband_stars", "single_curve",
+           "tls_curves"]

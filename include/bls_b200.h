@@ -228,6 +228,15 @@ typedef struct {
 int bls_tls_search(BlsEngine* engine, const BlsTlsInputs* inputs, const double* periods,
                    int64_t n_periods, double* out, void* stream);
 
+/* bls_tls_search in its three phases, as _tls_cuda runs them (uploads, launch,
+ * download).  A prepared batch stays on the device: bls_tls_launch may run
+ * again; the next bls_tls_prepare replaces it.  bls_tls_download waits for the
+ * stream. */
+int bls_tls_prepare(BlsEngine* engine, const BlsTlsInputs* inputs, const double* periods,
+                    int64_t n_periods, void* stream);
+int bls_tls_launch(BlsEngine* engine, void* stream);
+int bls_tls_download(BlsEngine* engine, double* out, void* stream);
+
 /* bls_search_joint in its three phases, as _joint_cuda runs them: the uploads
  * (joint_bands and the segment tables, 703-760), the launch (one persistent
  * launch for every segment) and the download of the fields (784-796).  A
