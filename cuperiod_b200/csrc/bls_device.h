@@ -196,11 +196,12 @@ struct JointArgs {
 // cuPeriod src/cuperiod/methods/tls.py.  Per curve the weighted residuals yw and
 // the weights w are quantised to 64-bit fixed point (a power-of-two scale each,
 // magnitudes summing below 2^61), stored in the same chunked point layout as
-// the BLS curves (kChunk), so a phase bin's sums are exact integers.
+// the BLS curves (kChunk); a phase bin's sums are exact int64s.
 
 constexpr int kTlsFields = 4;       // sr, depth, duration, t0 (from tau's origin)
 constexpr int kTlsMaxTile = 8;      // periods per work item
 constexpr int kTlsMaxDur = 64;
+constexpr int kTlsMaxPoints = INT32_MAX;
 
 struct TlsCurveDesc {
     int64_t point_off;      // first point slot

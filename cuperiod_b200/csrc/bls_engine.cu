@@ -1144,15 +1144,6 @@ int do_download_joint(BlsEngine* e, double* out, cudaStream_t st) {
 
 // ---- transit least squares ----------------------------------------------------
 
-// The largest power-of-two exponent e with total * 2^e below 2^61 (0 for an
-// all-zero or non-finite total).
-int fixed_exponent(double total) {
-    if (!(total > 0.0) || !std::isfinite(total)) return 0;
-    int x = 0;
-    std::frexp(total * (1.0 + 1e-12), &x);                  // total < 2^x
-    return std::max(-1000, std::min(1000, 61 - x));
-}
-
 int do_prepare_tls(BlsEngine* e, const BlsTlsInputs* in, const double* periods, int64_t P,
                    cudaStream_t st) {
     e->tls_prepared = false;
@@ -1185,8 +1176,9 @@ int do_prepare_tls(BlsEngine* e, const BlsTlsInputs* in, const double* periods, 
     const int64_t n_pts = in->offsets[nc];
     for (int c = 0; c < nc; ++c) {
         const int64_t b = in->offsets[c], en = in->offsets[c + 1];
-        if (en - b < 1 || en - b > INT32_MAX)
-            return fail(BLS_E_INVALID, "light curve %d has no points or too many", c);
+        if (en - b < 1 || en - b > kTlsMaxPoints)
+            return fail(BLS_E_INVALID, "light curve %d: TLS needs 1 to %d points", c,
+                        kTlsMaxPoints);
         if (!(std::isfinite(in->w_total[c]) && in->w_total[c] > 0.0))
             return fail(BLS_E_INVALID, "light curve %d: w_total must be finite and > 0", c);
         for (int64_t j = b; j < en; ++j)
@@ -1203,7 +1195,8 @@ int do_prepare_tls(BlsEngine* e, const BlsTlsInputs* in, const double* periods, 
 
     // one work item: a tile of periods, each one histogram of n_bins + max_w - 1 bins
     const int ext = nb + max_w - 1;
-    int tile = (int)std::max<int64_t>(1, (48 * 1024 - 8 * (int64_t)n_tmpl) / (16 * (int64_t)ext));
+    const int64_t per_period = 16 * (int64_t)ext;
+    int tile = (int)std::max<int64_t>(1, (64 * 1024 - 8 * (int64_t)n_tmpl) / per_period);
     tile = std::min<int>(tile, kTlsMaxTile);
     const size_t smem = tls_smem_bytes(nb, max_w, tile, n_tmpl);
     if (smem + 1024 > e->smem_optin)
@@ -1236,12 +1229,19 @@ int do_prepare_tls(BlsEngine* e, const BlsTlsInputs* in, const double* periods, 
     long long* hqw = reinterpret_cast<long long*>(h + o_qw);
     parallel_for(nc, [&](int c, int) {
         const int64_t b = in->offsets[c], n = in->offsets[c + 1] - b;
+        // 64-bit fixed point: the magnitudes sum below 2^61
         double abs_y = 0.0, sum_w = 0.0;
         for (int64_t j = 0; j < n; ++j) {
             abs_y += std::fabs(in->yw[b + j]);
             sum_w += in->w[b + j];
         }
-        const int e_y = fixed_exponent(abs_y), e_w = fixed_exponent(sum_w);
+        auto fixed_exp = [](double total) {
+            if (!(total > 0.0) || !std::isfinite(total)) return 0;
+            int x = 0;
+            std::frexp(total * (1.0 + 1e-12), &x);               // total < 2^x
+            return std::max(-1000, std::min(1000, 61 - x));
+        };
+        const int e_y = fixed_exp(abs_y), e_w = fixed_exp(sum_w);
         for (int64_t j = 0; j < n; ++j) {
             const int64_t m = b + point_slot(j, n);
             htau[m] = in->tau[b + j];

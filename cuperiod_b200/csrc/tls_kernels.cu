@@ -8,8 +8,12 @@
 //      the tile: the reference's bin, q = tau/P, ph = q - floor(q),
 //      bin = int(ph * n_bins) clipped, each operation IEEE-rounded on its own;
 //      a thread holds 8 time-consecutive points (the BLS engine's chunked
-//      layout), merges runs of equal bins in registers and adds the run's exact
-//      fixed-point sums of yw and w to the bin with 64-bit shared atomics;
+//      layout) and merges runs of equal bins in registers.  yw and w are 64-bit
+//      fixed point (a power-of-two scale per curve, magnitudes summing below
+//      2^61); a run's sum is added to a bin's int64 as two native 32-bit shared
+//      atomics, the low word first and then the high word plus the carry the
+//      low word's old value shows (64-bit shared atomics are emulated on
+//      sm_100), so every bin holds the exact integer sum;
 //   2. turns every bin into FP64 (one rounding of the exact sum) and pads the
 //      histogram circularly by max_width - 1 bins (the reference's pad);
 //   3. per period, one thread per start phase slides every template over the
@@ -64,10 +68,20 @@ __device__ __forceinline__ void tls_keep(double& sr, long long& key, double& dep
     }
 }
 
-__device__ __forceinline__ void flush_run(unsigned long long* h, int bin, long long ay,
-                                          long long aw) {
-    atomicAdd(h + 2 * bin, (unsigned long long)ay);
-    atomicAdd(h + 2 * bin + 1, (unsigned long long)aw);
+// Add v to the int64 at w[0..1] (little-endian words) with two 32-bit atomics:
+// the low word, then the high word with the carry out of the low word.  Each
+// add sees the old low word it added to, so every carry is counted once.
+__device__ __forceinline__ void add_i64(unsigned* w, long long v) {
+    const unsigned lo = (unsigned)v;
+    const unsigned old = atomicAdd(w, lo);
+    atomicAdd(w + 1, (unsigned)(v >> 32) + (old + lo < old ? 1u : 0u));
+}
+
+// Add a run's sums to one bin's {Y, W} record.
+__device__ __forceinline__ void flush_run(longlong2* bin, long long ay, long long aw) {
+    unsigned* w = reinterpret_cast<unsigned*>(bin);
+    add_i64(w, ay);
+    add_i64(w + 2, aw);
 }
 
 __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
@@ -75,7 +89,10 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
     __shared__ TlsShared s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nb = a.n_bins, ext = a.n_bins + a.max_width - 1;
+    // dynamic shared memory: the {Y, W} records (padded) of every period of the
+    // tile, turned into FP64 {a, b} in place after the fold; the templates
     longlong2* rec = reinterpret_cast<longlong2*>(tls_dyn);
+    double2* ab = reinterpret_cast<double2*>(tls_dyn);
     double* g = reinterpret_cast<double*>(rec + (size_t)a.tile * ext);
     for (int i = tid; i < a.n_tmpl; i += kTThreads) g[i] = a.tmpl[i];
     for (;;) {
@@ -87,8 +104,7 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
         const int64_t p0 = (int64_t)(item % a.tiles_per_curve) * a.tile;
         const int np = (int)min((int64_t)a.tile, a.n_periods - p0);
         const TlsCurveDesc cv = a.curves[c];
-        for (int i = tid; i < 2 * np * ext; i += kTThreads)
-            reinterpret_cast<long long*>(rec)[i] = 0;
+        for (int i = tid; i < np * ext; i += kTThreads) rec[i] = make_longlong2(0, 0);
         __syncthreads();
 
         // 1. fold: full chunks lane-interleaved, the tail in time order
@@ -106,14 +122,14 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
             }
             for (int p = 0; p < np; ++p) {
                 const double P = a.period[p0 + p];
-                unsigned long long* h = reinterpret_cast<unsigned long long*>(rec + p * ext);
+                longlong2* h = rec + (size_t)p * ext;
                 int prev = tls_bin(x[0], P, nb);
                 long long ay = yq[0], aw = wq[0];
 #pragma unroll
                 for (int r = 1; r < kTPts; ++r) {
                     const int b = tls_bin(x[r], P, nb);
                     if (b != prev) {
-                        flush_run(h, prev, ay, aw);
+                        flush_run(h + prev, ay, aw);
                         prev = b;
                         ay = yq[r];
                         aw = wq[r];
@@ -122,22 +138,19 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
                         aw += wq[r];
                     }
                 }
-                flush_run(h, prev, ay, aw);
+                flush_run(h + prev, ay, aw);
             }
         }
         for (int j = full + tid; j < n; j += kTThreads) {
             const int64_t slot = cv.point_off + j;
             const double xj = a.tau[slot];
             const long long yj = a.qy[slot], wj = a.qw[slot];
-            for (int p = 0; p < np; ++p) {
-                unsigned long long* h = reinterpret_cast<unsigned long long*>(rec + p * ext);
-                flush_run(h, tls_bin(xj, a.period[p0 + p], nb), yj, wj);
-            }
+            for (int p = 0; p < np; ++p)
+                flush_run(rec + (size_t)p * ext + tls_bin(xj, a.period[p0 + p], nb), yj, wj);
         }
         __syncthreads();
 
         // 2. FP64 bins (a = sum yw, b = sum w), then the circular pad (544-546)
-        double2* ab = reinterpret_cast<double2*>(rec);
         for (int i = tid; i < np * nb; i += kTThreads) {
             const int p = i / nb, bin = i - p * nb;
             const longlong2 e = rec[p * ext + bin];

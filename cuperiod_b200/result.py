@@ -122,19 +122,27 @@ class Periodogram:
         power = np.ascontiguousarray(power, dtype=np.float64)
         if frequency.ndim != 1 or power.shape != frequency.shape:
             raise ValueError("frequency must be 1-D and power of the same shape")
-        order = np.argsort(frequency, kind="stable")
-        frequency = frequency[order]
+        # the stable sort of a strictly monotone grid (every grid built from
+        # ascending periods) is the identity or a reversal: no gather needed
+        step = np.diff(frequency)
+        if frequency.size < 2 or bool(np.all(step > 0.0)):
+            order: Any = slice(None)
+        elif bool(np.all(step < 0.0)):
+            order = slice(None, None, -1)
+        else:
+            order = np.argsort(frequency, kind="stable")
+        frequency = np.ascontiguousarray(frequency[order])
         sorted_extras = {}
         for k, v in (extras or {}).items():
-            arr = np.ascontiguousarray(v, dtype=np.float64)
+            arr = np.asarray(v, dtype=np.float64)
             if arr.shape != frequency.shape:
                 raise ValueError(f"extras[{k!r}] shape does not match frequency")
-            sorted_extras[k] = arr[order]
+            sorted_extras[k] = np.ascontiguousarray(arr[order])
         with np.errstate(divide="ignore"):
             period = 1.0 / frequency
-        return cls(method, backend, frequency, period, power[order], objective_sense,
-                   int(n_samples), float(baseline), sorted_extras, dict(meta or {}),
-                   dict(peak_defaults or {}))
+        return cls(method, backend, frequency, period, np.ascontiguousarray(power[order]),
+                   objective_sense, int(n_samples), float(baseline), sorted_extras,
+                   dict(meta or {}), dict(peak_defaults or {}))
 
     def with_peak_defaults(self, defaults) -> "Periodogram":
         from .settings import peak_defaults as _from_settings

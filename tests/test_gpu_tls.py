@@ -3,8 +3,9 @@
 of that kernel on seeded curves.
 
 The engine's phase bins are the reference's bit for bit; its bin sums are exact
-fixed-point sums rounded once to FP64 where the reference adds FP64 values in
-point order, and from the bins on every operation is the reference's.  Values
+sums of 64-bit fixed-point values rounded once to FP64 where the reference adds
+FP64 values in point order, and from the bins on every operation is the
+reference's.  Values
 agree to rounding and the winning template and start agree except on near
 ties."""
 
@@ -106,3 +107,17 @@ def test_tls_rejects_bad_input():
                        **{**good, "dur_bins": [64], "templates": {64: np.ones(64)}})
     with pytest.raises(ValueError, match="periods"):
         eng.tls_search([(tau, np.zeros(50), np.ones(50), 50.0)], [0.0], **good)
+
+
+def test_tls_long_curve_bins_stay_exact():
+    # 600,000 points, many per bin: the fold's carry-propagating 32-bit atomics
+    # keep every bin's int64 sum exact at any count
+    from cuperiod_b200.settings import TLSSettings
+    from cuperiod_b200.tls import tls_power
+    t, y, dy = _curve(5, 600_000, span=400.0, period=4.7, depth=5e-4, noise=2e-3)
+    periods = np.array([1.3, 4.7, 9.1])
+    got = tls_power(t, y, dy, periods, settings=TLSSettings())
+    ref = oracle.tls_power(t, y, dy, periods, n_threads=8)
+    np.testing.assert_array_equal(got["duration"], ref["duration"])
+    np.testing.assert_array_equal(got["t0"], ref["t0"])
+    np.testing.assert_allclose(got["sr"], ref["sr"], rtol=1e-9)
