@@ -8,8 +8,9 @@
 // global counter.  Per period a CTA
 //   1. folds every point of the star into its band's histogram (per bin a
 //      16-byte record of the centred flux*weight and the weight, exact 64-bit
-//      fixed point, atomics in shared memory -- or in a per-CTA global slice
-//      when the bands do not fit); the bin is the reference's, from the fast
+//      fixed point, added with native 32-bit shared atomics and carries -- or
+//      in a per-CTA global slice when the bands do not fit); the bin is the
+//      reference's, from the fast
 //      fold where its margins prove it, else from the reference's IEEE chain;
 //   2. applies the reference's wrap pad per band and turns each histogram into
 //      prefix sums in place (every thread owns a run of bins of every band);
@@ -310,9 +311,9 @@ __global__ void __launch_bounds__(kJThreads, 1) joint_kernel(JointArgs a) {
                 atomicOr(a.error_flag, JERR_BIN);
                 continue;
             }
-            unsigned long long* r = reinterpret_cast<unsigned long long*>(hist + 2 * (k * L + ind));
-            atomicAdd(r, (unsigned long long)a.qy[j]);
-            atomicAdd(r + 1, (unsigned long long)a.qi[j]);
+            unsigned* r = reinterpret_cast<unsigned*>(hist + 2 * (k * L + ind));
+            add_i64(r, a.qy[j]);
+            add_i64(r + 2, a.qi[j]);
         }
         __syncthreads();
 

@@ -28,6 +28,7 @@
 #include <stdint.h>
 
 #include "bls_device.h"
+#include "bls_fold.cuh"
 #include "bls_launch.h"
 
 namespace blsb200 {
@@ -66,15 +67,6 @@ __device__ __forceinline__ void tls_keep(double& sr, long long& key, double& dep
         key = okey;
         depth = odepth;
     }
-}
-
-// Add v to the int64 at w[0..1] (little-endian words) with two 32-bit atomics:
-// the low word, then the high word with the carry out of the low word.  Each
-// add sees the old low word it added to, so every carry is counted once.
-__device__ __forceinline__ void add_i64(unsigned* w, long long v) {
-    const unsigned lo = (unsigned)v;
-    const unsigned old = atomicAdd(w, lo);
-    atomicAdd(w + 1, (unsigned)(v >> 32) + (old + lo < old ? 1u : 0u));
 }
 
 // Add a run's sums to one bin's {Y, W} record.
