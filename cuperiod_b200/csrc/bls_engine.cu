@@ -1195,7 +1195,7 @@ int do_prepare_tls(BlsEngine* e, const BlsTlsInputs* in, const double* periods, 
 
     // one work item: a tile of periods, each one histogram of n_bins + max_w - 1 bins
     const int ext = nb + max_w - 1;
-    const int64_t per_period = 16 * (int64_t)ext;
+    const int64_t per_period = 16 * (int64_t)ext + 16 * (int64_t)nb;
     int tile = (int)std::max<int64_t>(1, (64 * 1024 - 8 * (int64_t)n_tmpl) / per_period);
     tile = std::min<int>(tile, kTlsMaxTile);
     const size_t smem = tls_smem_bytes(nb, max_w, tile, n_tmpl);

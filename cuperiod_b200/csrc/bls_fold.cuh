@@ -34,15 +34,18 @@ __device__ __forceinline__ int fold_fast(double x, double f, uint32_t S, int fb,
     return ok ? (int)(v >> fb) + 1 : -1;
 }
 
-// Add v to the int64 at w[0..1] (little-endian words, shared memory) with two
-// native 32-bit atomics -- the low word, then the high word plus the carry out
-// of the low word -- where a 64-bit shared atomic would be emulated (sm_100).
+// Add v to an int64 kept as a low and a high 32-bit word (add_i64: the
+// little-endian words w[0..1]) with two native 32-bit atomics -- the low word,
+// then the high word plus the carry out of the low word -- where a 64-bit
+// shared atomic would be emulated (sm_100).
 // Each add sees the old low word it added to, so every carry is counted once
 // and the int64 is the exact sum at any number of adds.
-__device__ __forceinline__ void add_i64(unsigned* w, long long v) {
+__device__ __forceinline__ void add_i64_split(unsigned* lo_word, unsigned* hi_word, long long v) {
     const unsigned lo = (unsigned)v;
-    const unsigned old = atomicAdd(w, lo);
-    atomicAdd(w + 1, (unsigned)(v >> 32) + (old + lo < old ? 1u : 0u));
+    const unsigned old = atomicAdd(lo_word, lo);
+    atomicAdd(hi_word, (unsigned)(v >> 32) + (old + lo < old ? 1u : 0u));
 }
+
+__device__ __forceinline__ void add_i64(unsigned* w, long long v) { add_i64_split(w, w + 1, v); }
 
 }  // namespace blsb200

@@ -13,7 +13,9 @@
 //      2^61); a run's sum is added to a bin's int64 as two native 32-bit shared
 //      atomics, the low word first and then the high word plus the carry the
 //      low word's old value shows (64-bit shared atomics are emulated on
-//      sm_100), so every bin holds the exact integer sum;
+//      sm_100), so every bin holds the exact integer sum; the words lie in
+//      four planes (low and high of yw, of w), so different bins use
+//      different banks;
 //   2. turns every bin into FP64 (one rounding of the exact sum) and pads the
 //      histogram circularly by max_width - 1 bins (the reference's pad);
 //   3. per period, one thread per start phase slides every template over the
@@ -69,11 +71,17 @@ __device__ __forceinline__ void tls_keep(double& sr, long long& key, double& dep
     }
 }
 
-// Add a run's sums to one bin's {Y, W} record.
-__device__ __forceinline__ void flush_run(longlong2* bin, long long ay, long long aw) {
-    unsigned* w = reinterpret_cast<unsigned*>(bin);
-    add_i64(w, ay);
-    add_i64(w + 2, aw);
+// Add a run's sums to bin b of one period's four word planes (the low and high
+// words of Y, then of W, each plane `stride` words): plane-major, so that the
+// words of different bins fall on different banks.
+__device__ __forceinline__ void flush_run(unsigned* planes, int stride, int b, long long ay,
+                                          long long aw) {
+    add_i64_split(planes + b, planes + stride + b, ay);
+    add_i64_split(planes + 2 * stride + b, planes + 3 * stride + b, aw);
+}
+
+__device__ __forceinline__ long long plane_value(const unsigned* lo, const unsigned* hi, int b) {
+    return (long long)(((unsigned long long)hi[b] << 32) | lo[b]);
 }
 
 __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
@@ -81,11 +89,11 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
     __shared__ TlsShared s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nb = a.n_bins, ext = a.n_bins + a.max_width - 1;
-    // dynamic shared memory: the {Y, W} records (padded) of every period of the
-    // tile, turned into FP64 {a, b} in place after the fold; the templates
-    longlong2* rec = reinterpret_cast<longlong2*>(tls_dyn);
+    // dynamic shared memory: the FP64 bins {a, b} (padded) of every period of
+    // the tile, the four word planes of every period's exact sums, the templates
     double2* ab = reinterpret_cast<double2*>(tls_dyn);
-    double* g = reinterpret_cast<double*>(rec + (size_t)a.tile * ext);
+    unsigned* words = reinterpret_cast<unsigned*>(ab + (size_t)a.tile * ext);
+    double* g = reinterpret_cast<double*>(words + (size_t)a.tile * 4 * nb);
     for (int i = tid; i < a.n_tmpl; i += kTThreads) g[i] = a.tmpl[i];
     for (;;) {
         if (tid == 0) s.next = atomicAdd(a.work_counter, 1);
@@ -96,7 +104,7 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
         const int64_t p0 = (int64_t)(item % a.tiles_per_curve) * a.tile;
         const int np = (int)min((int64_t)a.tile, a.n_periods - p0);
         const TlsCurveDesc cv = a.curves[c];
-        for (int i = tid; i < np * ext; i += kTThreads) rec[i] = make_longlong2(0, 0);
+        for (int i = tid; i < np * 4 * nb; i += kTThreads) words[i] = 0u;
         __syncthreads();
 
         // 1. fold: full chunks lane-interleaved, the tail in time order
@@ -114,14 +122,14 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
             }
             for (int p = 0; p < np; ++p) {
                 const double P = a.period[p0 + p];
-                longlong2* h = rec + (size_t)p * ext;
+                unsigned* h = words + (size_t)p * 4 * nb;
                 int prev = tls_bin(x[0], P, nb);
                 long long ay = yq[0], aw = wq[0];
 #pragma unroll
                 for (int r = 1; r < kTPts; ++r) {
                     const int b = tls_bin(x[r], P, nb);
                     if (b != prev) {
-                        flush_run(h + prev, ay, aw);
+                        flush_run(h, nb, prev, ay, aw);
                         prev = b;
                         ay = yq[r];
                         aw = wq[r];
@@ -130,7 +138,7 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
                         aw += wq[r];
                     }
                 }
-                flush_run(h + prev, ay, aw);
+                flush_run(h, nb, prev, ay, aw);
             }
         }
         for (int j = full + tid; j < n; j += kTThreads) {
@@ -138,16 +146,19 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
             const double xj = a.tau[slot];
             const long long yj = a.qy[slot], wj = a.qw[slot];
             for (int p = 0; p < np; ++p)
-                flush_run(rec + (size_t)p * ext + tls_bin(xj, a.period[p0 + p], nb), yj, wj);
+                flush_run(words + (size_t)p * 4 * nb, nb, tls_bin(xj, a.period[p0 + p], nb), yj,
+                          wj);
         }
         __syncthreads();
 
         // 2. FP64 bins (a = sum yw, b = sum w), then the circular pad (544-546)
         for (int i = tid; i < np * nb; i += kTThreads) {
             const int p = i / nb, bin = i - p * nb;
-            const longlong2 e = rec[p * ext + bin];
-            ab[p * ext + bin] = make_double2(__dmul_rn(__ll2double_rn(e.x), cv.y_unit),
-                                             __dmul_rn(__ll2double_rn(e.y), cv.w_unit));
+            const unsigned* h = words + (size_t)p * 4 * nb;
+            const long long y = plane_value(h, h + nb, bin);
+            const long long w = plane_value(h + 2 * nb, h + 3 * nb, bin);
+            ab[p * ext + bin] = make_double2(__dmul_rn(__ll2double_rn(y), cv.y_unit),
+                                             __dmul_rn(__ll2double_rn(w), cv.w_unit));
         }
         __syncthreads();
         if (a.max_width > 1)
@@ -239,8 +250,8 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
 }  // namespace
 
 size_t tls_smem_bytes(int n_bins, int max_width, int tile, int n_tmpl) {
-    return (size_t)tile * (size_t)(n_bins + max_width - 1) * sizeof(longlong2) +
-           (size_t)n_tmpl * sizeof(double);
+    return (size_t)tile * (size_t)(n_bins + max_width - 1) * sizeof(double2) +
+           (size_t)tile * 4 * n_bins * sizeof(unsigned) + (size_t)n_tmpl * sizeof(double);
 }
 
 cudaError_t configure_tls(size_t smem) {
