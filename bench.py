@@ -322,8 +322,10 @@ JOINT_UNIT = "stars/s"
 JOINT_WORKLOAD = ("joint-ephemeris multi-band BLS: six-band stars (u/g/r/i/z/y share "
                   "6/9/26/26/17/16%), N~U[600,3000] points over 90 d, default grid of the "
                   "stacked baseline (~17,800 periods, 8 segments), snr objective")
-# FP64 divisions per SM clock on a B200 (profiles/pipe_rates.txt)
+# FP64 divisions and random-address 32-bit shared atomics per SM clock on a B200
+# (profiles/pipe_rates.txt)
 DDIV_PER_SM_CLOCK = 7.163
+SMEM_ATOM_U32_PER_SM_CLOCK = 16.671
 # DRAM bytes (read + write) of one joint launch over one star of this workload,
 # from one ncu capture (profiles/joint_kernel_6band_star.txt)
 JOINT_TRAFFIC_PER_STAR = 572416
@@ -663,11 +665,13 @@ def run_tls_ours(args) -> None:
         corr = 6.0 * settings.n_phase_bins * sum(dur) * P * len(lcs)
         f_clk = (clocks.get("sm_mhz") or 1900.0) * 1e6
         n_sm = torch.cuda.get_device_properties(local).multi_processor_count
-        # SM-pipe model: the fold's IEEE division per point-period at the probe's
-        # rate; the correlation's FP64 multiplies and adds at the DADD/DMUL rate
-        t_div = folds / (DDIV_PER_SM_CLOCK * n_sm * f_clk)
+        # SM-pipe model: the fold's four native 32-bit shared atomics per
+        # point-period (two per exact int64 sum, runs of equal bins not merged)
+        # at the probe's random-address rate; the correlation's FP64 multiplies
+        # and adds at the DADD/DMUL rate (profiles/pipe_rates.txt)
+        t_atom = folds * 4 / (SMEM_ATOM_U32_PER_SM_CLOCK * n_sm * f_clk)
         t_fp64 = corr / (108.0 * n_sm * f_clk)
-        t_model = max(t_div, t_fp64)
+        t_model = max(t_atom, t_fp64)
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -688,9 +692,9 @@ def run_tls_ours(args) -> None:
                              "no flush (the bound is the SM pipes)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_source": hbm_src, "traffic": None,
-                         "note": "SM-bound (the fold's FP64 division and shared atomics, the "
-                                 "FP64 correlation); see sm_roofline"},
-            "sm_roofline": {"bound": "fp64_div" if t_div >= t_fp64 else "fp64",
+                         "note": "SM-bound (the fold's shared atomics, the FP64 "
+                                 "correlation); see sm_roofline"},
+            "sm_roofline": {"bound": "smem_atomic" if t_atom >= t_fp64 else "fp64",
                             "model_ms": 1000.0 * t_model, "kernel_ms": kernel_ms,
                             "frac": 1000.0 * t_model / kernel_ms},
             "clocks": clocks,

@@ -218,6 +218,7 @@ struct TlsArgs {
     const long long* qy;        // per point slot: quantised yw
     const long long* qw;        // per point slot: quantised w
     const double* period;       // the shared trial periods
+    const double* freq;         // RN(1/P) (fast fold)
     const int32_t* dur_bins;    // template widths in bins
     const int32_t* tmpl_off;    // offsets of the templates in tmpl
     const double* tmpl;         // the templates, concatenated
@@ -226,6 +227,10 @@ struct TlsArgs {
     int64_t n_periods;
     int32_t* work_counter;
     int32_t* error_flag;
+    uint32_t margin_u;          // fast fold: bin-edge margin, units of 2^-32 bins
+    uint32_t margin_phi;        // fast fold: cycle-edge margin, units of 2^-32 cycles
+    int32_t fast_fold;          // 1: the fast fold's error bound holds for the batch
+    int32_t pad;
     double w_eps;               // smallest admissible template energy (1e-300)
     double den_rel;             // relative floor of the level-corrected energy
     int32_t n_curves;

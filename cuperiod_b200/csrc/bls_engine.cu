@@ -1213,7 +1213,8 @@ int do_prepare_tls(BlsEngine* e, const BlsTlsInputs* in, const double* periods, 
     const size_t o_qy = o_tau + align256(8 * (size_t)n_pts);
     const size_t o_qw = o_qy + align256(8 * (size_t)n_pts);
     const size_t o_per = o_qw + align256(8 * (size_t)n_pts);
-    const size_t o_dur = o_per + align256(8 * (size_t)P);
+    const size_t o_freq = o_per + align256(8 * (size_t)P);
+    const size_t o_dur = o_freq + align256(8 * (size_t)P);
     const size_t o_off = o_dur + align256(4 * (size_t)nd);
     const size_t o_tmpl = o_off + align256(4 * (size_t)nd);
     const size_t staged = o_tmpl + align256(8 * (size_t)n_tmpl);
@@ -1257,6 +1258,39 @@ int do_prepare_tls(BlsEngine* e, const BlsTlsInputs* in, const double* periods, 
         d.w_unit = std::ldexp(1.0, -e_w);
     });
     std::memcpy(h + o_per, periods, 8 * (size_t)P);
+    // fast fold: the phase frac(tau * RN(1/P)) on a 2^-32 grid is within e_phi
+    // cycles of frac(tau / P) (RN(1/P) and the grid), the reference's
+    // frac(RN(tau / P)) within e_ref, and its RN(ph * n_bins) within
+    // n_bins * 2^-53 bins; the kernel takes the fast bin only further than the
+    // sum from a cycle edge (mphi) and a bin edge (mu)
+    double* hfreq = reinterpret_cast<double*>(h + o_freq);
+    double f_max = 0.0, tau_max = 0.0;
+    for (int64_t i = 0; i < P; ++i) {
+        hfreq[i] = 1.0 / periods[i];
+        f_max = std::max(f_max, hfreq[i]);
+    }
+    for (int64_t j = 0; j < n_pts; ++j) tau_max = std::max(tau_max, std::fabs(in->tau[j]));
+    bool fast = false;
+    uint32_t mu = 0, mphi = 0;
+    {
+        const double q_max = tau_max * f_max;
+        bool tau_ok = true;
+        for (int64_t j = 0; j < n_pts && tau_ok; ++j) tau_ok = in->tau[j] >= 0.0;
+        if (tau_ok && q_max < 262144.0) {
+            const double two32 = 4294967296.0;
+            const double e_phi = q_max * std::ldexp(1.0, -52) * 1.01 + std::ldexp(1.0, -33);
+            const double e_ref = q_max * std::ldexp(1.0, -53);
+            const double m_phi = std::ceil((e_phi + e_ref) * two32) + 2.0;
+            const double m_u =
+                std::ceil(((double)nb * (e_phi + e_ref) + (double)nb * std::ldexp(1.0, -52)) *
+                          two32) + 2.0;
+            if (m_phi < 1e6 && m_u < 268435456.0) {
+                fast = true;
+                mu = (uint32_t)m_u;
+                mphi = (uint32_t)m_phi;
+            }
+        }
+    }
     int32_t* hoff = reinterpret_cast<int32_t*>(h + o_off);
     for (int d = 0, acc = 0; d < nd; ++d) {
         reinterpret_cast<int32_t*>(h + o_dur)[d] = in->dur_bins[d];
@@ -1275,6 +1309,10 @@ int do_prepare_tls(BlsEngine* e, const BlsTlsInputs* in, const double* periods, 
     a.qy = reinterpret_cast<const long long*>(d + o_qy);
     a.qw = reinterpret_cast<const long long*>(d + o_qw);
     a.period = reinterpret_cast<const double*>(d + o_per);
+    a.freq = reinterpret_cast<const double*>(d + o_freq);
+    a.margin_u = mu;
+    a.margin_phi = mphi;
+    a.fast_fold = fast ? 1 : 0;
     a.dur_bins = reinterpret_cast<const int32_t*>(d + o_dur);
     a.tmpl_off = reinterpret_cast<const int32_t*>(d + o_off);
     a.tmpl = reinterpret_cast<const double*>(d + o_tmpl);

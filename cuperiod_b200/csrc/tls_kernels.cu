@@ -6,7 +6,8 @@
 // kTlsMaxTile consecutive trial periods).  Per item a CTA
 //   1. folds every point of the curve into one phase histogram per period of
 //      the tile: the reference's bin, q = tau/P, ph = q - floor(q),
-//      bin = int(ph * n_bins) clipped, each operation IEEE-rounded on its own;
+//      bin = int(ph * n_bins) clipped -- from a fixed-point fast path where its
+//      host-derived margins prove the result, else from those IEEE operations;
 //      a thread holds 8 time-consecutive points (the BLS engine's chunked
 //      layout) and merges runs of equal bins in registers.  yw and w are 64-bit
 //      fixed point (a power-of-two scale per curve, magnitudes summing below
@@ -57,6 +58,21 @@ __device__ __forceinline__ int tls_bin(double x, double P, int n_bins) {
     int b = (int)__dmul_rn(ph, (double)n_bins);
     b = b > n_bins - 1 ? n_bins - 1 : b;
     return b < 0 ? 0 : b;
+}
+
+// Fast TLS bin: the phase frac(x * RN(1/P)) on a 2^-32 grid (one FMA, as the
+// BLS fast fold), times n_bins as a 64-bit integer product whose high word is
+// the bin and low word the position inside it.  Returns the reference's bin
+// when the phase is further than the combined rounding error from a cycle edge
+// (margin mphi) and from a bin edge (margin mu), else -1.
+__device__ __forceinline__ int tls_bin_fast(double x, double f, int n_bins, uint32_t mu,
+                                            uint32_t mphi) {
+    const double qm = __fma_rn(x, f, 1572864.0);
+    const uint32_t phi = (uint32_t)__double2loint(qm);
+    const unsigned long long prod = (unsigned long long)phi * (unsigned)n_bins;
+    const uint32_t fr = (uint32_t)prod;
+    const bool ok = ((phi - mphi) < (0u - 2u * mphi)) & ((fr - mu) < (0u - 2u * mu));
+    return ok ? (int)(prod >> 32) : -1;
 }
 
 // Of two candidates (sr, key = width index << 32 | start, depth), the one the
@@ -121,13 +137,20 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
                 wq[r] = a.qw[slot];
             }
             for (int p = 0; p < np; ++p) {
-                const double P = a.period[p0 + p];
+                const double P = a.period[p0 + p], f = a.freq[p0 + p];
                 unsigned* h = words + (size_t)p * 4 * nb;
-                int prev = tls_bin(x[0], P, nb);
+                int bins[kTPts];
+#pragma unroll
+                for (int r = 0; r < kTPts; ++r) {
+                    int b = a.fast_fold ? tls_bin_fast(x[r], f, nb, a.margin_u, a.margin_phi)
+                                        : -1;
+                    bins[r] = b >= 0 ? b : tls_bin(x[r], P, nb);
+                }
+                int prev = bins[0];
                 long long ay = yq[0], aw = wq[0];
 #pragma unroll
                 for (int r = 1; r < kTPts; ++r) {
-                    const int b = tls_bin(x[r], P, nb);
+                    const int b = bins[r];
                     if (b != prev) {
                         flush_run(h, nb, prev, ay, aw);
                         prev = b;
