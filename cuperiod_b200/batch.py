@@ -22,6 +22,8 @@ from .result import Periodogram
 
 #: Per-peak extras of a BLS row (io.py:66-70).
 PEAK_EXTRA_COLUMNS = ("depth", "depth_snr", "duration", "t0", "sde")
+#: Per-peak extras of each method's rows, in column order (batch/io.py:66-70).
+METHOD_PEAK_EXTRAS = {"BLS": PEAK_EXTRA_COLUMNS, "TLS": ("sr", "depth", "duration", "t0")}
 
 
 def periodogram_to_row(key: str, pg: Periodogram, *, n_best: int = 10,
@@ -169,7 +171,7 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
     ``sink``: optional ``.parquet`` or ``.csv`` path for the rows (``write_rows``).
     """
     m = get_method(method)
-    s = _settings(settings)
+    s = _settings(settings, m.settings_cls)
     eng = engine or _lib.default_engine()
     summary = BatchSummary()
     groups: dict[str, tuple[GridSpec, list[tuple[str, Any]]]] = {}
@@ -180,6 +182,8 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
             data = _load(data, columns, domain, band_column)
             lc = to_input(data, columns=columns, domain=domain)
             if isinstance(lc, MultiBandLightCurve):
+                if not m.supports_multiband:
+                    raise ValueError(f"{m.name} does not support multi-band input")
                 # one star's bands: one launch of its own, peaks ranked on the host
                 from .multiband import multiband_default_grid
                 pg = m.multiband_power(grid or multiband_default_grid(m, lc, s), lc, s,
@@ -204,17 +208,27 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
             for key, lc in chunk:
                 finite = lc.finite()
                 if finite.n < s.min_detections or finite.baseline <= 0.0:
-                    summary.errors[key] = (f"InsufficientDataError: BLS: {finite.n} finite "
-                                           f"points < min_detections {s.min_detections}"
+                    summary.errors[key] = (f"InsufficientDataError: {m.name}: {finite.n} "
+                                           f"finite points < min_detections {s.min_detections}"
                                            if finite.n < s.min_detections
-                                           else "InsufficientDataError: BLS: no usable time baseline")
+                                           else f"InsufficientDataError: {m.name}: no usable "
+                                                "time baseline")
                     continue
                 ok.append((key, lc))
             if not ok:
                 continue
-            # peaks ranked on the device: only the rows leave the GPU
-            summary.rows.extend(m.rows_many(g, ok, s, n_best=n_best,
-                                            extra_keys=PEAK_EXTRA_COLUMNS, engine=eng))
+            extras = METHOD_PEAK_EXTRAS.get(m.name, ())
+            if hasattr(m, "rows_many"):
+                # peaks ranked on the device: only the rows leave the GPU
+                summary.rows.extend(m.rows_many(g, ok, s, n_best=n_best, extra_keys=extras,
+                                                engine=eng))
+            else:
+                # one launch for the chunk, peaks ranked on the host
+                pgs = m.power_many(g, [lc for _, lc in ok], s, engine=eng)
+                summary.rows.extend(
+                    periodogram_to_row(key, pg.with_peak_defaults(s), n_best=n_best,
+                                       extra_keys=extras, alias_diverse=True)
+                    for (key, _), pg in zip(ok, pgs))
             summary.launches += 1
     if sink is not None and summary.rows:
         from .sinks import write_rows
@@ -222,5 +236,6 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
     return summary
 
 
-__all__ = ["BatchSummary", "PEAK_EXTRA_COLUMNS", "batch_periodograms", "periodogram_to_row",
+__all__ = ["BatchSummary", "METHOD_PEAK_EXTRAS", "PEAK_EXTRA_COLUMNS", "batch_periodograms",
+           "periodogram_to_row",
            "resolve_inputs"]

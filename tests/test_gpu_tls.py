@@ -121,3 +121,25 @@ def test_tls_long_curve_bins_stay_exact():
     np.testing.assert_array_equal(got["duration"], ref["duration"])
     np.testing.assert_array_equal(got["t0"], ref["t0"])
     np.testing.assert_allclose(got["sr"], ref["sr"], rtol=1e-9)
+
+
+def test_tls_batch_rows():
+    # batch_periodograms with method="TLS": one launch per chunk of curves that
+    # share a grid, rows with the reference's TLS peak columns; a short curve is
+    # recorded as an error, as the reference's runner records it
+    from cuperiod_b200.batch import batch_periodograms
+    from cuperiod_b200.grid import GridSpec
+    from cuperiod_b200.settings import TLSSettings
+    curves = [_curve(30 + i, 1500) for i in range(3)]
+    grid = GridSpec(kind="period", values=np.geomspace(0.7, 9.0, 600))
+    t0, y0, _ = curves[0]
+    inputs = [(f"c{i}", c) for i, c in enumerate(curves)] + [("short", (t0[:5], y0[:5]))]
+    out = batch_periodograms(inputs, "TLS", grid=grid, settings=TLSSettings(), domain="flux",
+                             n_best=3)
+    assert [r["key"] for r in out.rows] == ["c0", "c1", "c2"] and "short" in out.errors
+    row = out.rows[0]
+    assert row["method"] == "TLS" and {"sr_1", "depth_1", "duration_1", "t0_1"} <= set(row)
+    from cuperiod_b200.lightcurve import Domain, LightCurve
+    from cuperiod_b200.tls import TLSMethod
+    pg = TLSMethod().power(grid, LightCurve(*curves[0], Domain.FLUX), TLSSettings())
+    assert row["best_period"] == pg.best_period()
