@@ -100,7 +100,7 @@ __device__ __forceinline__ long long plane_value(const unsigned* lo, const unsig
     return (long long)(((unsigned long long)hi[b] << 32) | lo[b]);
 }
 
-__global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
+__global__ void __launch_bounds__(kTThreads, 3) tls_kernel(TlsArgs a) {
     extern __shared__ __align__(16) unsigned char tls_dyn[];
     __shared__ TlsShared s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -139,18 +139,15 @@ __global__ void __launch_bounds__(kTThreads, 2) tls_kernel(TlsArgs a) {
             for (int p = 0; p < np; ++p) {
                 const double P = a.period[p0 + p], f = a.freq[p0 + p];
                 unsigned* h = words + (size_t)p * 4 * nb;
-                int bins[kTPts];
-#pragma unroll
-                for (int r = 0; r < kTPts; ++r) {
-                    int b = a.fast_fold ? tls_bin_fast(x[r], f, nb, a.margin_u, a.margin_phi)
-                                        : -1;
-                    bins[r] = b >= 0 ? b : tls_bin(x[r], P, nb);
-                }
-                int prev = bins[0];
+                const bool fast = a.fast_fold != 0;
+                const uint32_t mu = a.margin_u, mphi = a.margin_phi;
+                int prev = fast ? tls_bin_fast(x[0], f, nb, mu, mphi) : -1;
+                if (prev < 0) prev = tls_bin(x[0], P, nb);
                 long long ay = yq[0], aw = wq[0];
 #pragma unroll
                 for (int r = 1; r < kTPts; ++r) {
-                    const int b = bins[r];
+                    int b = fast ? tls_bin_fast(x[r], f, nb, mu, mphi) : -1;
+                    if (b < 0) b = tls_bin(x[r], P, nb);
                     if (b != prev) {
                         flush_run(h, nb, prev, ay, aw);
                         prev = b;
