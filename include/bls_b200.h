@@ -1,5 +1,6 @@
 /*
- * C ABI of the B200 box-least-squares (BLS) engine: libbls_b200.so.
+ * C ABI of the B200 box-least-squares (BLS) engine: libbls_b200.so (the BLS
+ * search, the multi-band joint search and the transit least squares filter).
  *
  * Plain pointers and sizes only.  Host arrays in, host (or device) arrays out;
  * the engine owns its device buffers, pinned staging, CUDA stream and graphs.
@@ -29,6 +30,16 @@
  *       -- the phase-bin lines of the fold (_bls_core.py:369-376 / 536-538) and
  *          the padded cumulative sums (377-388), exported so tests can compare
  *          the device's intermediate results with the reference's;
+ *   bls_download_rows
+ *       -- the batch runner's per-curve rows with alias-diverse peaks
+ *          (src/cuperiod/batch/io.py:507-571, core/peaks.py:128-231);
+ *   bls_search_joint, bls_joint_prepare / _launch / _download
+ *       -- joint_search with the cupy backend and its _finish, the shared-box
+ *          multi-band statistic (src/cuperiod/multiband/_bls_joint.py:151-204,
+ *          359-404, 703-796);
+ *   bls_tls_search, bls_tls_prepare / _launch / _download
+ *       -- _tls_cuda / _tls_numba, the transit least squares matched filter
+ *          (src/cuperiod/methods/tls.py:428-621);
  *   bls_last_error
  *       -- the exceptions the reference raises before a launch (ValueError,
  *          BackendUnavailableError from core/backend.py:340-384).
