@@ -159,7 +159,8 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                        columns: Any = None, domain: Domain | str | None = None,
                        band_column: str | None = None, n_best: int = 10,
                        chunk_size: int = 4096, sink: str | os.PathLike | None = None,
-                       engine: _lib.Engine | None = None) -> BatchSummary:
+                       engine: _lib.Engine | None = None,
+                       workers: int | None = None) -> BatchSummary:
     """Search many light curves; one engine launch per chunk of curves that share
     a trial grid (the explicit ``grid``, or curves whose default grids coincide).
 
@@ -169,6 +170,11 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
     that cannot be searched (too few points, no baseline, unreadable) is recorded
     in ``errors`` like the reference's per-curve failures (runner.py:248-249).
     ``sink``: optional ``.parquet`` or ``.csv`` path for the rows (``write_rows``).
+    ``workers``: host threads that run the launches (default 4; each thread its
+    own engine and CUDA stream, so the small launches of curves with distinct
+    default grids overlap each other and the host work); with an explicit
+    ``engine`` every launch runs on that engine in this thread.  Rows keep the
+    order of a single-threaded run.
     """
     m = get_method(method)
     s = _settings(settings, m.settings_cls)
@@ -201,6 +207,7 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
             continue
         gk = fixed_key if fixed_key is not None else _grid_key(g)
         groups.setdefault(gk, (g, []))[1].append((str(key), lc))
+    jobs: list[tuple[GridSpec, list[tuple[str, Any]]]] = []
     for g, members in groups.values():
         for start in range(0, len(members), chunk_size):
             chunk = members[start:start + chunk_size]
@@ -215,21 +222,32 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                                                 "time baseline")
                     continue
                 ok.append((key, lc))
-            if not ok:
-                continue
-            extras = METHOD_PEAK_EXTRAS.get(m.name, ())
-            if hasattr(m, "rows_many"):
-                # peaks ranked on the device: only the rows leave the GPU
-                summary.rows.extend(m.rows_many(g, ok, s, n_best=n_best, extra_keys=extras,
-                                                engine=eng))
-            else:
-                # one launch for the chunk, peaks ranked on the host
-                pgs = m.power_many(g, [lc for _, lc in ok], s, engine=eng)
-                summary.rows.extend(
-                    periodogram_to_row(key, pg.with_peak_defaults(s), n_best=n_best,
-                                       extra_keys=extras, alias_diverse=True)
-                    for (key, _), pg in zip(ok, pgs))
-            summary.launches += 1
+            if ok:
+                jobs.append((g, ok))
+    extras = METHOD_PEAK_EXTRAS.get(m.name, ())
+
+    def run(job, job_engine):
+        g, ok = job
+        if hasattr(m, "rows_many"):
+            # peaks ranked on the device: only the rows leave the GPU
+            return m.rows_many(g, ok, s, n_best=n_best, extra_keys=extras, engine=job_engine)
+        # one launch for the chunk, peaks ranked on the host
+        pgs = m.power_many(g, [lc for _, lc in ok], s, engine=job_engine)
+        return [periodogram_to_row(key, pg.with_peak_defaults(s), n_best=n_best,
+                                   extra_keys=extras, alias_diverse=True)
+                for (key, _), pg in zip(ok, pgs)]
+
+    n_workers = 1 if engine is not None else max(1, int(workers if workers is not None else 4))
+    if n_workers == 1 or len(jobs) <= 1:
+        results = [run(job, eng) for job in jobs]
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=min(n_workers, len(jobs))) as pool:
+            # each worker thread searches with its own engine (default_engine)
+            results = list(pool.map(lambda job: run(job, _lib.default_engine()), jobs))
+    for rows in results:
+        summary.rows.extend(rows)
+    summary.launches += len(jobs)
     if sink is not None and summary.rows:
         from .sinks import write_rows
         write_rows(summary.rows, sink)

@@ -113,3 +113,23 @@ def test_device_rows_on_tiny_grids(engine, n_periods):
     dev, host = _rows_of_same_launch(engine, grid, _keyed()[:3], s, 3)
     for d, h in zip(dev, host):
         _same_row(d, h)
+
+
+def test_threaded_batch_rows_equal_single_threaded():
+    # curves with distinct baselines get distinct default grids (one launch
+    # each); worker threads with their own engines run those launches
+    # concurrently and must give the rows of a single-threaded run, in order
+    import numpy as np
+
+    from cuperiod_b200.batch import batch_periodograms
+    from cuperiod_b200.synthetic import batched_curves
+    rng = np.random.default_rng(8)
+    inputs = []
+    for i, c in enumerate(batched_curves(24, seed=9, n_range=(500, 3000))):
+        keep = c.t < c.t.min() + rng.uniform(15.0, 27.0)
+        inputs.append((f"c{i}", (c.t[keep], c.y[keep])))
+    one = batch_periodograms(inputs, "BLS", domain="flux", workers=1, n_best=3)
+    many = batch_periodograms(inputs, "BLS", domain="flux", workers=4, n_best=3)
+    assert one.launches == many.launches > 1
+    assert [r["key"] for r in many.rows] == [f"c{i}" for i in range(24)]
+    assert many.rows == one.rows
