@@ -172,15 +172,16 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
     ``sink``: optional ``.parquet`` or ``.csv`` path for the rows (``write_rows``).
     ``workers``: host threads that run the launches (default 4; each thread its
     own engine and CUDA stream, so the small launches of curves with distinct
-    default grids overlap each other and the host work); with an explicit
+    default grids, and of multi-band stars, overlap each other and the host
+    work); with an explicit
     ``engine`` every launch runs on that engine in this thread.  Rows keep the
     order of a single-threaded run.
     """
     m = get_method(method)
     s = _settings(settings, m.settings_cls)
-    eng = engine or _lib.default_engine()
     summary = BatchSummary()
     groups: dict[str, tuple[GridSpec, list[tuple[str, Any]]]] = {}
+    star_jobs: list[tuple[str, Any, GridSpec]] = []
     fixed_key = _grid_key(grid) if grid is not None else None     # one grid: hash it once
     for key, data in resolve_inputs(inputs, columns=columns, domain=domain,
                                     band_column=band_column):
@@ -190,15 +191,9 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
             if isinstance(lc, MultiBandLightCurve):
                 if not m.supports_multiband:
                     raise ValueError(f"{m.name} does not support multi-band input")
-                # one star's bands: one launch of its own, peaks ranked on the host
+                # one star's bands: a launch of its own, peaks ranked on the host
                 from .multiband import multiband_default_grid
-                pg = m.multiband_power(grid or multiband_default_grid(m, lc, s), lc, s,
-                                       engine=eng)
-                summary.rows.append(periodogram_to_row(str(key), pg.with_peak_defaults(s),
-                                                       n_best=n_best,
-                                                       extra_keys=PEAK_EXTRA_COLUMNS,
-                                                       alias_diverse=True))
-                summary.launches += 1
+                star_jobs.append((str(key), lc, grid or multiband_default_grid(m, lc, s)))
                 continue
             lc = lc.in_domain(m.natural_domain)
             g = grid or m.default_grid(lc, s)
@@ -207,7 +202,7 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
             continue
         gk = fixed_key if fixed_key is not None else _grid_key(g)
         groups.setdefault(gk, (g, []))[1].append((str(key), lc))
-    jobs: list[tuple[GridSpec, list[tuple[str, Any]]]] = []
+    jobs: list[Any] = [("star", job) for job in star_jobs]
     for g, members in groups.values():
         for start in range(0, len(members), chunk_size):
             chunk = members[start:start + chunk_size]
@@ -223,11 +218,24 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                     continue
                 ok.append((key, lc))
             if ok:
-                jobs.append((g, ok))
+                jobs.append(("curves", (g, ok)))
     extras = METHOD_PEAK_EXTRAS.get(m.name, ())
 
     def run(job, job_engine):
-        g, ok = job
+        """``(rows, {key: error})`` of one job."""
+        kind, body = job
+        if kind == "star":
+            key, star, g = body
+            try:
+                pg = m.multiband_power(g, star, s, engine=job_engine)
+            except (CuPeriodError, ValueError) as exc:
+                return [], {key: f"{type(exc).__name__}: {exc}"}
+            return [periodogram_to_row(key, pg.with_peak_defaults(s), n_best=n_best,
+                                       extra_keys=PEAK_EXTRA_COLUMNS, alias_diverse=True)], {}
+        return run_curves(body, job_engine), {}
+
+    def run_curves(body, job_engine):
+        g, ok = body
         if hasattr(m, "rows_many"):
             # peaks ranked on the device: only the rows leave the GPU
             return m.rows_many(g, ok, s, n_best=n_best, extra_keys=extras, engine=job_engine)
@@ -238,16 +246,18 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                 for (key, _), pg in zip(ok, pgs)]
 
     n_workers = 1 if engine is not None else max(1, int(workers if workers is not None else 4))
+    # engine None: each launch runs on its thread's own engine (default_engine),
+    # created at the first launch
     if n_workers == 1 or len(jobs) <= 1:
-        results = [run(job, eng) for job in jobs]
+        results = [run(job, engine) for job in jobs]
     else:
         from concurrent.futures import ThreadPoolExecutor
         with ThreadPoolExecutor(max_workers=min(n_workers, len(jobs))) as pool:
-            # each worker thread searches with its own engine (default_engine)
-            results = list(pool.map(lambda job: run(job, _lib.default_engine()), jobs))
-    for rows in results:
+            results = list(pool.map(lambda job: run(job, None), jobs))
+    for rows, errors in results:
         summary.rows.extend(rows)
-    summary.launches += len(jobs)
+        summary.errors.update(errors)
+        summary.launches += bool(rows)
     if sink is not None and summary.rows:
         from .sinks import write_rows
         write_rows(summary.rows, sink)

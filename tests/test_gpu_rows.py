@@ -133,3 +133,28 @@ def test_threaded_batch_rows_equal_single_threaded():
     assert one.launches == many.launches > 1
     assert [r["key"] for r in many.rows] == [f"c{i}" for i in range(24)]
     assert many.rows == one.rows
+
+
+def test_threaded_batch_of_stars_and_curves_equals_single_threaded():
+    # multi-band stars are launches of their own beside the single-band chunks;
+    # threaded and single-threaded runs give the same rows in the same order
+    # and record the same failures
+    from cuperiod_b200.batch import batch_periodograms
+    from cuperiod_b200.lightcurve import Domain, LightCurve, MultiBandLightCurve
+    from cuperiod_b200.settings import BLSSettings
+    from cuperiod_b200.synthetic import batched_curves, multiband_stars
+    inputs = []
+    for i, star in enumerate(multiband_stars(3, seed=21, n_range=(600, 1200))):
+        inputs.append((f"s{i}", MultiBandLightCurve.from_light_curves(
+            {b: LightCurve(c.t, c.y, c.dy, Domain.FLUX) for b, c in star.items()})))
+    for i, c in enumerate(batched_curves(4, seed=22, n_range=(500, 1500))):
+        inputs.append((f"c{i}", (c.t, c.y)))
+    inputs.append(("short", MultiBandLightCurve.from_light_curves({
+        "g": LightCurve(np.arange(2.0), np.ones(2), None, Domain.FLUX)})))
+    s = BLSSettings(mb_ephemeris="shared")
+    one = batch_periodograms(inputs, "BLS", domain="flux", settings=s, workers=1, n_best=3)
+    many = batch_periodograms(inputs, "BLS", domain="flux", settings=s, workers=4, n_best=3)
+    assert [r["key"] for r in many.rows][:3] == ["s0", "s1", "s2"]
+    assert len(many.rows) == 7 and many.launches == one.launches
+    assert many.errors == one.errors and list(many.errors) == ["short"]
+    assert many.rows == one.rows

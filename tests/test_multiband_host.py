@@ -71,3 +71,22 @@ def test_band_selection_fails_before_the_device(ephemeris):
     with pytest.raises(InsufficientDataError, match="no band has enough"):
         bls_multiband_power(GridSpec(kind="period", values=np.array([1.0, 2.0])), short,
                             BLSSettings(), ephemeris=ephemeris)
+
+
+def test_batch_records_short_stars_and_curves_without_a_launch():
+    # a star whose bands are all too short fails when its launch would start,
+    # in a worker; like a short single-band curve it lands in ``errors`` and no
+    # engine is created (there is nothing to launch)
+    from cuperiod_b200.batch import batch_periodograms
+    from cuperiod_b200.grid import GridSpec
+    from cuperiod_b200.lightcurve import Domain, LightCurve, MultiBandLightCurve
+    short = MultiBandLightCurve.from_light_curves({
+        "g": LightCurve(np.arange(2.0), np.ones(2), None, Domain.FLUX),
+        "r": LightCurve(np.arange(2.0) + 0.5, np.ones(2), None, Domain.FLUX)})
+    grid = GridSpec(kind="period", values=np.array([1.0, 2.0]))
+    res = batch_periodograms([("star", short), ("curve", (np.arange(3.0), np.ones(3)))],
+                             "BLS", grid=grid, domain="flux", workers=4)
+    assert res.rows == [] and res.launches == 0
+    assert set(res.errors) == {"star", "curve"}
+    assert "no band has enough" in res.errors["star"]
+    assert res.errors["curve"].startswith("InsufficientDataError")
