@@ -68,6 +68,9 @@ def parse_args():
                         "joint-ephemeris multi-band search of --stars six-band stars; tls: "
                         "the transit least squares search of --tls-curves curves")
     p.add_argument("--tls-curves", type=int, default=32, help="tls: light curves per rank")
+    p.add_argument("--tile", choices=("auto", "default"), default="auto",
+                   help="batch: tile shape from the autotuner (timed on a 128-curve sample "
+                        "before the warm-up) or the engine's default")
     p.add_argument("--stars", type=int, default=64, help="multiband-shared: stars per rank")
     return p.parse_args()
 
@@ -145,8 +148,16 @@ def cpu_baseline_sample(curves, segments, seconds: float) -> dict:
     from oracle import oracle
 
     order = np.argsort([c.t.size for c in curves])
-    picks = [order[int((k + 0.5) / 8 * len(order))] for k in range(8)]
-    picks = [picks[i] for i in (3, 4, 2, 5, 1, 6, 0, 7)]      # near the mean N first
+    # octiles of N, near the mean first, then the midpoints between them, ... until
+    # the time is up (the sample keeps the workload's length mix at any size)
+    picks, seen = [], set()
+    for level in (8, 16, 32, 64):
+        ks = sorted(range(level), key=lambda k: abs((k + 0.5) / level - 0.5))
+        for k in ks:
+            i = int(order[int((k + 0.5) / level * len(order))])
+            if i not in seen:
+                seen.add(i)
+                picks.append(i)
     cores = os.cpu_count() or 1
     done, t0, npts = 0, time.perf_counter(), 0
     for i in picks:
@@ -208,7 +219,12 @@ def run_ours(args) -> None:
 
 
     curves, segments, grid, packed = workload(args.curves, args.seed + rank)
-    engine = _lib.Engine(device=local)
+    tune = None
+    if args.tile == "auto":
+        from cuperiod_b200.autotune import tuned_engine
+        engine, tune = tuned_engine(grid, packed, device=local)
+    else:
+        engine = _lib.Engine(device=local)
     # a stream of our own: the C ABI reads a NULL stream as "the engine's stream",
     # so torch's legacy default stream (handle 0) would leave the events unordered
     # with the launches
@@ -289,6 +305,12 @@ def run_ours(args) -> None:
             "config": {"workload": WORKLOAD, "curves_per_rank": args.curves,
                        "variant": "plain full grid", "parallelism": f"replicas x{world}",
                        "l2": "inputs (~%d MB/rank) exceed L2; no flush" % (n_pts * 12 // 2**20),
+                       "tile": (tune.shape.label() if tune else "default")
+                               + ", %d CTAs x %d B smem" % (info["ctas"], info["smem_per_cta"]),
+                       "autotune": ({"sample_curves": tune.sample_curves,
+                                     "ms_per_sample_launch": {k: round(v, 2)
+                                                              for k, v in tune.ms.items()}}
+                                    if tune else None),
                        "folds_per_step": info["folds"] * world,
                        "boxes_per_step": info["boxes"] * world,
                        "trials_per_s": info["trials"] * world / (ms_per_step / 1000.0)},

@@ -93,6 +93,7 @@ def load() -> ctypes.CDLL:
         lib.bls_download_rows.argtypes = [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp]
         lib.bls_search.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_batch_info.argtypes = [_vp, P(BlsBatchInfo)]
+        lib.bls_time_launches.argtypes = [_vp, _i32, P(_dbl), _vp]
         lib.bls_search_joint.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_tls_search.argtypes = [_vp, P(BlsTlsInputs), _vp, _i64, _vp, _vp]
         lib.bls_tls_prepare.argtypes = [_vp, P(BlsTlsInputs), _vp, _i64, _vp]
@@ -110,7 +111,7 @@ def load() -> ctypes.CDLL:
                      "bls_launch_best_noalloc", "bls_download_rows", "bls_search_joint",
                      "bls_joint_prepare", "bls_joint_launch", "bls_joint_download",
                      "bls_tls_search", "bls_tls_prepare", "bls_tls_launch",
-                     "bls_tls_download"):
+                     "bls_tls_download", "bls_time_launches"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib
@@ -239,6 +240,13 @@ class Engine:
 
     def launch(self, stream: int | None = None) -> None:
         _check(self._lib.bls_launch(self._h, stream))
+
+    def time_launches(self, reps: int = 1, stream: int | None = None) -> float:
+        """Mean device milliseconds of one launch of the prepared batch over
+        ``reps`` launches (CUDA events on the launching stream)."""
+        ms = _dbl(0.0)
+        _check(self._lib.bls_time_launches(self._h, int(reps), ctypes.byref(ms), stream))
+        return float(ms.value)
 
     def download(self, stream: int | None = None) -> np.ndarray:
         """All fields: array of shape (7, n_curves, n_periods)."""

@@ -600,11 +600,14 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
             if (need > sm) sm = need;
         }
         sm = (sm + 15) & ~size_t(15);
-        if (modes[m] && sm > e->smem_optin)
+        // the opt-in limit covers the kernel's static shared state too
+        const size_t limit = modes[m] ? e->smem_optin + 1024 - search_static_smem(m) : 0;
+        if (modes[m] && sm > limit)
             return fail(BLS_E_RESOURCE,
-                        "BLS: %zu bytes of shared memory per period exceed the device's %zu; "
-                        "narrow the period range (max_period_days)",
-                        sm, e->smem_optin);
+                        "BLS: %zu bytes of shared memory per CTA exceed the device's %zu "
+                        "(a period of the widest segment, or BlsTune.smem_per_cta); narrow "
+                        "the period range (max_period_days)",
+                        sm, limit);
         smem_mode[m] = sm;
     }
     // per segment: boxes of one curve (the same for every curve)
@@ -1445,6 +1448,34 @@ int bls_launch(BlsEngine* e, void* stream) {
     }
     CUDA_TRY(cudaGraphLaunch(e->graph, st), "graph launch");
     return BLS_OK;
+}
+
+int bls_time_launches(BlsEngine* e, int32_t reps, double* ms_per_launch, void* stream) {
+    if (!e || !ms_per_launch) return fail(BLS_E_INVALID, "engine and output are required");
+    if (reps < 1) return fail(BLS_E_INVALID, "reps must be >= 1");
+    if (!e->prepared) return fail(BLS_E_STATE, "bls_time_launches before bls_prepare");
+    cudaSetDevice(e->device);
+    cudaStream_t st = pick(e, stream);
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    for (auto& x : ev)
+        if (cudaEventCreate(&x) != cudaSuccess) {
+            for (auto& y : ev)
+                if (y) cudaEventDestroy(y);
+            return cuda_fail(cudaGetLastError(), "event create");
+        }
+    int rc = BLS_OK;
+    cudaError_t ce = cudaEventRecord(ev[0], st);
+    for (int i = 0; i < reps && rc == BLS_OK && ce == cudaSuccess; ++i) rc = bls_launch(e, st);
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev[1], st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[1]);
+    float ms = 0.0f;
+    if (rc == BLS_OK && ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (rc != BLS_OK) return rc;
+    if (ce != cudaSuccess) return cuda_fail(ce, "timed launches");
+    *ms_per_launch = (double)ms / reps;
+    return check_device_flag(e, st);
 }
 
 int bls_download(BlsEngine* e, double* out, void* stream) {

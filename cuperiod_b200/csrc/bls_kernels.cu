@@ -31,6 +31,7 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <mutex>
 
@@ -1390,6 +1391,15 @@ size_t period_hist_bytes(int mode, int hl) {
     return mode == MODE_UNIFORM ? hist_period_bytes<MODE_UNIFORM>(hl)
            : mode == MODE_WIDE  ? hist_period_bytes<MODE_WIDE>(hl)
                                 : hist_period_bytes<MODE_GENERAL>(hl);
+}
+
+size_t search_static_smem(int mode) {
+    size_t most = 0;
+    for (const void* f : {search_fn<0>(mode), search_fn<1>(mode)}) {
+        cudaFuncAttributes at{};
+        if (cudaFuncGetAttributes(&at, f) == cudaSuccess) most = std::max(most, at.sharedSizeBytes);
+    }
+    return most;
 }
 
 int max_resident_ctas(int mode, size_t smem) {

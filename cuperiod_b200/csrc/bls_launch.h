@@ -68,5 +68,7 @@ cudaError_t launch_tls(const TlsArgs& args, int n_ctas, size_t smem, cudaStream_
 
 int search_threads();
 int max_resident_ctas(int mode, size_t smem);
+// Static shared memory of the search kernel of one accumulation mode (bytes).
+size_t search_static_smem(int mode);
 
 }  // namespace blsb200

@@ -130,6 +130,13 @@ int bls_prepare(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* curves,
 /* Run the search of the prepared batch on the device (no host transfers). */
 int bls_launch(BlsEngine* engine, void* stream);
 
+/* No counterpart in the reference (its tile shape is fixed at 128 threads per
+ * period).  Runs bls_launch `reps` times on `stream` between two CUDA events and
+ * returns the mean device time of one launch in milliseconds; the autotuner's
+ * clock for comparing tile shapes (BlsTune smem_per_cta / max_tile).  Waits
+ * for the stream. */
+int bls_time_launches(BlsEngine* engine, int32_t reps, double* ms_per_launch, void* stream);
+
 /* Copy every field of every curve, field-major: out[f][c][p] with
  * f < BLS_N_FIELDS, c < n_curves, p < n_periods (grid order).  Waits for the
  * stream. */
