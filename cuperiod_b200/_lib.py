@@ -11,6 +11,7 @@ import ctypes
 import os
 import threading
 from dataclasses import dataclass
+from typing import Sequence
 
 import numpy as np
 
@@ -58,7 +59,8 @@ class BlsBatchInfo(ctypes.Structure):
     _fields_ = [("n_curves", _i32), ("n_segments", _i32), ("n_periods", _i64),
                 ("n_items", _i64), ("n_points", _i64), ("folds", _dbl), ("boxes", _dbl),
                 ("trials", _dbl), ("h2d_bytes", _i64), ("ctas", _i32), ("smem_per_cta", _i32),
-                ("uniform_curves", _i32), ("fast_fold_segments", _i32)]
+                ("uniform_curves", _i32), ("fast_fold_segments", _i32), ("spectrum", _i64),
+                ("n_grids", _i32), ("reserved", _i32)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -94,6 +96,7 @@ def load() -> ctypes.CDLL:
         lib.bls_search.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_batch_info.argtypes = [_vp, P(BlsBatchInfo)]
         lib.bls_time_launches.argtypes = [_vp, _i32, P(_dbl), _vp]
+        lib.bls_prepare_grids.argtypes = [_vp, _i32, P(BlsGrid), _vp, P(BlsCurves), _vp]
         lib.bls_search_joint.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_tls_search.argtypes = [_vp, P(BlsTlsInputs), _vp, _i64, _vp, _vp]
         lib.bls_tls_prepare.argtypes = [_vp, P(BlsTlsInputs), _vp, _i64, _vp]
@@ -111,7 +114,7 @@ def load() -> ctypes.CDLL:
                      "bls_launch_best_noalloc", "bls_download_rows", "bls_search_joint",
                      "bls_joint_prepare", "bls_joint_launch", "bls_joint_download",
                      "bls_tls_search", "bls_tls_prepare", "bls_tls_launch",
-                     "bls_tls_download", "bls_time_launches"):
+                     "bls_tls_download", "bls_time_launches", "bls_prepare_grids"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib
@@ -219,6 +222,7 @@ class Engine:
         self._h = handle
         self._grid: PackedGrid | None = None
         self._curves: PackedCurves | None = None
+        self._spec_off = np.zeros(1, dtype=np.int64)
         self._joint_periods = 0
         self._tls_shape = (0, 0)
 
@@ -235,8 +239,43 @@ class Engine:
 
     def prepare(self, grid: PackedGrid, curves: PackedCurves, stream: int | None = None) -> None:
         self._grid, self._curves = grid, curves
+        self._spec_off = np.arange(curves.n_curves + 1, dtype=np.int64) * grid.n_periods
         g, c = grid.struct(), curves.struct()
         _check(self._lib.bls_prepare(self._h, ctypes.byref(g), ctypes.byref(c), stream))
+
+    def prepare_grids(self, grids: Sequence[PackedGrid], grid_of_curve, curves: PackedCurves,
+                      stream: int | None = None) -> None:
+        """A batch whose curves have their own grids, searched in one launch:
+        curve ``c`` over ``grids[grid_of_curve[c]]`` (``bls_prepare_grids``)."""
+        gids = np.ascontiguousarray(grid_of_curve, dtype=np.int32).reshape(-1)
+        if gids.size != curves.n_curves:
+            raise ValueError("grid_of_curve needs one grid index per curve")
+        if not grids:
+            raise ValueError("at least one grid is required")
+        structs = (BlsGrid * len(grids))(*[g.struct() for g in grids])
+        c = curves.struct()
+        # one grid: the layout of ``prepare``, so ``download`` keeps its shape
+        self._grid, self._curves = (grids[0] if len(grids) == 1 else None), curves
+        counts = np.array([g.n_periods for g in grids], dtype=np.int64)
+        if gids.size and (gids.min() < 0 or gids.max() >= len(grids)):
+            raise ValueError("grid_of_curve holds an index outside the grids")
+        self._spec_off = np.concatenate([[0], np.cumsum(counts[gids])]).astype(np.int64)
+        _check(self._lib.bls_prepare_grids(self._h, len(grids), structs, gids.ctypes.data,
+                                           ctypes.byref(c), stream))
+
+    @property
+    def spectrum_offsets(self) -> np.ndarray:
+        """Curve ``c``'s periods in the prepared batch's flat spectra:
+        ``[offsets[c], offsets[c + 1])``."""
+        return self._spec_off
+
+    def download_flat(self, stream: int | None = None) -> np.ndarray:
+        """All fields of every curve, ``(7, spectrum)``: curve ``c`` at
+        ``[:, spectrum_offsets[c]:spectrum_offsets[c + 1]]`` (its grid's order)."""
+        assert self._curves is not None
+        out = np.empty((N_FIELDS, int(self._spec_off[-1])), dtype=np.float64)
+        _check(self._lib.bls_download(self._h, out.ctypes.data, stream))
+        return out
 
     def launch(self, stream: int | None = None) -> None:
         _check(self._lib.bls_launch(self._h, stream))
@@ -249,8 +288,11 @@ class Engine:
         return float(ms.value)
 
     def download(self, stream: int | None = None) -> np.ndarray:
-        """All fields: array of shape (7, n_curves, n_periods)."""
-        assert self._grid is not None and self._curves is not None
+        """All fields: array of shape (7, n_curves, n_periods) (one grid; after
+        ``prepare_grids`` use ``download_flat``)."""
+        if self._grid is None:
+            raise ValueError("the prepared batch has one grid per curve: use download_flat")
+        assert self._curves is not None
         out = np.empty((N_FIELDS, self._curves.n_curves, self._grid.n_periods), dtype=np.float64)
         _check(self._lib.bls_download(self._h, out.ctypes.data, stream))
         return out

@@ -161,8 +161,11 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                        chunk_size: int = 4096, sink: str | os.PathLike | None = None,
                        engine: _lib.Engine | None = None,
                        workers: int | None = None) -> BatchSummary:
-    """Search many light curves; one engine launch per chunk of curves that share
-    a trial grid (the explicit ``grid``, or curves whose default grids coincide).
+    """Search many light curves: BLS searches each chunk of ``chunk_size`` curves
+    in one engine launch, every curve over its own grid (the explicit ``grid``,
+    else its default grid; equal grids are shared); other methods launch once per
+    chunk of curves that share a grid.  Multi-band stars are launches of their
+    own; their rows come first, then the curves' rows in input order.
 
     ``inputs``: ``(key, data)`` pairs (``data`` a LightCurve, MultiBandLightCurve,
     ``(t, y[, dy])`` tuple or table), light curves, files (a path, a directory, a
@@ -181,6 +184,7 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
     s = _settings(settings, m.settings_cls)
     summary = BatchSummary()
     groups: dict[str, tuple[GridSpec, list[tuple[str, Any]]]] = {}
+    entries: list[tuple[str, Any, str]] = []        # (key, curve, grid key) in input order
     star_jobs: list[tuple[str, Any, GridSpec]] = []
     fixed_key = _grid_key(grid) if grid is not None else None     # one grid: hash it once
     for key, data in resolve_inputs(inputs, columns=columns, domain=domain,
@@ -202,23 +206,33 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
             continue
         gk = fixed_key if fixed_key is not None else _grid_key(g)
         groups.setdefault(gk, (g, []))[1].append((str(key), lc))
+        entries.append((str(key), lc, gk))
+
+    def searchable(key: str, lc: Any) -> bool:
+        finite = lc.finite()
+        if finite.n < s.min_detections or finite.baseline <= 0.0:
+            summary.errors[key] = (f"InsufficientDataError: {m.name}: {finite.n} "
+                                   f"finite points < min_detections {s.min_detections}"
+                                   if finite.n < s.min_detections
+                                   else f"InsufficientDataError: {m.name}: no usable "
+                                        "time baseline")
+            return False
+        return True
+
     jobs: list[Any] = [("star", job) for job in star_jobs]
-    for g, members in groups.values():
-        for start in range(0, len(members), chunk_size):
-            chunk = members[start:start + chunk_size]
-            ok: list[tuple[str, Any]] = []
-            for key, lc in chunk:
-                finite = lc.finite()
-                if finite.n < s.min_detections or finite.baseline <= 0.0:
-                    summary.errors[key] = (f"InsufficientDataError: {m.name}: {finite.n} "
-                                           f"finite points < min_detections {s.min_detections}"
-                                           if finite.n < s.min_detections
-                                           else f"InsufficientDataError: {m.name}: no usable "
-                                                "time baseline")
-                    continue
-                ok.append((key, lc))
-            if ok:
-                jobs.append(("curves", (g, ok)))
+    if hasattr(m, "rows_by_grid"):
+        # one launch per chunk of curves in input order, each curve over its own
+        # grid (equal grids shared)
+        ok_all = [(key, lc, groups[gk][0]) for key, lc, gk in entries if searchable(key, lc)]
+        for start in range(0, len(ok_all), chunk_size):
+            jobs.append(("mixed", ok_all[start:start + chunk_size]))
+    else:
+        for g, members in groups.values():
+            for start in range(0, len(members), chunk_size):
+                ok = [(key, lc) for key, lc in members[start:start + chunk_size]
+                      if searchable(key, lc)]
+                if ok:
+                    jobs.append(("curves", (g, ok)))
     extras = METHOD_PEAK_EXTRAS.get(m.name, ())
 
     def run(job, job_engine):
@@ -232,6 +246,10 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                 return [], {key: f"{type(exc).__name__}: {exc}"}
             return [periodogram_to_row(key, pg.with_peak_defaults(s), n_best=n_best,
                                        extra_keys=PEAK_EXTRA_COLUMNS, alias_diverse=True)], {}
+        if kind == "mixed":
+            # peaks ranked on the device: only the rows leave the GPU
+            return m.rows_by_grid(body, s, n_best=n_best, extra_keys=extras,
+                                  engine=job_engine), {}
         return run_curves(body, job_engine), {}
 
     def run_curves(body, job_engine):

@@ -222,64 +222,106 @@ class BLSMethod:
         (batch/io.py:507-571, core/result.py:285-367), without bringing the
         spectra back.  ``extra_keys``: the per-peak extras every rank carries
         (NaN past the last peak)."""
+        return self.rows_by_grid([(key, lc, grid) for key, lc in keyed], settings,
+                                 n_best=n_best, extra_keys=extra_keys, engine=engine)
+
+    def rows_by_grid(self, items: Sequence[tuple[str, LightCurve, GridSpec]],
+                     settings: BLSSettings, *, n_best: int = 10,
+                     extra_keys: Sequence[str] = (),
+                     engine: _lib.Engine | None = None) -> list[dict]:
+        """``rows_many`` for curves that each bring their own grid (the
+        reference's batch searches every curve over its own default grid,
+        batch/runner.py:187-250): every curve of ``items`` -- ``(key, curve,
+        grid)``, equal grids passed as the same object -- in one launch, each
+        over its grid, peaks ranked on the device.  Rows in ``items`` order."""
         from .result import DEFAULT_HARMONIC_MAX, DEFAULT_SEPARATION_RAYLEIGH
         from .settings import peak_defaults
-        segments = _grid_segments(grid, settings)
-        if not segments:
-            raise InsufficientDataError("BLS: empty trial grid")
         count = max(int(n_best), 1)
-        prepared = [_prepared_curve(lc, settings) for _, lc in keyed]
+        slot: dict[int, int] = {}
+        grids: list[GridSpec] = []
+        gidx = np.empty(len(items), dtype=np.int32)
+        for i, (_, _, g) in enumerate(items):
+            k = slot.setdefault(id(g), len(grids))
+            if k == len(grids):
+                grids.append(g)
+            gidx[i] = k
+        segments = [_grid_segments(g, settings) for g in grids]
+        if any(not sg for sg in segments):
+            raise InsufficientDataError("BLS: empty trial grid")
+        prepared = [_prepared_curve(lc, settings) for _, lc, _ in items]
         eng = engine or _lib.default_engine()
-        periods = np.concatenate([np.asarray(p, dtype=np.float64) for p, _ in segments])
-        if count > 1024 or periods.size < 1 or not np.all(np.diff(periods) > 0.0):
+        periods = [np.concatenate([np.asarray(p, dtype=np.float64) for p, _ in sg])
+                   for sg in segments]
+        device_ok = [count <= 1024 and p.size >= 1 and bool(np.all(np.diff(p) > 0.0))
+                     for p in periods]
+        rows: list[dict | None] = [None] * len(items)
+        host = [i for i in range(len(items)) if not device_ok[gidx[i]]]
+        if host:
             # outside the device ranking's preconditions: rank on the host
             from .batch import periodogram_to_row
-            out = self._search(segments, [(f.time, f.value, e) for f, e in prepared], settings,
-                               eng)
-            return [periodogram_to_row(key, _assemble(_fields(out[:, i, :], segments), f.n,
-                                                      f.baseline, f.meta)
-                                       .with_peak_defaults(settings), n_best=count,
-                                       extra_keys=extra_keys, alias_diverse=True)
-                    for i, ((key, _), (f, _)) in enumerate(zip(keyed, prepared))]
-        grid_p = _lib.PackedGrid.from_segments(segments, settings.bins_per_duration,
-                                               _objective_flag(settings.objective))
-        eng.prepare(grid_p, _lib.PackedCurves.from_arrays(
-            [(f.time, f.value, e) for f, e in prepared]))
-        eng.launch()
-        d = peak_defaults(settings)
-        sep_r = float(d.get("min_separation_rayleigh", DEFAULT_SEPARATION_RAYLEIGH))
-        order = int(d.get("harmonic_max", DEFAULT_HARMONIC_MAX))
-        tol_set = d.get("alias_tolerance")
-        sep = np.empty(len(prepared))
-        tol = np.empty(len(prepared))
-        for i, (f, _) in enumerate(prepared):
-            resolved = f.baseline > 0.0
-            separation = sep_r / f.baseline if resolved else 0.0
-            t = tol_set if tol_set is not None else (
-                min(separation, 1.0 / f.baseline) if resolved else 0.0)
-            sep[i] = max(separation, 1e-12)
-            tol[i] = max(float(t), 1e-12)
-        n_peaks, _, fields = eng.rows(count, order, sep, tol)
+            for k in sorted({int(gidx[i]) for i in host}):
+                members = [i for i in host if gidx[i] == k]
+                out = self._search(segments[k], [(prepared[i][0].time, prepared[i][0].value,
+                                                  prepared[i][1]) for i in members],
+                                   settings, eng)
+                for j, i in enumerate(members):
+                    f = prepared[i][0]
+                    rows[i] = periodogram_to_row(
+                        items[i][0], _assemble(_fields(out[:, j, :], segments[k]), f.n,
+                                               f.baseline, f.meta).with_peak_defaults(settings),
+                        n_best=count, extra_keys=extra_keys, alias_diverse=True)
+        dev = [i for i in range(len(items)) if device_ok[gidx[i]]]
+        if dev:
+            used = sorted({int(gidx[i]) for i in dev})
+            local = {k: j for j, k in enumerate(used)}
+            flag = _objective_flag(settings.objective)
+            packed_grids = [_lib.PackedGrid.from_segments(segments[k], settings.bins_per_duration,
+                                                          flag) for k in used]
+            eng.prepare_grids(packed_grids, [local[int(gidx[i])] for i in dev],
+                              _lib.PackedCurves.from_arrays(
+                                  [(prepared[i][0].time, prepared[i][0].value, prepared[i][1])
+                                   for i in dev]))
+            eng.launch()
+            d = peak_defaults(settings)
+            sep_r = float(d.get("min_separation_rayleigh", DEFAULT_SEPARATION_RAYLEIGH))
+            order = int(d.get("harmonic_max", DEFAULT_HARMONIC_MAX))
+            tol_set = d.get("alias_tolerance")
+            sep = np.empty(len(dev))
+            tol = np.empty(len(dev))
+            for j, i in enumerate(dev):
+                f = prepared[i][0]
+                resolved = f.baseline > 0.0
+                separation = sep_r / f.baseline if resolved else 0.0
+                t = tol_set if tol_set is not None else (
+                    min(separation, 1.0 / f.baseline) if resolved else 0.0)
+                sep[j] = max(separation, 1e-12)
+                tol[j] = max(float(t), 1e-12)
+            n_peaks, _, fields = eng.rows(count, order, sep, tol)
+            for j, i in enumerate(dev):
+                rows[i] = self._row(items[i][0], prepared[i][0], int(n_peaks[j]), fields[j],
+                                    n_best, extra_keys)
+        return rows  # type: ignore[return-value]
+
+    def _row(self, key: str, f: LightCurve, k_have: int, fields: np.ndarray, n_best: int,
+             extra_keys: Sequence[str]) -> dict:
+        """One result row from the device's ranked peaks (period, frequency,
+        power, depth, depth_snr, duration, t0, sde per rank)."""
         names = ("depth", "depth_snr", "duration", "t0", "sde")
-        rows = []
-        for i, ((key, _), (f, _)) in enumerate(zip(keyed, prepared)):
-            k_have = int(n_peaks[i])
-            row: dict[str, Any] = {"key": key, "method": self.name, "backend": BACKEND_NAME,
-                                   "n_samples": f.n, "baseline": f.baseline}
-            row["best_period"] = float(fields[i, 0, 0]) if k_have else float("nan")
-            for rank in range(1, int(n_best) + 1):
-                have = rank <= k_have
-                fr = fields[i, rank - 1]
-                row[f"period_{rank}"] = float(fr[0]) if have else float("nan")
-                row[f"power_{rank}"] = float(fr[2]) if have else float("nan")
-                extra = {n: float(fr[3 + j]) for j, n in enumerate(names)} if have else {}
-                for ekey in extra_keys:
-                    row[f"{ekey}_{rank}"] = extra.get(ekey, float("nan"))
-                for ekey, v in extra.items():
-                    if ekey not in extra_keys:
-                        row[f"{ekey}_{rank}"] = v
-            rows.append(row)
-        return rows
+        row: dict[str, Any] = {"key": key, "method": self.name, "backend": BACKEND_NAME,
+                               "n_samples": f.n, "baseline": f.baseline}
+        row["best_period"] = float(fields[0, 0]) if k_have else float("nan")
+        for rank in range(1, int(n_best) + 1):
+            have = rank <= k_have
+            fr = fields[rank - 1] if rank - 1 < fields.shape[0] else None
+            row[f"period_{rank}"] = float(fr[0]) if have else float("nan")
+            row[f"power_{rank}"] = float(fr[2]) if have else float("nan")
+            extra = {n: float(fr[3 + j]) for j, n in enumerate(names)} if have else {}
+            for ekey in extra_keys:
+                row[f"{ekey}_{rank}"] = extra.get(ekey, float("nan"))
+            for ekey, v in extra.items():
+                if ekey not in extra_keys:
+                    row[f"{ekey}_{rank}"] = v
+        return row
 
     def _search(self, segments, curves, settings, engine):
         grid = _lib.PackedGrid.from_segments(segments, settings.bins_per_duration,

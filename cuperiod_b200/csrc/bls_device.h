@@ -67,7 +67,8 @@ struct SegmentDesc {
 
 struct CurveDesc {
     int64_t point_off;      // first point in the packed point arrays
-    int64_t out_off;        // offset of this curve's spectrum in each output field
+    int64_t out_off;        // this curve's spectrum in each output field starts at
+                            // out_off + (its grid's first period in the period arrays)
     int32_t n_points;
     int32_t mode;           // MODE_UNIFORM / MODE_GENERAL
     int32_t exact_all;      // 1: every admissible box is evaluated in FP64
@@ -90,18 +91,32 @@ struct WorkItem {
     int32_t p_count;        // periods in the tile (<= kMaxTile)
 };
 
-// The work of one launch is regular: every curve of one accumulation mode is cut
-// into the same tiles (segment s: ceil(n_periods / seg_cap[s]) tiles), so work
-// index i is curve order[i / tiles_per_curve] and tile i % tiles_per_curve of
-// that curve, located by a search of the per-segment tile prefix.
+// One launch may search several trial grids (each curve has one).  The curves
+// of one accumulation mode and one grid form a group whose work is regular:
+// every curve of the group is cut into the same tiles (segment s of the grid:
+// ceil(n_periods / seg_cap[s]) tiles), so the group's local work index i is
+// curve order[order_begin + i / tiles_per_curve] and tile i % tiles_per_curve of
+// that curve, located by a search of the group's per-segment tile prefix.
+// Groups follow one another in the item space, costliest curves first.
+struct WorkGroup {
+    int32_t item_begin;         // first work item of the group
+    int32_t tiles_per_curve;
+    int32_t seg_begin;          // the grid's first segment in the segment table
+    int32_t n_segments;         // the grid's segments
+    int32_t order_begin;        // the group's first entry of order
+    int32_t tiles_begin;        // the group's tile prefix: seg_tiles[tiles_begin ..
+                                // tiles_begin + n_segments]
+};
+
 struct BatchArgs {
     const CurveDesc* curves;
     const SegmentDesc* segments;
-    const int32_t* order;       // this mode's curves, most points first
-    const int32_t* seg_tiles;   // n_segments + 1: prefix of tiles per curve
-    const int32_t* seg_cap;     // n_segments: periods per tile
-    int32_t tiles_per_curve;
-    int32_t n_segments;
+    const WorkGroup* groups;    // n_groups, ascending item_begin (the first is 0)
+    const int32_t* order;       // per group: its curves, most points first
+    const int32_t* seg_tiles;   // per group: n_segments + 1 tile prefix per curve
+    const int32_t* seg_cap;     // per segment of the table: periods per tile
+    WorkGroup group0;           // groups[0], read from the launch parameters
+    int32_t n_groups;
     const double* tau;          // per point: t - t_min (FP64)
     const uint32_t* pay_r;      // per point: r_q as low 13 bits | signed high part << 16
     const double* r64;          // GENERAL: (y*ivar - ybar*ivar) * 2^e_r per point;

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cfloat>
 #include <cmath>
@@ -207,7 +208,12 @@ struct BlsEngine {
     // the prepared batch
     bool prepared = false;
     int n_curves = 0;
-    int64_t n_periods = 0;
+    int n_grids = 0;
+    int64_t spec_total = 0;             // spectrum entries per output field, all curves
+    int64_t max_periods = 0;            // the longest curve spectrum
+    std::vector<int64_t> grid_pbase;    // grid k's periods: [grid_pbase[k], grid_pbase[k + 1])
+    const int64_t* d_spec_off = nullptr;    // device: per-curve spectrum offsets (n_curves + 1)
+    const int64_t* d_grid_base = nullptr;   // device: per-curve first period of its grid
     int n_items_mode[kModes] = {0, 0, 0};
     int ctas_mode[kModes] = {0, 0, 0};
     size_t smem_mode[kModes] = {0, 0, 0};
@@ -448,22 +454,57 @@ int tile_cap(int mode, int hl, size_t smem, int max_tile) {
     return cap;
 }
 
-int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t st) {
-    if (!g || !cv) return fail(BLS_E_INVALID, "grid and curves are required");
-    if (g->n_segments < 0 || (g->n_segments > 0 && (!g->seg_offsets || !g->dur_offsets)))
-        return fail(BLS_E_INVALID, "bad segment table");
-    if (g->oversample < 1) return fail(BLS_E_INVALID, "oversample must be >= 1");
-    if (g->objective != 0 && g->objective != 1)
-        return fail(BLS_E_INVALID, "objective must be 'snr' or 'likelihood'");
+// Pack and upload one batch.  Curve c is searched over grids[grid_of_curve[c]]
+// (over grids[0] for every curve when grid_of_curve is NULL); the grids'
+// segments and periods are concatenated, grid k's from sbase[k] / pbase[k].
+int do_prepare(BlsEngine* e, const BlsGrid* grids, int n_grids, const int32_t* grid_of_curve,
+               const BlsCurves* cv, cudaStream_t st) {
+    if (!grids || !cv || n_grids < 1) return fail(BLS_E_INVALID, "grid and curves are required");
+    for (int k = 0; k < n_grids; ++k) {
+        const BlsGrid* g = grids + k;
+        if (g->n_segments < 0 || (g->n_segments > 0 && (!g->seg_offsets || !g->dur_offsets)))
+            return fail(BLS_E_INVALID, "bad segment table");
+        if (g->oversample < 1) return fail(BLS_E_INVALID, "oversample must be >= 1");
+        if (g->objective != 0 && g->objective != 1)
+            return fail(BLS_E_INVALID, "objective must be 'snr' or 'likelihood'");
+        if (g->oversample != grids[0].oversample || g->objective != grids[0].objective)
+            return fail(BLS_E_INVALID,
+                        "the grids of one batch must share oversample and objective (grid %d)", k);
+        if (g->n_segments > 0 && g->seg_offsets[0] != 0)
+            return fail(BLS_E_INVALID, "seg_offsets[0] must be 0");
+        if (g->n_segments > 0 && g->seg_offsets[g->n_segments] < 0)
+            return fail(BLS_E_INVALID, "grid %d: bad period offsets", k);
+    }
     if (cv->n_curves < 1 || !cv->offsets || !cv->t || !cv->y)
         return fail(BLS_E_INVALID, "at least one light curve is required");
     e->prepared = false;
     e->graph_valid = false;
     const int nc = cv->n_curves;
-    const int ns = g->n_segments;
-    const int o = g->oversample;
-    const int64_t P_total = ns > 0 ? g->seg_offsets[ns] - g->seg_offsets[0] : 0;
-    if (ns > 0 && g->seg_offsets[0] != 0) return fail(BLS_E_INVALID, "seg_offsets[0] must be 0");
+    const int o = grids[0].oversample;
+    std::vector<int> sbase(n_grids + 1, 0);
+    std::vector<int64_t> pbase(n_grids + 1, 0);
+    for (int k = 0; k < n_grids; ++k) {
+        const BlsGrid& g = grids[k];
+        if ((int64_t)sbase[k] + g.n_segments > (1 << 24))
+            return fail(BLS_E_INVALID, "too many segments in one batch");
+        sbase[k + 1] = sbase[k] + g.n_segments;
+        pbase[k + 1] = pbase[k] + (g.n_segments > 0 ? g.seg_offsets[g.n_segments] : 0);
+    }
+    const int ns = sbase[n_grids];
+    const int64_t P_total = pbase[n_grids];
+    std::vector<int32_t> gid(nc, 0);
+    if (grid_of_curve)
+        for (int c = 0; c < nc; ++c) {
+            if (grid_of_curve[c] < 0 || grid_of_curve[c] >= n_grids)
+                return fail(BLS_E_INVALID, "curve %d: grid index %d outside 0..%d", c,
+                            grid_of_curve[c], n_grids - 1);
+            gid[c] = grid_of_curve[c];
+        }
+    // curve c's spectrum: [spec_off[c], spec_off[c + 1]) of each output field
+    std::vector<int64_t> spec_off(nc + 1, 0);
+    for (int c = 0; c < nc; ++c)
+        spec_off[c + 1] = spec_off[c] + (pbase[gid[c] + 1] - pbase[gid[c]]);
+    const int64_t spec_total = spec_off[nc];
     const int64_t n_pts = cv->offsets[nc] - cv->offsets[0];
     if (cv->offsets[0] != 0 || n_pts < 0) return fail(BLS_E_INVALID, "offsets[0] must be 0");
 
@@ -484,117 +525,164 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
         const int64_t off = cv->offsets[c];
         pack_curve(cv, c, off, htau + off, hpr + off, hr64 + off, hiv64 + off, curves[c],
                    scratch[w]);
-        curves[c].d.out_off = (int64_t)c * P_total;
+        curves[c].d.out_off = spec_off[c] - pbase[gid[c]];
     });
-    double tau_max = 0.0;
     int n_uniform = 0;
     int n_mode[kModes] = {0, 0, 0};
+    std::vector<double> tau_max(n_grids, 0.0);                  // per grid, over its curves
+    std::vector<std::array<int, kModes>> grid_mode(n_grids, std::array<int, kModes>{0, 0, 0});
     for (int c = 0; c < nc; ++c) {
         if (curves[c].status) return fail(curves[c].status, "%s", curves[c].err.c_str());
         if (e->tune.exact_sweep) curves[c].d.exact_all = 1;
-        tau_max = std::max(tau_max, curves[c].tau_max);
+        tau_max[gid[c]] = std::max(tau_max[gid[c]], curves[c].tau_max);
         n_uniform += curves[c].d.mode == MODE_UNIFORM;
         n_mode[curves[c].d.mode]++;
+        grid_mode[gid[c]][curves[c].d.mode]++;
     }
 
-    // ---- segments and period constants (reference binning) ---------------------
+    // ---- segments and period constants (reference binning), grids in parallel ---
     std::vector<SegmentHost> segs(ns);
     std::vector<double> per(P_total);
     std::vector<PeriodConst> pc(P_total);
+    std::vector<double> grid_boxes(n_grids, 0.0), grid_trials(n_grids, 0.0);
+    std::vector<int> grid_err(n_grids, BLS_OK);
+    std::vector<std::string> grid_msg(n_grids);
+    parallel_for(n_grids, [&](int k, int /*w*/) {
+        const BlsGrid& g = grids[k];
+        auto bad = [&](int code, std::string msg) {
+            grid_err[k] = code;
+            grid_msg[k] = std::move(msg);
+        };
+        char buf[256];
+        for (int sl = 0; sl < g.n_segments; ++sl) {
+            const int s = sbase[k] + sl;
+            const int64_t q0 = g.seg_offsets[sl], q1 = g.seg_offsets[sl + 1];   // this grid's
+            const int64_t d0 = g.dur_offsets[sl], d1 = g.dur_offsets[sl + 1];
+            if (q1 < q0 || d1 < d0) {
+                std::snprintf(buf, sizeof buf, "segment %d: bad offsets", s);
+                return bad(BLS_E_INVALID, buf);
+            }
+            const int64_t p0 = pbase[k] + q0, p1 = pbase[k] + q1;                // concatenated
+            SegmentHost& sh = segs[s];
+            SegmentDesc& sd = sh.d;
+            std::memset(&sd, 0, sizeof(sd));
+            sd.period_off = p0;
+            sd.n_periods = (int32_t)(p1 - p0);
+            sd.oversample = o;
+            if (p1 == p0) {
+                sh.empty_periods = true;
+                continue;
+            }
+            if (d1 == d0) {
+                std::snprintf(buf, sizeof buf, "segment %d has no durations", s);
+                return bad(BLS_E_INVALID, buf);
+            }
+            double dmin = INFINITY, pmax = 0.0, fmax = 0.0;
+            for (int64_t i = d0; i < d1; ++i) {
+                const double d = g.durations[i];
+                if (!(std::isfinite(d) && d > 0.0)) {
+                    std::snprintf(buf, sizeof buf,
+                                  "segment %d: durations must be finite and > 0", s);
+                    return bad(BLS_E_INVALID, buf);
+                }
+                dmin = std::min(dmin, d);
+            }
+            for (int64_t i = q0; i < q1; ++i) {
+                const double P = g.periods[i];
+                if (!(std::isfinite(P) && P > 0.0)) {
+                    std::snprintf(buf, sizeof buf,
+                                  "BLS: trial periods must be finite and > 0 (segment %d)", s);
+                    return bad(BLS_E_INVALID, buf);
+                }
+                pmax = std::max(pmax, P);
+                per[pbase[k] + i] = P;
+            }
+            const double bin = dmin / (double)o;                              // _search_spec
+            for (int64_t i = d0; i < d1; ++i) {                               // _duration_bins
+                const double kd = std::floor(g.durations[i] / bin + 0.5);
+                if (kd >= 1.0 && kd < 2147483647.0) {
+                    const int32_t kk = (int32_t)kd;
+                    if (std::find(sh.dur.begin(), sh.dur.end(), kk) == sh.dur.end())
+                        sh.dur.push_back(kk);
+                }
+            }
+            if ((int)sh.dur.size() > kMaxDur) {
+                std::snprintf(buf, sizeof buf, "segment %d: more than %d distinct box widths", s,
+                              kMaxDur);
+                return bad(BLS_E_INVALID, buf);
+            }
+            const double wmax = std::ceil(pmax / bin) + (double)o + 1.0;
+            if (!(wmax < 1073741824.0)) {
+                std::snprintf(buf, sizeof buf, "segment %d: %.3g phase bins per period", s, wmax);
+                return bad(BLS_E_RESOURCE, buf);
+            }
+            const int64_t width = (int64_t)wmax;
+            int64_t hl = 2;
+            double smax = 0.0;
+            for (int64_t i = p0; i < p1; ++i) {
+                const double P = per[i];
+                const int64_t nb = period_bins(P, bin, o, width);
+                hl = std::max(hl, nb + 1);
+                fmax = std::max(fmax, 1.0 / P);
+                smax = std::max(smax, P / bin);
+            }
+            sd.width = (int32_t)width;
+            sd.bin_duration = bin;
+            sd.n_dur = (int32_t)sh.dur.size();
+            sd.hist_len = (int32_t)hl;
+            FoldParams fp = fold_params(width, bin, tau_max[k], fmax, smax);
+            const double scale = std::ldexp(1.0, fp.fb);
+            for (int64_t i = p0; i < p1 && fp.fast; ++i) {
+                const double P = per[i];
+                const double sc = std::nearbyint((P / bin) * scale);
+                const int64_t nb = period_bins(P, bin, o, width);
+                if (!(sc >= 1.0 && sc < 4294967296.0)) { fp.fast = false; break; }
+                const uint32_t S = (uint32_t)sc;
+                // the fast fold's largest bin, ((S - 1) >> fb) + 1, must stay inside n_bins
+                if ((int64_t)((S - 1u) >> fp.fb) + 1 > nb) { fp.fast = false; break; }
+            }
+            double boxes = 0.0;
+            for (int64_t i = p0; i < p1; ++i) {
+                const double P = per[i];
+                pc[i].f = 1.0 / P;
+                pc[i].nb = (int32_t)period_bins(P, bin, o, width);
+                pc[i].S = fp.fast ? (uint32_t)std::nearbyint((P / bin) * scale) : 0u;
+                for (int32_t kk : sh.dur)
+                    if (kk < pc[i].nb) boxes += (double)(pc[i].nb - kk + 1);
+            }
+            sd.fast_fold = fp.fast;
+            sd.frac_bits = fp.fast ? fp.fb : 0;
+            sd.margin_u = fp.mu;
+            sd.margin_phi = fp.mphi;
+            grid_boxes[k] += boxes;                  // per curve of this grid
+            grid_trials[k] += (double)sd.n_periods * sh.dur.size();
+        }
+    });
+    for (int k = 0; k < n_grids; ++k)
+        if (grid_err[k]) return fail(grid_err[k], "%s", grid_msg[k].c_str());
     std::vector<int32_t> dur_all;
     int max_hl = 2;
     int fast_segments = 0;
     for (int s = 0; s < ns; ++s) {
-        const int64_t p0 = g->seg_offsets[s], p1 = g->seg_offsets[s + 1];
-        const int64_t d0 = g->dur_offsets[s], d1 = g->dur_offsets[s + 1];
-        if (p1 < p0 || d1 < d0) return fail(BLS_E_INVALID, "segment %d: bad offsets", s);
         SegmentHost& sh = segs[s];
-        SegmentDesc& sd = sh.d;
-        std::memset(&sd, 0, sizeof(sd));
-        sd.period_off = p0;
-        sd.n_periods = (int32_t)(p1 - p0);
-        sd.oversample = o;
-        sd.dur_off = (int32_t)dur_all.size();
-        if (p1 == p0) {
-            sh.empty_periods = true;
-            continue;
-        }
-        if (d1 == d0) return fail(BLS_E_INVALID, "segment %d has no durations", s);
-        double dmin = INFINITY, pmax = 0.0, fmax = 0.0;
-        for (int64_t i = d0; i < d1; ++i) {
-            const double d = g->durations[i];
-            if (!(std::isfinite(d) && d > 0.0))
-                return fail(BLS_E_INVALID, "segment %d: durations must be finite and > 0", s);
-            dmin = std::min(dmin, d);
-        }
-        for (int64_t i = p0; i < p1; ++i) {
-            const double P = g->periods[i];
-            if (!(std::isfinite(P) && P > 0.0))
-                return fail(BLS_E_INVALID,
-                            "BLS: trial periods must be finite and > 0 (segment %d)", s);
-            pmax = std::max(pmax, P);
-            per[i] = P;
-        }
-        const double bin = dmin / (double)o;                                  // _search_spec
-        for (int64_t i = d0; i < d1; ++i) {                                   // _duration_bins
-            const double kd = std::floor(g->durations[i] / bin + 0.5);
-            if (kd >= 1.0 && kd < 2147483647.0) {
-                const int32_t k = (int32_t)kd;
-                if (std::find(sh.dur.begin(), sh.dur.end(), k) == sh.dur.end()) sh.dur.push_back(k);
-            }
-        }
-        if ((int)sh.dur.size() > kMaxDur)
-            return fail(BLS_E_INVALID, "segment %d: more than %d distinct box widths", s, kMaxDur);
-        const double wmax = std::ceil(pmax / bin) + (double)o + 1.0;
-        if (!(wmax < 1073741824.0))
-            return fail(BLS_E_RESOURCE, "segment %d: %.3g phase bins per period", s, wmax);
-        const int64_t width = (int64_t)wmax;
-        int64_t hl = 2;
-        double smax = 0.0;
-        for (int64_t i = p0; i < p1; ++i) {
-            const double P = per[i];
-            const int64_t nb = period_bins(P, bin, o, width);
-            hl = std::max(hl, nb + 1);
-            fmax = std::max(fmax, 1.0 / P);
-            smax = std::max(smax, P / bin);
-        }
-        sd.width = (int32_t)width;
-        sd.bin_duration = bin;
-        sd.n_dur = (int32_t)sh.dur.size();
-        sd.hist_len = (int32_t)hl;
-        FoldParams fp = fold_params(width, bin, tau_max, fmax, smax);
-        const double scale = std::ldexp(1.0, fp.fb);
-        for (int64_t i = p0; i < p1 && fp.fast; ++i) {
-            const double P = per[i];
-            const double sc = std::nearbyint((P / bin) * scale);
-            const int64_t nb = period_bins(P, bin, o, width);
-            if (!(sc >= 1.0 && sc < 4294967296.0)) { fp.fast = false; break; }
-            const uint32_t S = (uint32_t)sc;
-            // the fast fold's largest bin, ((S - 1) >> fb) + 1, must stay inside n_bins
-            if ((int64_t)((S - 1u) >> fp.fb) + 1 > nb) { fp.fast = false; break; }
-        }
-        for (int64_t i = p0; i < p1; ++i) {
-            const double P = per[i];
-            pc[i].f = 1.0 / P;
-            pc[i].nb = (int32_t)period_bins(P, bin, o, width);
-            pc[i].S = fp.fast ? (uint32_t)std::nearbyint((P / bin) * scale) : 0u;
-        }
-        sd.fast_fold = fp.fast;
-        sd.frac_bits = fp.fast ? fp.fb : 0;
-        sd.margin_u = fp.mu;
-        sd.margin_phi = fp.mphi;
-        fast_segments += fp.fast;
-        max_hl = std::max<int>(max_hl, (int)hl);
+        sh.d.dur_off = (int32_t)dur_all.size();
+        if (sh.empty_periods) continue;
+        fast_segments += sh.d.fast_fold;
+        max_hl = std::max<int>(max_hl, sh.d.hist_len);
         dur_all.insert(dur_all.end(), sh.dur.begin(), sh.dur.end());
     }
+    (void)max_hl;
+    std::vector<int> seg_grid(ns, 0);
+    for (int k = 0; k < n_grids; ++k)
+        for (int s = sbase[k]; s < sbase[k + 1]; ++s) seg_grid[s] = k;
 
-    // ---- shared memory, tiles, work items (largest first) ----------------------
+    // ---- shared memory, tiles, work groups (costliest first) -------------------
     bool modes[kModes] = {n_mode[0] > 0, n_mode[1] > 0, n_mode[2] > 0};
     size_t smem_mode[kModes];
     for (int m = 0; m < kModes; ++m) {
         size_t sm = e->tune.smem_per_cta > 0 ? (size_t)e->tune.smem_per_cta : kDefaultSmem[m];
         for (int s = 0; s < ns && modes[m]; ++s) {
-            if (segs[s].empty_periods) continue;
+            if (segs[s].empty_periods || grid_mode[seg_grid[s]][m] == 0) continue;
             const size_t need = screen_bytes(m, segs[s].d.hist_len) + 16 +
                                 period_bytes(m, segs[s].d.hist_len);
             if (need > sm) sm = need;
@@ -610,60 +698,92 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
                         sm, limit);
         smem_mode[m] = sm;
     }
-    // per segment: boxes of one curve (the same for every curve)
-    double seg_box_sum = 0.0, trials_per_curve = 0.0;
-    for (int s = 0; s < ns; ++s) {
-        const SegmentHost& sh = segs[s];
-        if (sh.empty_periods) continue;
-        const int64_t p0 = sh.d.period_off;
-        for (int32_t p = 0; p < sh.d.n_periods; ++p) {
-            const int nb = pc[p0 + p].nb;
-            for (int32_t k : sh.dur)
-                if (k < nb) seg_box_sum += (double)(nb - k + 1);
-        }
-        trials_per_curve += (double)sh.d.n_periods * sh.dur.size();
-    }
-    // per mode: tiles of each segment, their prefix, and the curves largest first
+    // per mode: one group per grid with curves of that mode -- the grid's tile
+    // prefix and its curves largest first -- groups in decreasing cost per curve
     // (so the last work items of a launch are the cheapest)
+    std::vector<WorkGroup> plan_groups[kModes];
     std::vector<int32_t> plan_tiles[kModes], plan_cap[kModes], plan_order[kModes];
     int64_t n_items_mode[kModes] = {0, 0, 0};
+    std::vector<std::vector<int32_t>> members(n_grids);
     for (int m = 0; m < kModes; ++m) {
-        plan_tiles[m].assign(ns + 1, 0);
         plan_cap[m].assign(std::max(ns, 1), 1);
         if (!modes[m]) continue;
-        int64_t acc = 0;
-        for (int s = 0; s < ns; ++s) {
-            plan_tiles[m][s] = (int32_t)acc;
-            if (segs[s].empty_periods) continue;
-            const int cap = tile_cap(m, segs[s].d.hist_len, smem_mode[m], e->tune.max_tile);
-            if (cap < 1) return fail(BLS_E_RESOURCE, "segment %d does not fit shared memory", s);
-            plan_cap[m][s] = cap;
-            acc += (segs[s].d.n_periods + cap - 1) / cap;
-            if (acc > INT32_MAX) return fail(BLS_E_RESOURCE, "too many period tiles per curve");
-        }
-        plan_tiles[m][ns] = (int32_t)acc;
+        for (auto& v : members) v.clear();
         for (int c = 0; c < nc; ++c)
-            if (curves[c].d.mode == m) plan_order[m].push_back(c);
-        std::stable_sort(plan_order[m].begin(), plan_order[m].end(), [&](int x, int y) {
-            return curves[x].d.n_points > curves[y].d.n_points;
-        });
-        n_items_mode[m] = acc * (int64_t)plan_order[m].size();
-        if (n_items_mode[m] > INT32_MAX)
-            return fail(BLS_E_RESOURCE,
-                        "%lld work items exceed one launch; split the batch into fewer curves",
-                        (long long)n_items_mode[m]);
+            if (curves[c].d.mode == m) members[gid[c]].push_back(c);
+        struct Cand {
+            int grid;
+            int64_t tiles;
+            double cost;
+            std::vector<int32_t> prefix;
+        };
+        std::vector<Cand> cands;
+        for (int k = 0; k < n_grids; ++k) {
+            if (members[k].empty()) continue;
+            Cand q{k, 0, 0.0, std::vector<int32_t>(grids[k].n_segments + 1, 0)};
+            int64_t acc = 0;
+            for (int sl = 0; sl < grids[k].n_segments; ++sl) {
+                const int s = sbase[k] + sl;
+                q.prefix[sl] = (int32_t)acc;
+                if (segs[s].empty_periods) continue;
+                const int cap = tile_cap(m, segs[s].d.hist_len, smem_mode[m], e->tune.max_tile);
+                if (cap < 1) return fail(BLS_E_RESOURCE, "segment %d does not fit shared memory", s);
+                plan_cap[m][s] = cap;
+                acc += (segs[s].d.n_periods + cap - 1) / cap;
+                if (acc > INT32_MAX) return fail(BLS_E_RESOURCE, "too many period tiles per curve");
+            }
+            q.prefix[grids[k].n_segments] = (int32_t)acc;
+            q.tiles = acc;
+            if (acc == 0) continue;                  // no trial period: nothing to search
+            std::stable_sort(members[k].begin(), members[k].end(), [&](int x, int y) {
+                return curves[x].d.n_points > curves[y].d.n_points;
+            });
+            q.cost = (double)curves[members[k][0]].d.n_points *
+                     (double)(pbase[k + 1] - pbase[k]);
+            cands.push_back(std::move(q));
+        }
+        std::stable_sort(cands.begin(), cands.end(),
+                         [](const Cand& x, const Cand& y) { return x.cost > y.cost; });
+        int64_t items = 0;
+        for (const Cand& q : cands) {
+            WorkGroup w;
+            w.item_begin = (int32_t)items;
+            w.tiles_per_curve = (int32_t)q.tiles;
+            w.seg_begin = sbase[q.grid];
+            w.n_segments = grids[q.grid].n_segments;
+            w.order_begin = (int32_t)plan_order[m].size();
+            w.tiles_begin = (int32_t)plan_tiles[m].size();
+            plan_groups[m].push_back(w);
+            plan_tiles[m].insert(plan_tiles[m].end(), q.prefix.begin(), q.prefix.end());
+            plan_order[m].insert(plan_order[m].end(), members[q.grid].begin(),
+                                 members[q.grid].end());
+            items += q.tiles * (int64_t)members[q.grid].size();
+            if (items > INT32_MAX)
+                return fail(BLS_E_RESOURCE,
+                            "%lld work items exceed one launch; split the batch into fewer curves",
+                            (long long)items);
+        }
+        n_items_mode[m] = items;
     }
-    const double folds = (double)n_pts * (double)P_total;   // each point, each period
-    const double boxes = seg_box_sum * nc;
-    const double trials = trials_per_curve * nc;
+    double folds = 0.0, boxes = 0.0, trials = 0.0;
+    for (int c = 0; c < nc; ++c) {
+        const int k = gid[c];
+        folds += (double)curves[c].d.n_points * (double)(pbase[k + 1] - pbase[k]);
+        boxes += grid_boxes[k];
+        trials += grid_trials[k];
+    }
 
     // ---- stage metadata and upload ---------------------------------------------
     const int64_t n_items = n_items_mode[0] + n_items_mode[1] + n_items_mode[2];
     const size_t grid_bytes = (size_t)P_total * (8 + 8 + 4 + 4) + dur_all.size() * 4 + 64;
-    // descriptors, then per mode: order (nc in all), seg_tiles (ns + 1), seg_cap (ns)
-    const size_t plan_words =
-        (size_t)nc + kModes * (size_t)(ns + 1) + kModes * (size_t)std::max(ns, 1);
+    // descriptors, per-curve spectrum offsets and grid bases (int64), then per
+    // mode: groups, order, seg_tiles and seg_cap (int32 words)
+    size_t plan_words = 0;
+    for (int m = 0; m < kModes; ++m)
+        plan_words += plan_groups[m].size() * (sizeof(WorkGroup) / 4) + plan_order[m].size() +
+                      plan_tiles[m].size() + plan_cap[m].size();
     const size_t meta_bytes = sizeof(CurveDesc) * nc + sizeof(SegmentDesc) * std::max(ns, 1) +
+                              sizeof(int64_t) * (2 * (size_t)nc + 1) +
                               sizeof(int32_t) * plan_words + 64;
     if ((rc = e->h_grid.ensure(grid_bytes))) return rc;
     if ((rc = e->h_meta.ensure(meta_bytes))) return rc;
@@ -683,29 +803,34 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     char* mp = e->h_meta.as<char>();
     CurveDesc* hcur = reinterpret_cast<CurveDesc*>(mp);
     SegmentDesc* hseg = reinterpret_cast<SegmentDesc*>(hcur + nc);
-    int32_t* hplan = reinterpret_cast<int32_t*>(hseg + std::max(ns, 1));
+    int64_t* hspec = reinterpret_cast<int64_t*>(hseg + std::max(ns, 1));
+    int64_t* hgbase = hspec + nc + 1;
+    int32_t* hplan = reinterpret_cast<int32_t*>(hgbase + nc);
     for (int c = 0; c < nc; ++c) hcur[c] = curves[c].d;
     for (int s = 0; s < ns; ++s) hseg[s] = segs[s].d;
-    size_t plan_off[kModes][3];     // per mode: order, seg_tiles, seg_cap (in words)
+    std::copy(spec_off.begin(), spec_off.end(), hspec);
+    for (int c = 0; c < nc; ++c) hgbase[c] = pbase[gid[c]];
+    size_t plan_off[kModes][4];     // per mode: groups, order, seg_tiles, seg_cap (in words)
     {
         size_t w = 0;
         for (int m = 0; m < kModes; ++m) {
             plan_off[m][0] = w;
+            std::memcpy(hplan + w, plan_groups[m].data(), plan_groups[m].size() * sizeof(WorkGroup));
+            w += plan_groups[m].size() * (sizeof(WorkGroup) / 4);
+            plan_off[m][1] = w;
             std::copy(plan_order[m].begin(), plan_order[m].end(), hplan + w);
             w += plan_order[m].size();
-        }
-        for (int m = 0; m < kModes; ++m) {
-            plan_off[m][1] = w;
-            std::copy(plan_tiles[m].begin(), plan_tiles[m].end(), hplan + w);
-            w += ns + 1;
             plan_off[m][2] = w;
+            std::copy(plan_tiles[m].begin(), plan_tiles[m].end(), hplan + w);
+            w += plan_tiles[m].size();
+            plan_off[m][3] = w;
             std::copy(plan_cap[m].begin(), plan_cap[m].end(), hplan + w);
-            w += std::max(ns, 1);
+            w += plan_cap[m].size();
         }
     }
     for (int m = 0; m < kModes; ++m) e->n_items_mode[m] = (int32_t)n_items_mode[m];
 
-    const size_t out_elems = (size_t)kFields * nc * std::max<int64_t>(P_total, 1);
+    const size_t out_elems = (size_t)kFields * std::max<int64_t>(spec_total, 1);
     if ((rc = e->d_tau.ensure(sizeof(double) * std::max<int64_t>(n_pts, 1)))) return rc;
     if ((rc = e->d_pay_r.ensure(sizeof(uint32_t) * std::max<int64_t>(n_pts, 1)))) return rc;
     if ((rc = e->d_r64.ensure(sizeof(double) * std::max<int64_t>(n_pts, 1)))) return rc;
@@ -748,18 +873,21 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     const char* dmp = e->d_curves.as<char>();
     const CurveDesc* dcur = reinterpret_cast<const CurveDesc*>(dmp);
     const SegmentDesc* dseg = reinterpret_cast<const SegmentDesc*>(dcur + nc);
-    const int32_t* dplan = reinterpret_cast<const int32_t*>(dseg + std::max(ns, 1));
+    const int64_t* dspec = reinterpret_cast<const int64_t*>(dseg + std::max(ns, 1));
+    const int64_t* dgbase = dspec + nc + 1;
+    const int32_t* dplan = reinterpret_cast<const int32_t*>(dgbase + nc);
     int32_t* ctl = e->d_ctl.as<int32_t>();
     int ctas_total = 0;
     for (int m = 0; m < kModes; ++m) {
         BatchArgs& a = e->args[m];
         a.curves = dcur;
         a.segments = dseg;
-        a.order = dplan + plan_off[m][0];
-        a.seg_tiles = dplan + plan_off[m][1];
-        a.seg_cap = dplan + plan_off[m][2];
-        a.tiles_per_curve = plan_tiles[m][ns];
-        a.n_segments = ns;
+        a.groups = reinterpret_cast<const WorkGroup*>(dplan + plan_off[m][0]);
+        a.n_groups = (int32_t)plan_groups[m].size();
+        a.group0 = plan_groups[m].empty() ? WorkGroup{} : plan_groups[m][0];
+        a.order = dplan + plan_off[m][1];
+        a.seg_tiles = dplan + plan_off[m][2];
+        a.seg_cap = dplan + plan_off[m][3];
         a.n_items = e->n_items_mode[m];
         a.tau = e->d_tau.as<double>();
         a.pay_r = e->d_pay_r.as<uint32_t>();
@@ -771,22 +899,29 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
         a.nbins = dnb;
         a.dur_bins = ddur;
         a.out = e->d_out.as<double>();
-        a.out_stride = (int64_t)nc * P_total;
+        a.out_stride = spec_total;
         a.work_counter = ctl + m;
         a.error_flag = ctl + 8;
         a.debug_prefix = nullptr;
-        a.obj_flag = g->objective;
+        a.obj_flag = grids[0].objective;
         const int per_sm = std::max(1, max_resident_ctas(m, smem_mode[m]));
         e->ctas_mode[m] = std::min(a.n_items, e->n_sm * per_sm);
         ctas_total = std::max(ctas_total, e->ctas_mode[m]);
     }
+    int64_t max_periods = 0;
+    for (int k = 0; k < n_grids; ++k) max_periods = std::max(max_periods, pbase[k + 1] - pbase[k]);
     for (int m = 0; m < kModes; ++m) e->smem_mode[m] = smem_mode[m];
     e->n_curves = nc;
-    e->n_periods = P_total;
+    e->n_grids = n_grids;
+    e->spec_total = spec_total;
+    e->max_periods = max_periods;
+    e->grid_pbase = pbase;
+    e->d_spec_off = dspec;
+    e->d_grid_base = dgbase;
     BlsBatchInfo& in = e->info;
     in.n_curves = nc;
     in.n_segments = ns;
-    in.n_periods = P_total;
+    in.n_periods = max_periods;
     in.n_items = (int64_t)n_items;
     in.n_points = n_pts;
     in.folds = folds;
@@ -797,6 +932,9 @@ int do_prepare(BlsEngine* e, const BlsGrid* g, const BlsCurves* cv, cudaStream_t
     in.smem_per_cta = (int32_t)(modes[0] ? smem_mode[0] : modes[2] ? smem_mode[2] : smem_mode[1]);
     in.uniform_curves = n_uniform;
     in.fast_fold_segments = fast_segments;
+    in.spectrum = spec_total;
+    in.n_grids = n_grids;
+    in.reserved = 0;
     e->prepared = true;
     return BLS_OK;
 }
@@ -1415,7 +1553,17 @@ int bls_engine_destroy(BlsEngine* engine) {
 int bls_prepare(BlsEngine* e, const BlsGrid* grid, const BlsCurves* curves, void* stream) {
     if (!e) return fail(BLS_E_INVALID, "engine is NULL");
     cudaSetDevice(e->device);
-    return do_prepare(e, grid, curves, pick(e, stream));
+    return do_prepare(e, grid, 1, nullptr, curves, pick(e, stream));
+}
+
+int bls_prepare_grids(BlsEngine* e, int32_t n_grids, const BlsGrid* grids,
+                      const int32_t* grid_of_curve, const BlsCurves* curves, void* stream) {
+    if (!e) return fail(BLS_E_INVALID, "engine is NULL");
+    if (n_grids < 1 || !grids) return fail(BLS_E_INVALID, "at least one grid is required");
+    if (n_grids > 1 && !grid_of_curve)
+        return fail(BLS_E_INVALID, "grid_of_curve is required with more than one grid");
+    cudaSetDevice(e->device);
+    return do_prepare(e, grids, n_grids, grid_of_curve, curves, pick(e, stream));
 }
 
 int bls_launch(BlsEngine* e, void* stream) {
@@ -1483,7 +1631,7 @@ int bls_download(BlsEngine* e, double* out, void* stream) {
     if (!e->prepared) return fail(BLS_E_STATE, "bls_download before bls_prepare");
     cudaSetDevice(e->device);
     cudaStream_t st = pick(e, stream);
-    const size_t bytes = sizeof(double) * kFields * e->n_curves * e->n_periods;
+    const size_t bytes = sizeof(double) * kFields * (size_t)e->spec_total;
     if (bytes) CUDA_TRY(cudaMemcpyAsync(out, e->d_out.p, bytes, cudaMemcpyDeviceToHost, st),
                         "download outputs");
     return check_device_flag(e, st);
@@ -1510,7 +1658,8 @@ int bls_download_best(BlsEngine* e, int64_t* best_index, double* best_power, dou
     if ((rc = e->h_best.ensure(bytes))) return rc;
     int64_t* di = e->d_best.as<int64_t>();
     double* dv = reinterpret_cast<double*>(di + nc);
-    CUDA_TRY(launch_best(e->d_out.as<double>(), nc, e->n_periods, di, dv, dv + nc, dv + 2 * nc, st),
+    CUDA_TRY(launch_best(e->d_out.as<double>(), nc, e->d_spec_off, di, dv, dv + nc, dv + 2 * nc,
+                         st),
              "best-of-spectrum launch");
     CUDA_TRY(cudaMemcpyAsync(e->h_best.p, e->d_best.p, bytes, cudaMemcpyDeviceToHost, st),
              "download best");
@@ -1534,13 +1683,14 @@ int bls_download_rows(BlsEngine* e, int32_t n_best, int32_t harmonic_max,
     if (harmonic_max < 1 || harmonic_max > 4096)
         return fail(BLS_E_INVALID, "harmonic_max must be in 1..4096");
     const int nc = e->n_curves;
-    const int64_t P = e->n_periods;
+    const int64_t P = e->max_periods;
     if (P < 1) return fail(BLS_E_INVALID, "the prepared grid has no periods");
     // frequency order is reversed grid order only for strictly increasing periods
     const double* hper = e->h_grid.as<double>();
-    for (int64_t i = 1; i < P; ++i)
-        if (!(hper[i] > hper[i - 1]))
-            return fail(BLS_E_INVALID, "rows need strictly increasing trial periods");
+    for (int k = 0; k < e->n_grids; ++k)
+        for (int64_t i = e->grid_pbase[k] + 1; i < e->grid_pbase[k + 1]; ++i)
+            if (!(hper[i] > hper[i - 1]))
+                return fail(BLS_E_INVALID, "rows need strictly increasing trial periods");
     const size_t mask_bytes = sizeof(uint32_t) * (size_t)((P + 31) / 32);
     if (mask_bytes + 4096 > e->smem_optin)
         return fail(BLS_E_RESOURCE, "%lld periods exceed the peak search's shared memory",
@@ -1568,8 +1718,9 @@ int bls_download_rows(BlsEngine* e, int32_t n_best, int32_t harmonic_max,
     int64_t* didx = reinterpret_cast<int64_t*>(db + in_bytes);
     double* dfld = reinterpret_cast<double*>(db + in_bytes + idx_bytes);
     int32_t* dcnt = reinterpret_cast<int32_t*>(db + in_bytes + idx_bytes + fld_bytes);
-    CUDA_TRY(launch_rows(e->d_out.as<double>(), (int64_t)nc * P, nc, P, e->args[0].period,
-                         e->args[0].freq, dsep, dtol, n_best, harmonic_max, dcnt, didx, dfld, st),
+    CUDA_TRY(launch_rows(e->d_out.as<double>(), e->spec_total, nc, e->d_spec_off, e->d_grid_base,
+                         P, e->args[0].freq, dsep, dtol, n_best, harmonic_max, dcnt, didx, dfld,
+                         st),
              "peak search launch");
     CUDA_TRY(cudaMemcpyAsync(hb + in_bytes, db + in_bytes, out_bytes, cudaMemcpyDeviceToHost, st),
              "download rows");
@@ -1608,7 +1759,7 @@ int bls_launch_best_noalloc(BlsEngine* e, int64_t* best_index, double* best_powe
     double* dv = reinterpret_cast<double*>(di + kStaticMaxCurves);
     double* dmean = dv + kStaticMaxCurves;
     double* dstd = dmean + kStaticMaxCurves;
-    CUDA_TRY(launch_best(e->d_out.as<double>(), nc, e->n_periods, di, dv, dmean, dstd, st),
+    CUDA_TRY(launch_best(e->d_out.as<double>(), nc, e->d_spec_off, di, dv, dmean, dstd, st),
              "best-of-spectrum launch");
     // copies into the caller's (pageable) arrays complete before they return
     int32_t flag = 0;
@@ -1707,7 +1858,7 @@ int bls_debug_prefix(BlsEngine* e, const double* t, const double* y, const doubl
     const int64_t offs[2] = {0, n};
     BlsCurves c{1, offs, t, y, dy};
     int rc;
-    if ((rc = do_prepare(e, &g, &c, e->stream))) return rc;
+    if ((rc = do_prepare(e, &g, 1, nullptr, &c, e->stream))) return rc;
     int mode = 0;
     while (mode < kModes - 1 && e->args[mode].n_items <= 0) ++mode;
     int32_t hl = 0;

@@ -401,20 +401,34 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
         const int it = s.next;
         if (it >= a.n_items) break;
         if (tid == 0) {
-            const int r = it / a.tiles_per_curve;
-            const int j = it - r * a.tiles_per_curve;
-            int lo = 0, hi = a.n_segments;          // seg_tiles[lo] <= j < seg_tiles[hi]
+            // one grid: the group is a launch parameter; several: a search
+            WorkGroup gr = a.group0;
+            if (a.n_groups > 1) {
+                int glo = 0, ghi = a.n_groups;      // groups[glo].item_begin <= it
+                while (ghi - glo > 1) {
+                    const int mid = (glo + ghi) >> 1;
+                    if (__ldg(&a.groups[mid].item_begin) <= it) glo = mid;
+                    else ghi = mid;
+                }
+                gr = a.groups[glo];
+            }
+            const int local = it - gr.item_begin;
+            const int r = local / gr.tiles_per_curve;
+            const int j = local - r * gr.tiles_per_curve;
+            const int32_t* tiles = a.seg_tiles + gr.tiles_begin;
+            int lo = 0, hi = gr.n_segments;         // tiles[lo] <= j < tiles[hi]
             while (hi - lo > 1) {
                 const int mid = (lo + hi) >> 1;
-                if (__ldg(a.seg_tiles + mid) <= j) lo = mid;
+                if (__ldg(tiles + mid) <= j) lo = mid;
                 else hi = mid;
             }
-            const int cap = __ldg(a.seg_cap + lo);
-            s.seg = a.segments[lo];
+            const int sg = gr.seg_begin + lo;
+            const int cap = __ldg(a.seg_cap + sg);
+            s.seg = a.segments[sg];
             WorkItem w;
-            w.curve = __ldg(a.order + r);
-            w.segment = lo;
-            w.p_begin = (j - __ldg(a.seg_tiles + lo)) * cap;
+            w.curve = __ldg(a.order + gr.order_begin + r);
+            w.segment = sg;
+            w.p_begin = (j - __ldg(tiles + lo)) * cap;
             w.p_count = min(cap, s.seg.n_periods - w.p_begin);
             s.item = w;
             s.curve = a.curves[w.curve];
@@ -1076,8 +1090,8 @@ __device__ __forceinline__ long long cand_pos(long long j, long long P) {
 }
 
 __global__ void __launch_bounds__(kThreads) rows_kernel(
-    const double* __restrict__ out, int64_t out_stride, int64_t P,
-    const double* __restrict__ period, const double* __restrict__ freq,
+    const double* __restrict__ out, int64_t out_stride, const int64_t* __restrict__ spec_off,
+    const int64_t* __restrict__ grid_base, const double* __restrict__ freq_all,
     const double* __restrict__ sep_c,
     const double* __restrict__ tol_c, int n_best, int hmax, int32_t* n_peaks,
     int64_t* index, double* fields) {
@@ -1091,8 +1105,15 @@ __global__ void __launch_bounds__(kThreads) rows_kernel(
     __shared__ AliasRound s_alias;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int c = blockIdx.x;
-    const double* pw = out + (int64_t)c * P;             // field 0 (power) of curve c
+    const int64_t so = spec_off[c];
+    const int64_t P = spec_off[c + 1] - so;              // curve c's trial periods
+    const double* pw = out + so;                         // field 0 (power) of curve c
+    const double* freq = freq_all + grid_base[c];        // its grid's RN(1/P)
     const int64_t nw = (P + 31) / 32;
+    if (P < 1) {
+        if (tid == 0) n_peaks[c] = 0;
+        return;
+    }
     const double sep = sep_c[c], tol = tol_c[c];
     double offs[5];
     offs[0] = 1.0027379;                                 // sidereal day, cycles/day
@@ -1187,10 +1208,10 @@ __global__ void __launch_bounds__(kThreads) rows_kernel(
                 fo[0] = __ddiv_rn(1.0, f);                          // period = 1 / frequency
                 fo[1] = f;
                 fo[2] = v;                                          // power
-                fo[3] = out[1 * out_stride + (int64_t)c * P + bj];  // depth
-                fo[4] = out[3 * out_stride + (int64_t)c * P + bj];  // depth_snr
-                fo[5] = out[4 * out_stride + (int64_t)c * P + bj];  // duration
-                fo[6] = out[5 * out_stride + (int64_t)c * P + bj];  // t0
+                fo[3] = out[1 * out_stride + so + bj];              // depth
+                fo[4] = out[3 * out_stride + so + bj];              // depth_snr
+                fo[5] = out[4 * out_stride + so + bj];              // duration
+                fo[6] = out[5 * out_stride + so + bj];              // t0
                 fo[7] = s_std > 0.0 ? (v - s_mean) / s_std : 0.0;  // sde
                 index[(int64_t)c * n_best + r] = bj;
             }
@@ -1243,13 +1264,14 @@ __global__ void fold_bins_kernel(const double* tau, int n, double P, double f, u
 // Per curve: the largest power (non-finite values count as 0, as the
 // reference's assembly does before its SDE and peak search) with its first
 // index, and the mean and population standard deviation of that power.
-__global__ void best_kernel(const double* power, int64_t n_periods, int64_t* best_index,
+__global__ void best_kernel(const double* power, const int64_t* spec_off, int64_t* best_index,
                             double* best_power, double* mean_out, double* std_out) {
     __shared__ double red_s[kWarps];
     __shared__ double red_v[kWarps];
     __shared__ long long red_i[kWarps];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const double* p = power + (int64_t)blockIdx.x * n_periods;
+    const double* p = power + spec_off[blockIdx.x];
+    const int64_t n_periods = spec_off[blockIdx.x + 1] - spec_off[blockIdx.x];
     double sum = 0.0, bv = -CUDART_INF;
     long long bi = -1;
     for (int64_t i = tid; i < n_periods; i += kThreads) {
@@ -1334,24 +1356,26 @@ cudaError_t launch_search(const BatchArgs& args, int mode, int n_ctas, size_t sm
     return cudaGetLastError();
 }
 
-cudaError_t launch_best(const double* power, int n_curves, int64_t n_periods, int64_t* best_index,
-                        double* best_power, double* mean, double* sd, cudaStream_t stream) {
+cudaError_t launch_best(const double* power, int n_curves, const int64_t* spec_off,
+                        int64_t* best_index, double* best_power, double* mean, double* sd,
+                        cudaStream_t stream) {
     if (n_curves <= 0) return cudaSuccess;
-    best_kernel<<<n_curves, kThreads, 0, stream>>>(power, n_periods, best_index, best_power, mean,
+    best_kernel<<<n_curves, kThreads, 0, stream>>>(power, spec_off, best_index, best_power, mean,
                                                    sd);
     return cudaGetLastError();
 }
 
-cudaError_t launch_rows(const double* out, int64_t out_stride, int n_curves, int64_t n_periods,
-                        const double* period, const double* freq, const double* sep,
-                        const double* tol, int n_best, int harmonic_max, int32_t* n_peaks,
-                        int64_t* index, double* fields, cudaStream_t stream) {
+cudaError_t launch_rows(const double* out, int64_t out_stride, int n_curves,
+                        const int64_t* spec_off, const int64_t* grid_base, int64_t max_periods,
+                        const double* freq, const double* sep, const double* tol, int n_best,
+                        int harmonic_max, int32_t* n_peaks, int64_t* index, double* fields,
+                        cudaStream_t stream) {
     if (n_curves <= 0) return cudaSuccess;
-    const size_t smem = sizeof(uint32_t) * (size_t)((n_periods + 31) / 32);
+    const size_t smem = sizeof(uint32_t) * (size_t)((max_periods + 31) / 32);
     cudaError_t e = cudaFuncSetAttribute(rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    rows_kernel<<<n_curves, kThreads, smem, stream>>>(out, out_stride, n_periods, period, freq,
+    rows_kernel<<<n_curves, kThreads, smem, stream>>>(out, out_stride, spec_off, grid_base, freq,
                                                       sep, tol, n_best, harmonic_max, n_peaks,
                                                       index, fields);
     return cudaGetLastError();

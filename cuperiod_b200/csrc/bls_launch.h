@@ -22,8 +22,10 @@ cudaError_t launch_fold_bins(const double* tau, int n, double P, double f, uint3
                              int32_t* out, int32_t* used_fast, cudaStream_t stream);
 
 // Per-curve largest power, its index, and the power's mean and standard deviation.
-cudaError_t launch_best(const double* power, int n_curves, int64_t n_periods, int64_t* best_index,
-                        double* best_power, double* mean, double* sd, cudaStream_t stream);
+// Curve c's spectrum is power[spec_off[c] .. spec_off[c + 1]).
+cudaError_t launch_best(const double* power, int n_curves, const int64_t* spec_off,
+                        int64_t* best_index, double* best_power, double* mean, double* sd,
+                        cudaStream_t stream);
 
 // Scratch of the allocation-free search (bls_launch_best_noalloc): one
 // file-scope device array per device.  Bytes [0, 64): the work counters of the
@@ -41,11 +43,14 @@ cudaError_t static_scratch_address(int device, void** ptr);
 
 // Per-curve result rows: the up to n_best alias-diverse peaks of each curve's
 // spectrum (grid index and 8 fields each: period, frequency, power, depth,
-// depth_snr, duration, t0, sde) and their count.
-cudaError_t launch_rows(const double* out, int64_t out_stride, int n_curves, int64_t n_periods,
-                        const double* period, const double* freq, const double* sep,
-                        const double* tol, int n_best, int harmonic_max, int32_t* n_peaks,
-                        int64_t* index, double* fields, cudaStream_t stream);
+// depth_snr, duration, t0, sde) and their count.  Curve c's spectrum is
+// [spec_off[c], spec_off[c + 1]) of each field; its grid's frequencies start at
+// freq[grid_base[c]]; max_periods bounds every curve's spectrum length.
+cudaError_t launch_rows(const double* out, int64_t out_stride, int n_curves,
+                        const int64_t* spec_off, const int64_t* grid_base, int64_t max_periods,
+                        const double* freq, const double* sep, const double* tol, int n_best,
+                        int harmonic_max, int32_t* n_peaks, int64_t* index, double* fields,
+                        cudaStream_t stream);
 
 // Bytes of one period's histogram in the kernel's layout.
 size_t period_hist_bytes(int mode, int hl);

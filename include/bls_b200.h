@@ -106,7 +106,7 @@ typedef struct {
 typedef struct {
     int32_t n_curves;
     int32_t n_segments;
-    int64_t n_periods;            /* periods per curve */
+    int64_t n_periods;            /* periods per curve (the most, with several grids) */
     int64_t n_items;              /* work items of one launch */
     int64_t n_points;             /* points over all curves */
     double folds;                 /* point-period folds per launch */
@@ -117,6 +117,9 @@ typedef struct {
     int32_t smem_per_cta;
     int32_t uniform_curves;       /* curves on the one-weight fast path */
     int32_t fast_fold_segments;   /* segments whose fold runs the fast path */
+    int64_t spectrum;             /* output entries per field: the curves' periods summed */
+    int32_t n_grids;              /* trial grids of the batch (bls_prepare_grids) */
+    int32_t reserved;
 } BlsBatchInfo;
 
 int bls_engine_create(const BlsTune* tune, BlsEngine** engine);
@@ -126,6 +129,18 @@ const char* bls_last_error(void);
 /* Pack and upload a batch (host preparation runs on all host cores).  `stream`
  * is a cudaStream_t; NULL selects the engine's own stream. */
 int bls_prepare(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* curves, void* stream);
+
+/* No counterpart in the reference, whose batch runner searches each curve over
+ * its own default grid in a launch of its own (batch/runner.py:187-250 ->
+ * methods/bls.py:361-395).  bls_prepare for a batch whose curves have different
+ * grids: curve c is searched over grids[grid_of_curve[c]], every curve of the
+ * batch in one launch.  The grids share oversample and objective.  Outputs are
+ * field-major with each curve's spectrum in turn: field f of curve c at grid
+ * index p is out[f * S + spec(c) + p], S = BlsBatchInfo.spectrum and spec(c) the
+ * summed period counts of the grids of curves 0..c-1; bls_download_best and
+ * bls_download_rows index each curve's own grid. */
+int bls_prepare_grids(BlsEngine* engine, int32_t n_grids, const BlsGrid* grids,
+                      const int32_t* grid_of_curve, const BlsCurves* curves, void* stream);
 
 /* Run the search of the prepared batch on the device (no host transfers). */
 int bls_launch(BlsEngine* engine, void* stream);
@@ -138,8 +153,8 @@ int bls_launch(BlsEngine* engine, void* stream);
 int bls_time_launches(BlsEngine* engine, int32_t reps, double* ms_per_launch, void* stream);
 
 /* Copy every field of every curve, field-major: out[f][c][p] with
- * f < BLS_N_FIELDS, c < n_curves, p < n_periods (grid order).  Waits for the
- * stream. */
+ * f < BLS_N_FIELDS, c < n_curves, p < n_periods (grid order); after
+ * bls_prepare_grids, out[f * spectrum + spec(c) + p].  Waits for the stream. */
 int bls_download(BlsEngine* engine, double* out, void* stream);
 
 /* Device address of the output fields (layout as bls_download), valid until the

@@ -36,7 +36,7 @@ def test_struct_layouts_match_the_header():
     assert ctypes.sizeof(_lib.BlsTune) == 20
     assert ctypes.sizeof(_lib.BlsGrid) == 8 + 4 * 8 + 8
     assert ctypes.sizeof(_lib.BlsCurves) == 8 + 4 * 8
-    assert ctypes.sizeof(_lib.BlsBatchInfo) == 4 + 4 + 8 * 3 + 8 * 3 + 8 + 4 * 4
+    assert ctypes.sizeof(_lib.BlsBatchInfo) == 4 + 4 + 8 * 3 + 8 * 3 + 8 + 4 * 4 + 8 + 4 + 4
 
 
 def test_engine_creation_without_a_device_raises():

@@ -116,9 +116,10 @@ def test_device_rows_on_tiny_grids(engine, n_periods):
 
 
 def test_threaded_batch_rows_equal_single_threaded():
-    # curves with distinct baselines get distinct default grids (one launch
-    # each); worker threads with their own engines run those launches
-    # concurrently and must give the rows of a single-threaded run, in order
+    # curves with distinct baselines get distinct default grids; chunks of 5
+    # curves (each chunk one launch over its curves' own grids) run on worker
+    # threads with their own engines and must give the rows of a
+    # single-threaded run, in order
     import numpy as np
 
     from cuperiod_b200.batch import batch_periodograms
@@ -128,11 +129,14 @@ def test_threaded_batch_rows_equal_single_threaded():
     for i, c in enumerate(batched_curves(24, seed=9, n_range=(500, 3000))):
         keep = c.t < c.t.min() + rng.uniform(15.0, 27.0)
         inputs.append((f"c{i}", (c.t[keep], c.y[keep])))
-    one = batch_periodograms(inputs, "BLS", domain="flux", workers=1, n_best=3)
-    many = batch_periodograms(inputs, "BLS", domain="flux", workers=4, n_best=3)
-    assert one.launches == many.launches > 1
+    one = batch_periodograms(inputs, "BLS", domain="flux", workers=1, n_best=3, chunk_size=5)
+    many = batch_periodograms(inputs, "BLS", domain="flux", workers=4, n_best=3, chunk_size=5)
+    assert one.launches == many.launches == 5
     assert [r["key"] for r in many.rows] == [f"c{i}" for i in range(24)]
     assert many.rows == one.rows
+    # and one launch for the whole catalogue gives the same rows
+    whole = batch_periodograms(inputs, "BLS", domain="flux", n_best=3)
+    assert whole.launches == 1 and whole.rows == one.rows
 
 
 def test_threaded_batch_of_stars_and_curves_equals_single_threaded():
