@@ -12,6 +12,7 @@ batch runner uses instead of a per-curve loop.
 
 from __future__ import annotations
 
+import functools
 import math
 from typing import Any, ClassVar, Literal, Sequence
 
@@ -35,12 +36,23 @@ BACKEND_NAME = "b200"
 
 
 def _segment_durations(p_lo: float, settings: BLSSettings) -> np.ndarray:
-    """Box durations of the segment starting at ``p_lo`` (bls.py:39-49)."""
-    d_hi = settings.duration_max_frac * p_lo
-    d_lo = max(settings.duration_min_frac * p_lo, settings.min_duration_days)
-    if d_lo >= d_hi:
-        return np.asarray([d_hi], dtype=np.float64)
-    return np.asarray(np.geomspace(d_lo, d_hi, settings.n_durations), dtype=np.float64)
+    """Box durations of the segment starting at ``p_lo`` (bls.py:39-49), read-only
+    and shared: default grids of every baseline start their segments at the same
+    ``min_period_days * segment_factor**k``, so a catalogue reuses a few arrays."""
+    return _durations(float(p_lo), float(settings.duration_max_frac),
+                      float(settings.duration_min_frac), float(settings.min_duration_days),
+                      int(settings.n_durations))
+
+
+@functools.lru_cache(maxsize=4096)
+def _durations(p_lo: float, max_frac: float, min_frac: float, min_days: float,
+               n: int) -> np.ndarray:
+    d_hi = max_frac * p_lo
+    d_lo = max(min_frac * p_lo, min_days)
+    out = (np.asarray([d_hi], dtype=np.float64) if d_lo >= d_hi
+           else np.asarray(np.geomspace(d_lo, d_hi, n), dtype=np.float64))
+    out.setflags(write=False)
+    return out
 
 
 def _max_period(baseline: float, settings: BLSSettings) -> float:
