@@ -501,8 +501,7 @@ __global__ void __launch_bounds__(kJThreads, 1) joint_kernel(JointArgs a) {
 size_t joint_static_smem() { return sizeof(JointShared); }
 
 cudaError_t configure_joint(size_t smem) {
-    return cudaFuncSetAttribute(joint_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem);
+    return raise_smem_limit((const void*)joint_kernel<true>, smem);
 }
 
 int joint_resident_ctas(bool in_smem, size_t smem) {

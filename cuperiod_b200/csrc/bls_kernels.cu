@@ -33,7 +33,9 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <map>
 #include <mutex>
+#include <utility>
 
 #include "bls_device.h"
 #include "bls_fold.cuh"
@@ -1331,10 +1333,23 @@ const void* search_fn(int mode) {
 }
 }  // namespace
 
+cudaError_t raise_smem_limit(const void* fn, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& have = limit[{dev, fn}];
+    if (smem <= have) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) have = smem;
+    return e;
+}
+
 cudaError_t configure_search(int mode, size_t smem) {
     for (const void* f : {search_fn<0>(mode), search_fn<1>(mode)}) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const cudaError_t e = raise_smem_limit(f, smem);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -1372,8 +1387,7 @@ cudaError_t launch_rows(const double* out, int64_t out_stride, int n_curves,
                         cudaStream_t stream) {
     if (n_curves <= 0) return cudaSuccess;
     const size_t smem = sizeof(uint32_t) * (size_t)((max_periods + 31) / 32);
-    cudaError_t e = cudaFuncSetAttribute(rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = raise_smem_limit((const void*)rows_kernel, smem);
     if (e != cudaSuccess) return e;
     rows_kernel<<<n_curves, kThreads, smem, stream>>>(out, out_stride, spec_off, grid_base, freq,
                                                       sep, tol, n_best, harmonic_max, n_peaks,

@@ -12,6 +12,12 @@ namespace blsb200 {
 // shared memory (called outside any stream capture).
 cudaError_t configure_search(int mode, size_t smem);
 
+// Raise kernel fn's dynamic shared-memory limit on the current device to at
+// least smem bytes.  The limit is process-wide per kernel and device, so it only
+// ever grows (under a lock): a launch from one thread cannot lower it under a
+// concurrent launch from another that needs more.
+cudaError_t raise_smem_limit(const void* fn, size_t smem);
+
 // Persistent search over every work item of the batch in `args`.
 cudaError_t launch_search(const BatchArgs& args, int mode, int n_ctas, size_t smem,
                           cudaStream_t stream);

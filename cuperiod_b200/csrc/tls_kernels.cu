@@ -275,8 +275,7 @@ size_t tls_smem_bytes(int n_bins, int max_width, int tile, int n_tmpl) {
 }
 
 cudaError_t configure_tls(size_t smem) {
-    return cudaFuncSetAttribute(tls_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem);
+    return raise_smem_limit((const void*)tls_kernel, smem);
 }
 
 int tls_resident_ctas(size_t smem) {

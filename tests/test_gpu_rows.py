@@ -162,3 +162,31 @@ def test_threaded_batch_of_stars_and_curves_equals_single_threaded():
     assert len(many.rows) == 7 and many.launches == one.launches
     assert many.errors == one.errors and list(many.errors) == ["short"]
     assert many.rows == one.rows
+
+
+def test_concurrent_launches_with_different_shared_memory_needs():
+    # a launch raises its kernel's dynamic shared-memory limit, which is one
+    # value per kernel and device for the whole process: threads whose batches
+    # need different amounts (the peak ranking's candidate mask grows with the
+    # grid) must never lower it under one another
+    from concurrent.futures import ThreadPoolExecutor
+
+    from cuperiod_b200 import _lib
+    from cuperiod_b200.bls import BLSMethod
+    from cuperiod_b200.grid import GridSpec
+    from cuperiod_b200.settings import BLSSettings
+    s = BLSSettings()
+    keyed = _keyed()[:2]
+    sizes = [60000, 2000, 45000, 3000, 30000, 5000, 20000, 1000] * 3
+
+    def job(n_periods):
+        grid = GridSpec(kind="period", values=np.geomspace(0.5, 12.0, n_periods))
+        return BLSMethod().rows_many(grid, keyed, s, n_best=3, engine=_lib.default_engine())
+
+    with ThreadPoolExecutor(max_workers=4) as pool:
+        results = list(pool.map(job, sizes))
+    assert all(len(r) == 2 and r[0]["key"] == keyed[0][0] for r in results)
+    # the same grid gives the same rows whichever thread ran it
+    for n in set(sizes):
+        runs = [r for r, k in zip(results, sizes) if k == n]
+        assert all(run == runs[0] for run in runs)
