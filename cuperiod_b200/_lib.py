@@ -55,6 +55,14 @@ class BlsTlsInputs(ctypes.Structure):
 TLS_FIELD_NAMES = ("sr", "depth", "duration", "t0")
 
 
+class BlsDefaultGrid(ctypes.Structure):
+    _fields_ = [("min_period_days", _dbl), ("max_period_days", _dbl), ("min_transits", _dbl),
+                ("segment_factor", _dbl), ("grid_duration_frac", _dbl),
+                ("grid_oversample", _dbl), ("n_starts", _i32), ("oversample", _i32),
+                ("objective", _i32), ("reserved", _i32), ("dur_offsets", _vp),
+                ("durations", _vp)]
+
+
 class BlsBatchInfo(ctypes.Structure):
     _fields_ = [("n_curves", _i32), ("n_segments", _i32), ("n_periods", _i64),
                 ("n_items", _i64), ("n_points", _i64), ("folds", _dbl), ("boxes", _dbl),
@@ -97,6 +105,10 @@ def load() -> ctypes.CDLL:
         lib.bls_batch_info.argtypes = [_vp, P(BlsBatchInfo)]
         lib.bls_time_launches.argtypes = [_vp, _i32, P(_dbl), _vp]
         lib.bls_prepare_grids.argtypes = [_vp, _i32, P(BlsGrid), _vp, P(BlsCurves), _vp]
+        lib.bls_default_grid.argtypes = [P(BlsDefaultGrid), _dbl, _i64, _vp, _vp, _vp,
+                                         P(_i32), P(_i64)]
+        lib.bls_default_grid_sizes.argtypes = [P(BlsDefaultGrid), _i32, _vp, _vp]
+        lib.bls_prepare_default.argtypes = [_vp, P(BlsDefaultGrid), _vp, P(BlsCurves), _vp]
         lib.bls_search_joint.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp, _vp]
         lib.bls_tls_search.argtypes = [_vp, P(BlsTlsInputs), _vp, _i64, _vp, _vp]
         lib.bls_tls_prepare.argtypes = [_vp, P(BlsTlsInputs), _vp, _i64, _vp]
@@ -114,7 +126,8 @@ def load() -> ctypes.CDLL:
                      "bls_launch_best_noalloc", "bls_download_rows", "bls_search_joint",
                      "bls_joint_prepare", "bls_joint_launch", "bls_joint_download",
                      "bls_tls_search", "bls_tls_prepare", "bls_tls_launch",
-                     "bls_tls_download", "bls_time_launches", "bls_prepare_grids"):
+                     "bls_tls_download", "bls_time_launches", "bls_prepare_grids",
+                     "bls_default_grid", "bls_default_grid_sizes", "bls_prepare_default"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib
@@ -169,6 +182,58 @@ class PackedGrid:
         return BlsGrid(len(self.seg_offsets) - 1, _addr(self.seg_offsets), _addr(self.periods),
                        _addr(self.dur_offsets), _addr(self.durations), self.oversample,
                        self.objective)
+
+
+@dataclass
+class DefaultGridSpec:
+    """The default-grid parameters in the C ABI's layout (``BlsDefaultGrid``),
+    with the box durations of each segment start (keeps its arrays alive)."""
+    min_period_days: float
+    max_period_days: float
+    min_transits: float
+    segment_factor: float
+    grid_duration_frac: float
+    grid_oversample: float
+    dur_offsets: np.ndarray         # n_starts + 1
+    durations: np.ndarray
+    oversample: int
+    objective: int
+
+    def struct(self) -> BlsDefaultGrid:
+        return BlsDefaultGrid(float(self.min_period_days), float(self.max_period_days),
+                              float(self.min_transits), float(self.segment_factor),
+                              float(self.grid_duration_frac), float(self.grid_oversample),
+                              len(self.dur_offsets) - 1, int(self.oversample),
+                              int(self.objective), 0, _addr(self.dur_offsets),
+                              _addr(self.durations))
+
+
+def default_grid(spec: DefaultGridSpec, baseline: float):
+    """The default grid of one baseline built by the engine library on the host:
+    ``(periods, seg_offsets, seg_start)`` (``bls_default_grid``)."""
+    lib = load()
+    st = spec.struct()
+    ns, npd = _i32(0), _i64(0)
+    _check(lib.bls_default_grid(ctypes.byref(st), float(baseline), 0, None, None, None,
+                                ctypes.byref(ns), ctypes.byref(npd)))
+    periods = np.empty(npd.value, dtype=np.float64)
+    offs = np.empty(ns.value + 1, dtype=np.int64)
+    starts = np.empty(ns.value, dtype=np.int32)
+    _check(lib.bls_default_grid(ctypes.byref(st), float(baseline), periods.size,
+                                periods.ctypes.data, offs.ctypes.data, starts.ctypes.data,
+                                ctypes.byref(ns), ctypes.byref(npd)))
+    return periods, offs, starts
+
+
+def default_grid_sizes(spec: DefaultGridSpec, baselines) -> np.ndarray:
+    """Periods of the default grid of each baseline (-1: none can be built)."""
+    lib = load()
+    b = _f64(baselines).ravel()
+    out = np.empty(b.size, dtype=np.int64)
+    st = spec.struct()
+    _check(lib.bls_default_grid_sizes(ctypes.byref(st), b.size, b.ctypes.data,
+                                      out.ctypes.data))
+    return out
 
 
 @dataclass
@@ -262,6 +327,20 @@ class Engine:
         self._spec_off = np.concatenate([[0], np.cumsum(counts[gids])]).astype(np.int64)
         _check(self._lib.bls_prepare_grids(self._h, len(grids), structs, gids.ctypes.data,
                                            ctypes.byref(c), stream))
+
+    def prepare_default(self, spec: DefaultGridSpec, baselines, curves: PackedCurves,
+                        stream: int | None = None) -> None:
+        """Every curve over the default grid of its baseline, the grids built by
+        the library on the host cores, in one launch (``bls_prepare_default``)."""
+        b = _f64(baselines).ravel()
+        if b.size != curves.n_curves:
+            raise ValueError("one baseline per curve is required")
+        sizes = default_grid_sizes(spec, b)
+        st, c = spec.struct(), curves.struct()
+        self._grid, self._curves = None, curves
+        self._spec_off = np.concatenate([[0], np.cumsum(np.maximum(sizes, 0))]).astype(np.int64)
+        _check(self._lib.bls_prepare_default(self._h, ctypes.byref(st), b.ctypes.data,
+                                             ctypes.byref(c), stream))
 
     @property
     def spectrum_offsets(self) -> np.ndarray:

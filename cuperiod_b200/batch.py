@@ -163,8 +163,8 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                        workers: int | None = None) -> BatchSummary:
     """Search many light curves: BLS searches each chunk of ``chunk_size`` curves
     in one engine launch, every curve over its own grid (the explicit ``grid``,
-    else its default grid; equal grids are shared); other methods launch once per
-    chunk of curves that share a grid.  Multi-band stars are launches of their
+    else its default grid, which the engine library builds on the host cores);
+    other methods launch once per chunk of curves that share a grid.  Multi-band stars are launches of their
     own; their rows come first, then the curves' rows in input order.
 
     ``inputs``: ``(key, data)`` pairs (``data`` a LightCurve, MultiBandLightCurve,
@@ -187,6 +187,8 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
     entries: list[tuple[str, Any, str]] = []        # (key, curve, grid key) in input order
     star_jobs: list[tuple[str, Any, GridSpec]] = []
     fixed_key = _grid_key(grid) if grid is not None else None     # one grid: hash it once
+    # BLS default grids are built by the engine library at launch time
+    native_default = grid is None and hasattr(m, "rows_default")
     for key, data in resolve_inputs(inputs, columns=columns, domain=domain,
                                     band_column=band_column):
         try:
@@ -200,6 +202,9 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                 star_jobs.append((str(key), lc, grid or multiband_default_grid(m, lc, s)))
                 continue
             lc = lc.in_domain(m.natural_domain)
+            if native_default:
+                entries.append((str(key), lc, ""))
+                continue
             g = grid or m.default_grid(lc, s)
         except (CuPeriodError, ValueError, OSError) as exc:
             summary.errors[str(key)] = f"{type(exc).__name__}: {exc}"
@@ -220,7 +225,14 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
         return True
 
     jobs: list[Any] = [("star", job) for job in star_jobs]
-    if hasattr(m, "rows_by_grid"):
+    if native_default:
+        # one launch per chunk of curves in input order, each over its default grid
+        ok_all, failed = m.split_default([(key, lc) for key, lc, _ in entries
+                                          if searchable(key, lc)], s)
+        summary.errors.update(failed)
+        for start in range(0, len(ok_all), chunk_size):
+            jobs.append(("default", ok_all[start:start + chunk_size]))
+    elif hasattr(m, "rows_by_grid"):
         # one launch per chunk of curves in input order, each curve over its own
         # grid (equal grids shared)
         ok_all = [(key, lc, groups[gk][0]) for key, lc, gk in entries if searchable(key, lc)]
@@ -246,6 +258,9 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                 return [], {key: f"{type(exc).__name__}: {exc}"}
             return [periodogram_to_row(key, pg.with_peak_defaults(s), n_best=n_best,
                                        extra_keys=PEAK_EXTRA_COLUMNS, alias_diverse=True)], {}
+        if kind == "default":
+            return m.rows_default(body, s, n_best=n_best, extra_keys=extras,
+                                  engine=job_engine), {}
         if kind == "mixed":
             # peaks ranked on the device: only the rows leave the GPU
             return m.rows_by_grid(body, s, n_best=n_best, extra_keys=extras,

@@ -90,6 +90,36 @@ def _segment_periods(baseline: float, settings: BLSSettings, *, time=None,
     return parts
 
 
+def _default_total(baseline: float, settings: BLSSettings) -> int:
+    """The size the reference checks before building a default grid (bls.py:81-84)."""
+    bounds = _segment_bounds(baseline, settings)
+    if not bounds:
+        return 0
+    df = settings.grid_duration_frac / (settings.grid_oversample * baseline)
+    return sum(max(0, math.ceil((1.0 / p_lo - 1.0 / p_hi) / df)) for p_lo, p_hi in bounds)
+
+
+def default_grid_spec(settings: BLSSettings, max_baseline: float) -> _lib.DefaultGridSpec:
+    """The default grid's parameters for the engine library's host builder, with
+    the box durations of every segment start that a baseline up to
+    ``max_baseline`` reaches (starts min_period_days * segment_factor**k, as
+    _segment_bounds steps them)."""
+    max_period = _max_period(max_baseline, settings)
+    durations = []
+    p_lo = settings.min_period_days
+    while p_lo < max_period:
+        durations.append(_segment_durations(p_lo, settings))
+        p_lo = p_lo * settings.segment_factor
+    offsets = np.zeros(len(durations) + 1, dtype=np.int64)
+    offsets[1:] = np.cumsum([d.size for d in durations]) if durations else []
+    return _lib.DefaultGridSpec(
+        settings.min_period_days, settings.max_period_days, settings.min_transits,
+        settings.segment_factor, settings.grid_duration_frac, settings.grid_oversample,
+        offsets, np.ascontiguousarray(np.concatenate(durations) if durations else np.empty(0),
+                                      dtype=np.float64),
+        settings.bins_per_duration, _objective_flag(settings.objective))
+
+
 def _segment_grids(baseline: float, settings: BLSSettings, *, time=None,
                    context: str = "BLS default grid") -> list[Segment]:
     """``[(periods, durations), ...]`` of the default grid (bls.py:108-125)."""
@@ -313,6 +343,75 @@ class BLSMethod:
                 rows[i] = self._row(items[i][0], prepared[i][0], int(n_peaks[j]), fields[j],
                                     n_best, extra_keys)
         return rows  # type: ignore[return-value]
+
+    def split_default(self, keyed: Sequence[tuple[str, LightCurve]], settings: BLSSettings
+                      ) -> tuple[list[tuple[str, LightCurve]], dict[str, str]]:
+        """The curves whose default grid can be searched, and the failure of each
+        other curve as ``default_grid`` would raise it (the grid-size guard,
+        GridTooLargeError, or an empty grid, InsufficientDataError), without
+        building the grids in Python."""
+        from .errors import CuPeriodError
+        good: list[tuple[str, LightCurve]] = []
+        errors: dict[str, str] = {}
+        base: list[float] = []
+        for key, lc in keyed:
+            finite = lc.finite()
+            try:
+                check_grid_size(_default_total(finite.baseline, settings), automatic=True,
+                                time=finite.time, baseline=finite.baseline,
+                                context="BLS default grid")
+            except (CuPeriodError, ValueError) as exc:
+                errors[key] = f"{type(exc).__name__}: {exc}"
+                continue
+            good.append((key, lc))
+            base.append(finite.baseline)
+        if not good:
+            return good, errors
+        spec = default_grid_spec(settings, max(base))
+        sizes = _lib.default_grid_sizes(spec, np.asarray(base))
+        kept = []
+        for (key, lc), n in zip(good, sizes):
+            if n > 0:
+                kept.append((key, lc))
+            else:
+                errors[key] = ("InsufficientDataError: BLS: baseline too short for the "
+                               "configured period range")
+        return kept, errors
+
+    def rows_default(self, keyed: Sequence[tuple[str, LightCurve]], settings: BLSSettings, *,
+                     n_best: int = 10, extra_keys: Sequence[str] = (),
+                     engine: _lib.Engine | None = None) -> list[dict]:
+        """``rows_by_grid`` with every curve over its own default grid
+        (``default_grid``), the grids built by the engine library on the host
+        cores (``bls_prepare_default``) instead of as one GridSpec per curve:
+        the same trial periods bit for bit, the same rows.  The curves must pass
+        ``split_default``."""
+        count = max(int(n_best), 1)
+        if count > 1024:
+            return self.rows_by_grid([(key, lc, self.default_grid(lc, settings))
+                                      for key, lc in keyed], settings, n_best=n_best,
+                                     extra_keys=extra_keys, engine=engine)
+        from .result import DEFAULT_HARMONIC_MAX, DEFAULT_SEPARATION_RAYLEIGH
+        from .settings import peak_defaults
+        prepared = [_prepared_curve(lc, settings) for _, lc in keyed]
+        if not prepared:
+            return []
+        baselines = np.array([f.baseline for f, _ in prepared], dtype=np.float64)
+        spec = default_grid_spec(settings, float(baselines.max()))
+        eng = engine or _lib.default_engine()
+        eng.prepare_default(spec, baselines, _lib.PackedCurves.from_arrays(
+            [(f.time, f.value, e) for f, e in prepared]))
+        eng.launch()
+        d = peak_defaults(settings)
+        sep_r = float(d.get("min_separation_rayleigh", DEFAULT_SEPARATION_RAYLEIGH))
+        order = int(d.get("harmonic_max", DEFAULT_HARMONIC_MAX))
+        tol_set = d.get("alias_tolerance")
+        sep = np.maximum(sep_r / baselines, 1e-12)
+        tol = np.maximum(np.full(baselines.size, float(tol_set)) if tol_set is not None
+                         else np.minimum(sep_r / baselines, 1.0 / baselines), 1e-12)
+        n_peaks, _, fields = eng.rows(count, order, sep, tol)
+        return [self._row(key, f, int(n_peaks[j]), fields[j], n_best, extra_keys)
+                for j, ((key, _), (f, _)) in enumerate(zip(keyed, prepared))]
 
     def _row(self, key: str, f: LightCurve, k_have: int, fields: np.ndarray, n_best: int,
              extra_keys: Sequence[str]) -> dict:

@@ -20,10 +20,12 @@
 #include <cstring>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/bls_b200.h"
 #include "bls_device.h"
+#include "bls_grid.h"
 #include "bls_launch.h"
 
 using namespace blsb200;
@@ -1564,6 +1566,87 @@ int bls_prepare_grids(BlsEngine* e, int32_t n_grids, const BlsGrid* grids,
         return fail(BLS_E_INVALID, "grid_of_curve is required with more than one grid");
     cudaSetDevice(e->device);
     return do_prepare(e, grids, n_grids, grid_of_curve, curves, pick(e, stream));
+}
+
+int bls_default_grid(const BlsDefaultGrid* spec, double baseline, int64_t capacity,
+                     double* periods, int64_t* seg_offsets, int32_t* seg_start,
+                     int32_t* n_segments, int64_t* n_periods) {
+    if (!spec || !n_segments || !n_periods) return fail(BLS_E_INVALID, "bad arguments");
+    DefaultGrid g;
+    std::string err;
+    const int rc = build_default_grid(*spec, baseline, g, err);
+    if (rc) return fail(rc, "%s", err.c_str());
+    *n_segments = (int32_t)g.seg_start.size();
+    *n_periods = (int64_t)g.periods.size();
+    if (!periods) return BLS_OK;
+    if (!seg_offsets || !seg_start || capacity < *n_periods)
+        return fail(BLS_E_INVALID, "the default grid needs %lld periods", (long long)*n_periods);
+    std::copy(g.periods.begin(), g.periods.end(), periods);
+    std::copy(g.seg_offsets.begin(), g.seg_offsets.end(), seg_offsets);
+    std::copy(g.seg_start.begin(), g.seg_start.end(), seg_start);
+    return BLS_OK;
+}
+
+int bls_default_grid_sizes(const BlsDefaultGrid* spec, int32_t n, const double* baselines,
+                           int64_t* n_periods) {
+    if (!spec || n < 0 || (n > 0 && (!baselines || !n_periods)))
+        return fail(BLS_E_INVALID, "bad arguments");
+    parallel_for(n, [&](int i, int) { n_periods[i] = default_grid_size(*spec, baselines[i]); });
+    return BLS_OK;
+}
+
+int bls_prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* baselines,
+                        const BlsCurves* cv, void* stream) {
+    if (!e) return fail(BLS_E_INVALID, "engine is NULL");
+    if (!spec || !baselines || !cv || cv->n_curves < 1)
+        return fail(BLS_E_INVALID, "spec, baselines and curves are required");
+    if (spec->n_starts < 0 || (spec->n_starts > 0 && (!spec->dur_offsets || !spec->durations)))
+        return fail(BLS_E_INVALID, "bad duration table");
+    const int nc = cv->n_curves;
+    // one grid per distinct baseline (bit pattern)
+    std::unordered_map<uint64_t, int32_t> slot;
+    std::vector<double> uniq;
+    std::vector<int32_t> gid(nc);
+    for (int c = 0; c < nc; ++c) {
+        uint64_t bits;
+        std::memcpy(&bits, baselines + c, sizeof bits);
+        auto it = slot.emplace(bits, (int32_t)uniq.size());
+        if (it.second) uniq.push_back(baselines[c]);
+        gid[c] = it.first->second;
+    }
+    const int ng = (int)uniq.size();
+    std::vector<DefaultGrid> built(ng);
+    std::vector<int> codes(ng, BLS_OK);
+    std::vector<std::string> msgs(ng);
+    parallel_for(ng, [&](int k, int) { codes[k] = build_default_grid(*spec, uniq[k], built[k], msgs[k]); });
+    std::vector<std::vector<int64_t>> dur_off(ng);
+    std::vector<std::vector<double>> dur(ng);
+    std::vector<BlsGrid> grids(ng);
+    for (int k = 0; k < ng; ++k) {
+        if (codes[k]) return fail(codes[k], "baseline %.9g: %s", uniq[k], msgs[k].c_str());
+        const DefaultGrid& g = built[k];
+        if (g.periods.empty())
+            return fail(BLS_E_INVALID,
+                        "BLS: the default grid of a %.6g-day baseline is empty (baseline too "
+                        "short for the configured period range)", uniq[k]);
+        dur_off[k].assign(1, 0);
+        for (int32_t st : g.seg_start) {
+            const int64_t d0 = spec->dur_offsets[st], d1 = spec->dur_offsets[st + 1];
+            if (d1 < d0) return fail(BLS_E_INVALID, "bad duration table");
+            dur[k].insert(dur[k].end(), spec->durations + d0, spec->durations + d1);
+            dur_off[k].push_back((int64_t)dur[k].size());
+        }
+        BlsGrid& bg = grids[k];
+        bg.n_segments = (int32_t)g.seg_start.size();
+        bg.seg_offsets = g.seg_offsets.data();
+        bg.periods = g.periods.data();
+        bg.dur_offsets = dur_off[k].data();
+        bg.durations = dur[k].data();
+        bg.oversample = spec->oversample;
+        bg.objective = spec->objective;
+    }
+    cudaSetDevice(e->device);
+    return do_prepare(e, grids.data(), ng, gid.data(), cv, pick(e, stream));
 }
 
 int bls_launch(BlsEngine* e, void* stream) {

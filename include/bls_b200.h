@@ -142,6 +142,52 @@ int bls_prepare(BlsEngine* engine, const BlsGrid* grid, const BlsCurves* curves,
 int bls_prepare_grids(BlsEngine* engine, int32_t n_grids, const BlsGrid* grids,
                       const int32_t* grid_of_curve, const BlsCurves* curves, void* stream);
 
+/* The reference's default trial grid (BLSMethod.default_grid, methods/bls.py:
+ * 52-125 and 327-359) of a baseline: log segments [p_lo, p_hi) from
+ * min_period_days, segment_factor wide, capped at min(max_period_days,
+ * baseline / min_transits); each uniform in frequency with step
+ * grid_duration_frac / (grid_oversample * baseline) as numpy's
+ * arange(1/p_hi, 1/p_lo, step) trimmed below 1/p_lo, periods = 1/frequency
+ * ascending; empty segments dropped.  Segment starts are min_period_days *
+ * segment_factor^k (k = 0, 1, ...); the segment starting at start k searches
+ * durations[dur_offsets[k] .. dur_offsets[k + 1]) (the reference's
+ * _segment_durations of that start, which the caller computes). */
+typedef struct {
+    double min_period_days;
+    double max_period_days;
+    double min_transits;
+    double segment_factor;
+    double grid_duration_frac;
+    double grid_oversample;
+    int32_t n_starts;             /* segment starts covered by the duration table */
+    int32_t oversample;           /* phase bins per shortest duration */
+    int32_t objective;            /* 0 = depth SNR, 1 = log-likelihood */
+    int32_t reserved;
+    const int64_t* dur_offsets;   /* n_starts + 1 */
+    const double* durations;
+} BlsDefaultGrid;
+
+/* No counterpart in the reference's ABI.  The default grid of one baseline on
+ * the host: with periods == NULL only *n_segments and *n_periods are set;
+ * otherwise periods (capacity entries), the segment offsets (n_segments + 1)
+ * and each segment's start index k are written.  BLS_E_INVALID when capacity
+ * is too small or the baseline is not positive. */
+int bls_default_grid(const BlsDefaultGrid* spec, double baseline, int64_t capacity,
+                     double* periods, int64_t* seg_offsets, int32_t* seg_start,
+                     int32_t* n_segments, int64_t* n_periods);
+
+/* Periods of the default grid of each of n baselines (-1 where none can be
+ * built), on all host cores. */
+int bls_default_grid_sizes(const BlsDefaultGrid* spec, int32_t n, const double* baselines,
+                           int64_t* n_periods);
+
+/* bls_prepare_grids with every curve over the default grid of its baseline
+ * (baselines[c], the span of its finite times): the grids are built on the host
+ * cores, one per distinct baseline, and the batch searched in one launch.
+ * A curve whose default grid is empty is refused (BLS_E_INVALID). */
+int bls_prepare_default(BlsEngine* engine, const BlsDefaultGrid* spec, const double* baselines,
+                        const BlsCurves* curves, void* stream);
+
 /* Run the search of the prepared batch on the device (no host transfers). */
 int bls_launch(BlsEngine* engine, void* stream);
 

@@ -96,3 +96,46 @@ def test_rows_by_grid_equal_rows_of_each_grid():
     each = [m.rows_many(g, [(key, lc)], s, n_best=4)[0] for key, lc, g in triples]
     assert [r["key"] for r in together] == [f"k{i}" for i in range(5)]
     assert together == each
+
+
+def _same_rows(a, b, loose=()):
+    """Rows equal field by field (NaN equal to NaN); for the keys in ``loose``
+    (FP64 sums in atomic order) floats within 1e-9 relative."""
+    assert len(a) == len(b)
+    for x, y in zip(a, b):
+        assert x.keys() == y.keys()
+        for k in x:
+            vx, vy = x[k], y[k]
+            if isinstance(vx, float) and isinstance(vy, float):
+                if vx != vx and vy != vy:
+                    continue
+                if x["key"] in loose:
+                    assert abs(vx - vy) <= 1e-9 * max(abs(vx), abs(vy)), (x["key"], k, vx, vy)
+                    continue
+            assert vx == vy, (x["key"], k, vx, vy)
+
+
+def test_native_default_grids_give_the_rows_of_python_default_grids():
+    from cuperiod_b200.batch import batch_periodograms
+    from cuperiod_b200.bls import BLSMethod
+    from cuperiod_b200.lightcurve import Domain, LightCurve
+    from cuperiod_b200.settings import BLSSettings
+    m = BLSMethod()
+    keyed = []
+    for i, (n, span, w, seed) in enumerate([(900, 8.5, "uniform", 31), (1500, 13.2, "hetero", 32),
+                                            (2400, 27.0, "uniform", 33), (700, 8.5, "wild", 34),
+                                            (400, 5.1, "uniform", 35), (3000, 44.0, "hetero", 36)]):
+        t, y, dy = transit_curve(n, span=span, weights=w, seed=seed, period=1.7)
+        keyed.append((f"d{i}", LightCurve(t, y, dy, Domain.FLUX)))
+    for s in (BLSSettings(), BLSSettings(objective="likelihood", grid_oversample=3)):
+        native = m.rows_default(keyed, s, n_best=12)
+        python = m.rows_by_grid([(k, lc, m.default_grid(lc, s)) for k, lc in keyed], s,
+                                n_best=12)
+        _same_rows(native, python, loose=("d3",))   # d3: weights over four decades
+    # the batch runner takes the native path and records the same failures
+    short = ("short", LightCurve(np.linspace(0.0, 0.3, 40), np.ones(40), None, Domain.FLUX))
+    res = batch_periodograms(keyed + [short], "BLS", n_best=12)
+    assert res.launches == 1 and list(res.errors) == ["short"]
+    from cuperiod_b200.batch import PEAK_EXTRA_COLUMNS
+    _same_rows(res.rows, m.rows_default(keyed, BLSSettings(), n_best=12,
+                                        extra_keys=PEAK_EXTRA_COLUMNS), loose=("d3",))
