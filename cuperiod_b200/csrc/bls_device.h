@@ -11,8 +11,9 @@
 namespace blsb200 {
 
 // Accumulation modes.  Every sum is an exact integer built from native 32-bit
-// shared atomics: a point's quantised value v (|v| <= 2^24) is added as its
-// unsigned low 13 bits to one word and its signed high part to another, so a
+// shared atomics: a point's quantised value v (|v| <= 2^bits, bits =
+// min(27, 41 - ceil(log2 n)) for a curve of n points, at least 24) is added as
+// its unsigned low 13 bits to one word and its signed high part to another, so a
 // bin's sum is (signed) B * 2^13 + A with no carry lost for up to 2^17 points.
 //  UNIFORM: every point has the same inverse variance w: r_q (the quantised
 //           centred flux * weight) and a count per bin (three atomics).

@@ -260,7 +260,7 @@ cudaStream_t pick(BlsEngine* e, void* s) {
     return s ? static_cast<cudaStream_t>(s) : e->stream;
 }
 
-// One quantised value (|v| <= 2^24) as the kernel adds it: the unsigned low 13
+// One quantised value (|v| <= 2^27) as the kernel adds it: the unsigned low 13
 // bits in the low half-word, the signed high part in the high half-word.
 inline uint32_t split_word(long long v) {
     const uint32_t lo = (uint32_t)(v & ((1 << kHalfBits) - 1));
@@ -352,11 +352,18 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
         max_r = std::max(max_r, std::fabs(r[j]));
         max_i = std::max(max_i, iv[j]);
     }
+    // r_q = r * 2^e_r with |r_q| <= 2^bits: bits = min(27, 41 - ceil(log2 n)), so
+    // the signed high part (r_q >> 13, 16 bits in the payload word) fits and the
+    // high-part word's prefix sums, doubled at most by the wrap pad, stay below
+    // 2^31 (n * 2^(bits - 12) <= 2^29); at least 24 bits up to 2^17 points
+    int m = 0;
+    while (m < 62 && ((int64_t)1 << m) < n) ++m;
+    const int bits = std::min(27, 41 - m);
     int k = 0;
     int e_r = 0;
     if (max_r > 0.0 && std::isfinite(max_r)) {
         std::frexp(max_r, &k);             // max_r < 2^k
-        e_r = 24 - k;                      // |r_q| <= 2^24
+        e_r = bits - k;                    // |r_q| <= 2^bits
     }
     for (int64_t j = 0; j < n; ++j)
         pay_r[point_slot(j, n)] = split_word(std::llrint(std::ldexp(r[j], e_r)));

@@ -13,8 +13,9 @@
 //      runs.  With one weight for every point the bin sums are exact integers
 //      built with native 32-bit shared atomics only (64-bit and floating-point
 //      shared atomics are emulated on sm_100): each point adds the unsigned low
-//      13 bits and the signed high part of r_q (its quantised centred
-//      flux*weight) to two words and 1 to the bin's count.  With per-point
+//      13 bits and the signed high part of r_q (its centred flux*weight
+//      quantised to 24-27 bits of the curve's largest, by its length) to two
+//      words and 1 to the bin's count.  With per-point
 //      weights the two sums stay FP64.  A lane holds 8 time-consecutive points
 //      (the lanes of a warp 8 points apart, so their bins rarely collide);
 //   2. per period: applies the reference's wrap pad (_bls_core.py:377-381),

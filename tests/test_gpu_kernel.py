@@ -125,7 +125,8 @@ def test_padded_prefix_sums_match_oracle(engine, weights, period):
     med = np.median(y)
     ivar = 1.0 / dy**2
     r = (y - med) * ivar - ivar * (np.sum((y - med) * ivar) / ivar.sum())
-    # one weight: r quantised to 2^-24 of max|r| per point; weights within 2^8 of
+    # one weight: r quantised to at most 2^-24 of max|r| per point (finer for
+    # curves below 2^17 points); weights within 2^8 of
     # each other: r and ivar quantised to 2^-38 of their largest; wider: FP64
     uniform = np.all(dy == dy[0])
     wide = not uniform and ivar.max() <= 256.0 * ivar.min()
