@@ -43,6 +43,9 @@ METRIC = "BLS light curves/s on 1 B200: plain vs learned-pruned at ≥99% same-b
 UNIT = "light curves/s"
 WORKLOAD = ("batched plain full-grid BLS: 4096 curves, N~U[500,20000], 27 d at 2-min cadence, "
             "50,000 log periods 0.3-13 d, 8 durations/segment, snr objective")
+LB_WORKLOAD = ("long-baseline precision stress BLS: {n} curves of 60,000 points at 30-min cadence "
+               "over 1461 d (times offset 1.4e3 d, FP32 flux, depths 5e-5-1e-2), 200,000 log "
+               "periods 0.5-400 d, 12 durations/segment, snr objective")
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one search launch
 # over the first 256 curves of this workload, from one ncu capture
 # (profiles/bls_search_kernel_launches_256curves.txt); a launch's traffic grows in
@@ -63,10 +66,17 @@ def parse_args():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target duration of the CPU-baseline sample")
-    p.add_argument("--workload", choices=("batch", "multiband-shared", "tls"), default="batch",
-                   help="batch: the headline batched search; multiband-shared: the "
-                        "joint-ephemeris multi-band search of --stars six-band stars; tls: "
-                        "the transit least squares search of --tls-curves curves")
+    p.add_argument("--lb-curves", type=int, default=512,
+                   help="long-baseline: light curves per rank")
+    p.add_argument("--lb-check", type=int, default=2,
+                   help="long-baseline: curves checked against the oracle (rank 0)")
+    p.add_argument("--workload", choices=("batch", "long-baseline", "multiband-shared", "tls"),
+                   default="batch",
+                   help="batch: the headline batched search; long-baseline: the 4-year "
+                        "precision stress search of --lb-curves curves with an oracle check; "
+                        "multiband-shared: the joint-ephemeris multi-band search of --stars "
+                        "six-band stars; tls: the transit least squares search of "
+                        "--tls-curves curves")
     p.add_argument("--tls-curves", type=int, default=32, help="tls: light curves per rank")
     p.add_argument("--tile", choices=("auto", "default"), default="auto",
                    help="batch: tile shape from the autotuner (timed on a 128-curve sample "
@@ -127,16 +137,23 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def workload(n_curves: int, seed: int):
+def workload(n_curves: int, seed: int, kind: str = "batch"):
     from cuperiod_b200 import _lib
     from cuperiod_b200.bls import _grid_segments
     from cuperiod_b200.grid import GridSpec
     from cuperiod_b200.settings import BLSSettings
-    from cuperiod_b200.synthetic import batched_curves, batched_periods
+    from cuperiod_b200.synthetic import (batched_curves, batched_periods, long_baseline_curves,
+                                         long_baseline_periods)
 
-    curves = batched_curves(n_curves, seed=seed)
-    settings = BLSSettings()
-    segments = _grid_segments(GridSpec(kind="period", values=batched_periods()), settings)
+    if kind == "long-baseline":
+        curves = long_baseline_curves(n_curves, seed=seed)
+        settings = BLSSettings(n_durations=12, max_period_days=400.0)
+        periods = long_baseline_periods()
+    else:
+        curves = batched_curves(n_curves, seed=seed)
+        settings = BLSSettings()
+        periods = batched_periods()
+    segments = _grid_segments(GridSpec(kind="period", values=periods), settings)
     grid = _lib.PackedGrid.from_segments(segments, settings.bins_per_duration, 0)
     packed = _lib.PackedCurves.from_arrays([(c.t, c.y, c.dy) for c in curves])
     return curves, segments, grid, packed
@@ -178,10 +195,57 @@ def cpu_baseline_sample(curves, segments, seconds: float) -> dict:
                       f"workload mean N {mean_n:.0f}) in {dt:.1f} s"}
 
 
+def long_baseline_check(engine, curves, segments, grid, n_check: int):
+    """Per-curve errors of the engine against the oracle (the reference's
+    algorithm in FP64, on every host core) on the first ``n_check`` curves of
+    the long-baseline workload, and that CPU search's speed."""
+    from cuperiod_b200 import _lib
+    from oracle import oracle
+
+    picks = list(range(min(n_check, len(curves))))
+    if not picks:
+        return None, None
+    got = engine.search(grid, _lib.PackedCurves.from_arrays(
+        [(curves[i].t, curves[i].y, curves[i].dy) for i in picks]))[0]
+    cores = os.cpu_count() or 1
+    raw, floored, at_best, within, agree = [], [], [], [], 0
+    t0 = time.perf_counter()
+    for j, i in enumerate(picks):
+        c = curves[i]
+        dy = np.ones_like(c.y) if c.dy is None else c.dy
+        ref = np.concatenate([oracle.bls_power(c.t, c.y, dy, p, d, 10, n_threads=cores)["power"]
+                              for p, d in segments])
+        fin = np.isfinite(ref)
+        err = np.abs(got[j][fin] - ref[fin])
+        mag = np.abs(ref[fin])
+        rel = err / np.maximum(mag, 1e-300)
+        raw.append(float(rel.max()))
+        # relative to the power, with an absolute floor of 1e-3 of the curve's
+        # largest power (a box with no dip has a power near 0)
+        floored.append(float(np.max(err / np.maximum(mag, 1e-3 * mag.max()))))
+        within.append(float(np.mean(rel <= 1e-6)))
+        best = int(np.argmax(np.where(fin, ref, -np.inf)))
+        at_best.append(float(abs(got[j][best] - ref[best]) / abs(ref[best])))
+        agree += int(best == np.argmax(np.where(np.isfinite(got[j]), got[j], -np.inf)))
+    dt = time.perf_counter() - t0
+    precision = {"curves_checked": len(picks), "argmax_agree": agree,
+                 "rel_power_err_at_best": max(at_best),
+                 "max_rel_power_err_floored": max(floored),
+                 "floor": "1e-3 x the curve's largest power",
+                 "max_rel_power_err_raw": max(raw),
+                 "periods_within_1e-6_raw": min(within),
+                 "reference": "oracle (the reference's algorithm, FP64) on the host cores"}
+    cpu = {"value": len(picks) / dt, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"{len(picks)} curves of the workload in {dt:.1f} s"}
+    return precision, cpu
+
+
 def run_reference(args) -> None:
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    curves, segments, _, _ = workload(args.curves, args.seed)
+    lb = args.workload == "long-baseline"
+    n_curves = args.lb_curves if lb else args.curves
+    curves, segments, _, _ = workload(n_curves, args.seed, args.workload)
     for _ in range(args.warmup):
         cpu_baseline_sample(curves, segments, args.cpu_seconds / 4)
     vals = [cpu_baseline_sample(curves, segments, args.cpu_seconds) for _ in range(args.steps)]
@@ -189,9 +253,10 @@ def run_reference(args) -> None:
     cb = dict(vals[-1], value=value)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.curves / value,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * n_curves / value,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "curves_per_rank": args.curves,
+        "data": "synthetic", "config": {"workload": LB_WORKLOAD.format(n=n_curves) if lb
+                                        else WORKLOAD, "curves_per_rank": n_curves,
                                         "variant": "plain full grid", "cpu": "host cores"},
         "cpu_baseline": cb,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -218,11 +283,13 @@ def run_ours(args) -> None:
             dist.barrier()
 
 
-    curves, segments, grid, packed = workload(args.curves, args.seed + rank)
+    lb = args.workload == "long-baseline"
+    n_curves = args.lb_curves if lb else args.curves
+    curves, segments, grid, packed = workload(n_curves, args.seed + rank, args.workload)
     tune = None
     if args.tile == "auto":
         from cuperiod_b200.autotune import tuned_engine
-        engine, tune = tuned_engine(grid, packed, device=local)
+        engine, tune = tuned_engine(grid, packed, device=local, sample=32 if lb else 128)
     else:
         engine = _lib.Engine(device=local)
     # a stream of our own: the C ABI reads a NULL stream as "the engine's stream",
@@ -255,7 +322,7 @@ def run_ours(args) -> None:
     total_ms = starts[0].elapsed_time(ends[-1])
     ms_per_step = max_over_ranks(total_ms / args.steps)
     kernel_ms = max_over_ranks(statistics.mean(step_ms))
-    value = world * args.curves / (ms_per_step / 1000.0)
+    value = world * n_curves / (ms_per_step / 1000.0)
 
     # ---- end to end through the C ABI, host buffers in and out ------------------
     e2e_ms = []
@@ -272,7 +339,7 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
         e2e_ms.append(s.elapsed_time(e))
     e2e_step = max_over_ranks(statistics.mean(e2e_ms))
-    e2e_value = world * args.curves / (e2e_step / 1000.0)
+    e2e_value = world * n_curves / (e2e_step / 1000.0)
 
     if rank == 0:
         peaks = {}
@@ -284,7 +351,7 @@ def run_ours(args) -> None:
         hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
         n_pts = info["n_points"]
         P = info["n_periods"]
-        alg_bytes = n_pts * 12 + P * 24 + 7 * 8 * args.curves * P
+        alg_bytes = n_pts * 12 + P * 24 + 7 * 8 * n_curves * P
         achieved = alg_bytes / (kernel_ms / 1000.0) / 1e9
         # SM-pipe model: 3 native shared atomics per fold at the measured random
         # rate, 2 FP64 ops per fold, ~10 FP32 ops per box
@@ -302,7 +369,8 @@ def run_ours(args) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "curves_per_rank": args.curves,
+            "config": {"workload": LB_WORKLOAD.format(n=n_curves) if lb else WORKLOAD,
+                       "curves_per_rank": n_curves,
                        "variant": "plain full grid", "parallelism": f"replicas x{world}",
                        "l2": "inputs (~%d MB/rank) exceed L2; no flush" % (n_pts * 12 // 2**20),
                        "tile": (tune.shape.label() if tune else "default")
@@ -316,7 +384,7 @@ def run_ours(args) -> None:
                        "trials_per_s": info["trials"] * world / (ms_per_step / 1000.0)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm,
-                         "traffic": TRAFFIC_256 * args.curves / 256.0,
+                         "traffic": None if lb else TRAFFIC_256 * n_curves / 256.0,
                          "peak_source": hbm_src,
                          "note": "the search is SM-bound (shared atomics, FP64/FP32 pipes); "
                                  "see sm_roofline"},
@@ -327,9 +395,12 @@ def run_ours(args) -> None:
             "clocks": clocks,
             "gpu_launches": args.steps * n_modes,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": info["h2d_bytes"],
-                    "d2h_bytes_per_step": 32 * args.curves},
+                    "d2h_bytes_per_step": 32 * n_curves},
         }
-        if world == 1:
+        if world == 1 and lb:
+            out["precision"], out["cpu_baseline"] = long_baseline_check(
+                engine, curves, segments, grid, args.lb_check)
+        elif world == 1:
             out["cpu_baseline"] = cpu_baseline_sample(curves, segments, args.cpu_seconds)
         print(json.dumps(out), flush=True)
     engine.close()
