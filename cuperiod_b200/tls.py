@@ -162,7 +162,8 @@ def tls_power_many(curves: Sequence[tuple], periods, *, settings: TLSSettings,
             [prepared[i][0] for i in live], periods, n_bins=settings.n_phase_bins,
             dur_bins=dur, templates=templates, den_rel=DEN_REL_EPS)
         for j, i in enumerate(live):
-            res = {name: np.array(out[f, j]) for f, name in enumerate(_lib.TLS_FIELD_NAMES)}
+            # views of the downloaded block (_finish replaces, never writes, them)
+            res = {name: out[f, j] for f, name in enumerate(_lib.TLS_FIELD_NAMES)}
             results[i] = _finish(res, curves[i][2], prepared[i][1], prepared[i][2])
     return results  # type: ignore[return-value]
 
@@ -211,14 +212,42 @@ class TLSMethod:
             raise InsufficientDataError("TLS: no usable time baseline")
         return finite
 
-    def _periodogram(self, res, periods, finite: LightCurve) -> Periodogram:
+    def _periodogram(self, res, periods, finite: LightCurve, axis=None) -> Periodogram:
+        """``axis``: ``(frequency, period, order)`` of the grid sorted into
+        ascending frequency once for many curves (``_sorted_axis``)."""
         extras = {"sr": res["sr"], "depth": res["depth"], "duration": res["duration"],
                   "t0": res["t0"]}
-        return Periodogram.from_spectrum(method="TLS", backend=BACKEND_NAME,
-                                         frequency=1.0 / periods, power=res["sde"],
-                                         objective_sense="max", n_samples=finite.n,
-                                         baseline=finite.baseline, extras=extras,
-                                         meta=finite.meta)
+        if axis is None:
+            return Periodogram.from_spectrum(method="TLS", backend=BACKEND_NAME,
+                                             frequency=1.0 / periods, power=res["sde"],
+                                             objective_sense="max", n_samples=finite.n,
+                                             baseline=finite.baseline, extras=extras,
+                                             meta=finite.meta)
+        frequency, period, order = axis
+        return Periodogram("TLS", BACKEND_NAME, frequency, period,
+                           np.ascontiguousarray(res["sde"][order]), "max", int(finite.n),
+                           float(finite.baseline),
+                           {k: np.ascontiguousarray(np.asarray(v, dtype=np.float64)[order])
+                            for k, v in extras.items()}, dict(finite.meta or {}), {})
+
+    @staticmethod
+    def _sorted_axis(periods):
+        """The grid in ascending frequency as ``Periodogram.from_spectrum`` sorts
+        it, once: shared read-only frequency and period arrays and the order."""
+        frequency = 1.0 / np.asarray(periods, dtype=np.float64)
+        step = np.diff(frequency)
+        if frequency.size < 2 or bool(np.all(step > 0.0)):
+            order = slice(None)
+        elif bool(np.all(step < 0.0)):
+            order = slice(None, None, -1)
+        else:
+            order = np.argsort(frequency, kind="stable")
+        frequency = np.ascontiguousarray(frequency[order])
+        with np.errstate(divide="ignore"):
+            period = 1.0 / frequency
+        frequency.setflags(write=False)
+        period.setflags(write=False)
+        return frequency, period, order
 
     def power(self, grid: GridSpec, lc: LightCurve, settings: TLSSettings,
               backend: str = BACKEND_NAME, engine: _lib.Engine | None = None) -> Periodogram:
@@ -239,7 +268,8 @@ class TLSMethod:
         periods = grid.period
         res = tls_power_many([(f.time, f.value, f.error) for f in finite], periods,
                              settings=settings, engine=engine)
-        return [self._periodogram(r, periods, f) for r, f in zip(res, finite)]
+        axis = self._sorted_axis(periods)
+        return [self._periodogram(r, periods, f, axis) for r, f in zip(res, finite)]
 
 
 def _register() -> None:
