@@ -83,6 +83,12 @@ struct CurveDesc {
     double i_total;         // GENERAL: sum of the scaled weights
     int32_t e_r;            // r (reference units) = stored r * 2^-e_r
     int32_t e_i;            // GENERAL: ivar (reference units) = stored weight * 2^-e_i
+    // UNIFORM: a point's stored value is round(y*ivar * 2^e_r) - round(ybar*ivar
+    // * 2^e_r): centred by a whole number of quanta, so each point's rounding is
+    // its own (centring by ybar itself gave every point the same rounding error,
+    // which grew with the box instead of its square root).
+    double center;          // the per-point centring, reference units
+    double center_frac;     // ybar*ivar*2^e_r minus that whole number (|.| <= 1/2)
 };
 
 struct WorkItem {

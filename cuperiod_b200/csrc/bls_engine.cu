@@ -365,8 +365,21 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
         std::frexp(max_r, &k);             // max_r < 2^k
         e_r = bits - k;                    // |r_q| <= 2^bits
     }
-    for (int64_t j = 0; j < n; ++j)
-        pay_r[point_slot(j, n)] = split_word(std::llrint(std::ldexp(r[j], e_r)));
+    // one weight: every point is centred by the same whole number of quanta cq
+    // (|stored| <= |r| * 2^e_r + 1: the median-centred mean is within max|r| of
+    // 0, so nothing overflows); per-point weights keep r
+    long long cq = 0;
+    double c_frac = 0.0;
+    if (uniform) {
+        const double cw = std::ldexp(ybar * iv[0], e_r);
+        cq = std::llrint(cw);
+        c_frac = cw - (double)cq;
+        for (int64_t j = 0; j < n; ++j)
+            pay_r[point_slot(j, n)] = split_word(std::llrint(std::ldexp(yw[j], e_r)) - cq);
+    } else {
+        for (int64_t j = 0; j < n; ++j)
+            pay_r[point_slot(j, n)] = split_word(std::llrint(std::ldexp(r[j], e_r)));
+    }
     int e_i = 0;
     double i_total = 0.0;
     // per-point weights within a factor 2^8 of each other: 38-bit fixed point
@@ -421,6 +434,8 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
     d.i_total = i_total;
     d.e_r = e_r;
     d.e_i = e_i;
+    d.center = std::ldexp((double)cq, -e_r);
+    d.center_frac = c_frac;
     ch.tau_max = tau_max;
 }
 

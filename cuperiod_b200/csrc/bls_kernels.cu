@@ -373,9 +373,10 @@ template <int MODE>
 __device__ __forceinline__ BoxSums box_sums(uint32_t hq, const CurveDesc& cv, int n, int d) {
     BoxSums b;
     if (MODE == MODE_UNIFORM) {
-        b.iv_in = (double)(prefix_c(hq, n + d) - prefix_c(hq, n)) * cv.w_uniform;
+        const double cnt = (double)(prefix_c(hq, n + d) - prefix_c(hq, n));
+        b.iv_in = cnt * cv.w_uniform;
         b.y_in = ldexp((double)(prefix_r(hq, n + d) - prefix_r(hq, n)), -cv.e_r) +
-                 cv.ybar * b.iv_in;
+                 cv.center * cnt;
     } else if (MODE == MODE_WIDE) {
         b.iv_in = ldexp((double)(wide_prefix_i(hq, n + d) - wide_prefix_i(hq, n)), -cv.e_i);
         b.y_in = ldexp((double)(wide_prefix_r(hq, n + d) - wide_prefix_r(hq, n)), -cv.e_r) +
@@ -632,9 +633,10 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
                         rw += s.tot_wd[wp];
                     }
                 }
+                const float cfrac = (float)cv.center_frac;
                 for (int i = l0; i < l1; ++i) {
                     const uint32_t rec = hq + (uint32_t)i * kRec;
-                    float tf, wf;
+                    float tf, wf, tm = 0.0f;
                     if (MODE != MODE_GENERAL) {
 #pragma unroll
                         for (int w = 0; w < kNW; ++w) {
@@ -642,8 +644,17 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
                             st_u32(rec + 4 * w, run[w]);
                         }
                         if (MODE == MODE_UNIFORM) {
-                            tf = (float)((long long)(int32_t)run[1] * (1ll << kHalfBits) +
-                                         (long long)run[0]);
+                            // the screen's t is centred by ybar itself: the stored
+                            // prefix minus center_frac per point, in FP32.  tf is
+                            // within 2^-23 tm of the exact value (pf and tf round
+                            // once each, cf <= 2^16 twice), so a box's t is within
+                            // 1.5 * 2^-22 of the largest tm, inside Et
+                            const float pf = (float)((long long)(int32_t)run[1] *
+                                                         (1ll << kHalfBits) +
+                                                     (long long)run[0]);
+                            const float cf = cfrac * (float)run[2];
+                            tf = pf - cf;
+                            tm = fmaxf(fabsf(pf), fabsf(tf)) + fabsf(cf);
                             wf = (float)run[2];
                         } else {
                             tf = (float)wide_value(run[0], run[1], run[2]);
@@ -659,7 +670,7 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
                         wf = (float)rw;
                     }
                     st_f2(scr_s + (uint32_t)i * 8u, make_float2(tf, wf));
-                    tmax = fmaxf(tmax, fabsf(tf));
+                    tmax = fmaxf(tmax, MODE == MODE_UNIFORM ? tm : fabsf(tf));
                 }
                 tmax = warp_max(tmax);
                 if (lane == 0) s.red_t[warp] = tmax;
@@ -705,13 +716,18 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
                         MODE == MODE_UNIFORM ? ldexp((double)prefix_r(hq, i), -e_r)
                         : MODE == MODE_WIDE  ? ldexp((double)wide_prefix_r(hq, i), -e_r)
                                              : ldexp(ld_f64(hq + (uint32_t)i * 16u), -e_r);
-                    a.debug_prefix[i] = r_i + cv.ybar * iv_prefix(i);
+                    a.debug_prefix[i] =
+                        r_i + (MODE == MODE_UNIFORM ? cv.center * (double)prefix_c(hq, i)
+                                                    : cv.ybar * iv_prefix(i));
                     a.debug_prefix[hl + i] = iv_prefix(i);
                 }
             }
 
             // ---- sweep: durations outer (the reference's order), two starts per lane ----
-            const float Et = cv.exact_all ? CUDART_INF_F : tmax * (1.0f / 2097152.0f);  // 2^-21
+            // bound on the FP32 error of a box's t: 2^-21 of the largest prefix
+            // (one rounding per prefix, one per difference: 2^-22, 2x slack; one
+            // weight: 1.5 * 2^-22 of the largest tm, 1.33x slack)
+            const float Et = cv.exact_all ? CUDART_INF_F : tmax * (1.0f / 2097152.0f);
             const float Wt = MODE == MODE_UNIFORM ? (float)cv.n_points
                              : MODE == MODE_WIDE  ? (float)ldexp(cv.i_total, -kWideScreenShift)
                                                   : (float)cv.i_total;
