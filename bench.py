@@ -50,7 +50,7 @@ LB_WORKLOAD = ("long-baseline precision stress BLS: {n} curves of 60,000 points 
 # over the first 256 curves of this workload, from one ncu capture
 # (profiles/bls_search_kernel_launches_256curves.txt); a launch's traffic grows in
 # proportion to its curves (points in, 7 fields x periods out)
-TRAFFIC_256 = 65201408 + 679578368
+TRAFFIC_256 = 58348800 + 678396928
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
