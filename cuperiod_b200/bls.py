@@ -276,8 +276,6 @@ class BLSMethod:
         batch/runner.py:187-250): every curve of ``items`` -- ``(key, curve,
         grid)``, equal grids passed as the same object -- in one launch, each
         over its grid, peaks ranked on the device.  Rows in ``items`` order."""
-        from .result import DEFAULT_HARMONIC_MAX, DEFAULT_SEPARATION_RAYLEIGH
-        from .settings import peak_defaults
         count = max(int(n_best), 1)
         slot: dict[int, int] = {}
         grids: list[GridSpec] = []
@@ -324,20 +322,7 @@ class BLSMethod:
                                   [(prepared[i][0].time, prepared[i][0].value, prepared[i][1])
                                    for i in dev]))
             eng.launch()
-            d = peak_defaults(settings)
-            sep_r = float(d.get("min_separation_rayleigh", DEFAULT_SEPARATION_RAYLEIGH))
-            order = int(d.get("harmonic_max", DEFAULT_HARMONIC_MAX))
-            tol_set = d.get("alias_tolerance")
-            sep = np.empty(len(dev))
-            tol = np.empty(len(dev))
-            for j, i in enumerate(dev):
-                f = prepared[i][0]
-                resolved = f.baseline > 0.0
-                separation = sep_r / f.baseline if resolved else 0.0
-                t = tol_set if tol_set is not None else (
-                    min(separation, 1.0 / f.baseline) if resolved else 0.0)
-                sep[j] = max(separation, 1e-12)
-                tol[j] = max(float(t), 1e-12)
+            order, sep, tol = _peak_params([prepared[i][0].baseline for i in dev], settings)
             n_peaks, _, fields = eng.rows(count, order, sep, tol)
             for j, i in enumerate(dev):
                 rows[i] = self._row(items[i][0], prepared[i][0], int(n_peaks[j]), fields[j],
@@ -391,8 +376,6 @@ class BLSMethod:
             return self.rows_by_grid([(key, lc, self.default_grid(lc, settings))
                                       for key, lc in keyed], settings, n_best=n_best,
                                      extra_keys=extra_keys, engine=engine)
-        from .result import DEFAULT_HARMONIC_MAX, DEFAULT_SEPARATION_RAYLEIGH
-        from .settings import peak_defaults
         prepared = [_prepared_curve(lc, settings) for _, lc in keyed]
         if not prepared:
             return []
@@ -402,13 +385,7 @@ class BLSMethod:
         eng.prepare_default(spec, baselines, _lib.PackedCurves.from_arrays(
             [(f.time, f.value, e) for f, e in prepared]))
         eng.launch()
-        d = peak_defaults(settings)
-        sep_r = float(d.get("min_separation_rayleigh", DEFAULT_SEPARATION_RAYLEIGH))
-        order = int(d.get("harmonic_max", DEFAULT_HARMONIC_MAX))
-        tol_set = d.get("alias_tolerance")
-        sep = np.maximum(sep_r / baselines, 1e-12)
-        tol = np.maximum(np.full(baselines.size, float(tol_set)) if tol_set is not None
-                         else np.minimum(sep_r / baselines, 1.0 / baselines), 1e-12)
+        order, sep, tol = _peak_params(baselines, settings)
         n_peaks, _, fields = eng.rows(count, order, sep, tol)
         return [self._row(key, f, int(n_peaks[j]), fields[j], n_best, extra_keys)
                 for j, ((key, _), (f, _)) in enumerate(zip(keyed, prepared))]
@@ -439,6 +416,25 @@ class BLSMethod:
                                              _objective_flag(settings.objective))
         packed = _lib.PackedCurves.from_arrays(curves)
         return (engine or _lib.default_engine()).search(grid, packed)
+
+
+def _peak_params(baselines, settings: BLSSettings) -> tuple[int, np.ndarray, np.ndarray]:
+    """The device ranking's inputs for curves of these baselines (all > 0):
+    the harmonic order, and per curve the minimum frequency separation
+    max(min_separation_rayleigh / baseline, 1e-12) and the alias tolerance
+    max(alias_tolerance or min(separation, 1 / baseline), 1e-12) -- the
+    defaults Periodogram.best_periods resolves (core/result.py:285-367)."""
+    from .result import DEFAULT_HARMONIC_MAX, DEFAULT_SEPARATION_RAYLEIGH
+    from .settings import peak_defaults
+    d = peak_defaults(settings)
+    sep_r = float(d.get("min_separation_rayleigh", DEFAULT_SEPARATION_RAYLEIGH))
+    order = int(d.get("harmonic_max", DEFAULT_HARMONIC_MAX))
+    tol_set = d.get("alias_tolerance")
+    b = np.asarray(baselines, dtype=np.float64)
+    separation = sep_r / b
+    tol = (np.full(b.size, float(tol_set)) if tol_set is not None
+           else np.minimum(separation, 1.0 / b))
+    return order, np.maximum(separation, 1e-12), np.maximum(tol, 1e-12)
 
 
 def _fields(out: np.ndarray, segments: list[Segment]) -> dict[str, np.ndarray]:

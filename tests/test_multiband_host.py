@@ -90,3 +90,4 @@ def test_batch_records_short_stars_and_curves_without_a_launch():
     assert set(res.errors) == {"star", "curve"}
     assert "no band has enough" in res.errors["star"]
     assert res.errors["curve"].startswith("InsufficientDataError")
+
