@@ -18,6 +18,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <new>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -47,6 +48,17 @@ int fail(int code, const char* fmt, ...) {
 int cuda_fail(cudaError_t e, const char* what) {
     return fail(e == cudaErrorMemoryAllocation ? BLS_E_NOMEM : BLS_E_CUDA, "%s: %s", what,
                 cudaGetErrorString(e));
+}
+
+// Runs an entry's body; host allocation failures become BLS_E_NOMEM instead of
+// an exception escaping the C ABI.
+template <typename F>
+int guarded(F&& body) {
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        return fail(BLS_E_NOMEM, "host allocation failed");
+    }
 }
 
 #define CUDA_TRY(expr, what)                          \
@@ -547,8 +559,13 @@ int do_prepare(BlsEngine* e, const BlsGrid* grids, int n_grids, const int32_t* g
     double* hiv64 = e->h_iv64.as<double>();
     parallel_for(nc, [&](int c, int w) {
         const int64_t off = cv->offsets[c];
-        pack_curve(cv, c, off, htau + off, hpr + off, hr64 + off, hiv64 + off, curves[c],
-                   scratch[w]);
+        try {                       // a worker thread: nothing may escape it
+            pack_curve(cv, c, off, htau + off, hpr + off, hr64 + off, hiv64 + off, curves[c],
+                       scratch[w]);
+        } catch (const std::bad_alloc&) {
+            curves[c].status = BLS_E_NOMEM;
+            curves[c].err = "host allocation failed while packing a light curve";
+        }
         curves[c].d.out_off = spec_off[c] - pbase[gid[c]];
     });
     int n_uniform = 0;
@@ -572,6 +589,7 @@ int do_prepare(BlsEngine* e, const BlsGrid* grids, int n_grids, const int32_t* g
     std::vector<int> grid_err(n_grids, BLS_OK);
     std::vector<std::string> grid_msg(n_grids);
     parallel_for(n_grids, [&](int k, int /*w*/) {
+      try {                         // a worker thread: nothing may escape it
         const BlsGrid& g = grids[k];
         auto bad = [&](int code, std::string msg) {
             grid_err[k] = code;
@@ -681,6 +699,10 @@ int do_prepare(BlsEngine* e, const BlsGrid* grids, int n_grids, const int32_t* g
             grid_boxes[k] += boxes;                  // per curve of this grid
             grid_trials[k] += (double)sd.n_periods * sh.dur.size();
         }
+      } catch (const std::bad_alloc&) {
+        grid_err[k] = BLS_E_NOMEM;
+        grid_msg[k] = "host allocation failed while preparing a grid";
+      }
     });
     for (int k = 0; k < n_grids; ++k)
         if (grid_err[k]) return fail(grid_err[k], "%s", grid_msg[k].c_str());
@@ -1577,7 +1599,7 @@ int bls_engine_destroy(BlsEngine* engine) {
 int bls_prepare(BlsEngine* e, const BlsGrid* grid, const BlsCurves* curves, void* stream) {
     if (!e) return fail(BLS_E_INVALID, "engine is NULL");
     cudaSetDevice(e->device);
-    return do_prepare(e, grid, 1, nullptr, curves, pick(e, stream));
+    return guarded([&] { return do_prepare(e, grid, 1, nullptr, curves, pick(e, stream)); });
 }
 
 int bls_prepare_grids(BlsEngine* e, int32_t n_grids, const BlsGrid* grids,
@@ -1587,7 +1609,8 @@ int bls_prepare_grids(BlsEngine* e, int32_t n_grids, const BlsGrid* grids,
     if (n_grids > 1 && !grid_of_curve)
         return fail(BLS_E_INVALID, "grid_of_curve is required with more than one grid");
     cudaSetDevice(e->device);
-    return do_prepare(e, grids, n_grids, grid_of_curve, curves, pick(e, stream));
+    return guarded(
+        [&] { return do_prepare(e, grids, n_grids, grid_of_curve, curves, pick(e, stream)); });
 }
 
 int bls_default_grid(const BlsDefaultGrid* spec, double baseline, int64_t capacity,
@@ -1617,6 +1640,11 @@ int bls_default_grid_sizes(const BlsDefaultGrid* spec, int32_t n, const double* 
     return BLS_OK;
 }
 
+namespace {
+int prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* baselines,
+                    const BlsCurves* cv, void* stream);
+}  // namespace
+
 int bls_prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* baselines,
                         const BlsCurves* cv, void* stream) {
     if (!e) return fail(BLS_E_INVALID, "engine is NULL");
@@ -1624,6 +1652,12 @@ int bls_prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* 
         return fail(BLS_E_INVALID, "spec, baselines and curves are required");
     if (spec->n_starts < 0 || (spec->n_starts > 0 && (!spec->dur_offsets || !spec->durations)))
         return fail(BLS_E_INVALID, "bad duration table");
+    return guarded([&] { return prepare_default(e, spec, baselines, cv, stream); });
+}
+
+namespace {
+int prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* baselines,
+                    const BlsCurves* cv, void* stream) {
     const int nc = cv->n_curves;
     // one grid per distinct baseline (bit pattern)
     std::unordered_map<uint64_t, int32_t> slot;
@@ -1670,6 +1704,7 @@ int bls_prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* 
     cudaSetDevice(e->device);
     return do_prepare(e, grids.data(), ng, gid.data(), cv, pick(e, stream));
 }
+}  // namespace
 
 int bls_launch(BlsEngine* e, void* stream) {
     if (!e) return fail(BLS_E_INVALID, "engine is NULL");

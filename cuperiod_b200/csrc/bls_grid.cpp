@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -24,8 +25,27 @@
 
 namespace blsb200 {
 
+namespace {
+// The reference's hard limit on a grid's trial samples (MAX_GRID_SIZE,
+// core/grid.py:417-505): a baseline beyond it is refused, not allocated.
+constexpr int64_t kMaxGridPeriods = 250000000;
+
+int build(const BlsDefaultGrid& sp, double baseline, DefaultGrid& out, std::string& err);
+}  // namespace
+
 int build_default_grid(const BlsDefaultGrid& sp, double baseline, DefaultGrid& out,
                        std::string& err) {
+    try {
+        return build(sp, baseline, out, err);
+    } catch (const std::bad_alloc&) {
+        out = DefaultGrid();
+        err = "host allocation failed while building the default grid";
+        return BLS_E_NOMEM;
+    }
+}
+
+namespace {
+int build(const BlsDefaultGrid& sp, double baseline, DefaultGrid& out, std::string& err) {
     out.periods.clear();
     out.seg_offsets.assign(1, 0);
     out.seg_start.clear();
@@ -51,6 +71,10 @@ int build_default_grid(const BlsDefaultGrid& sp, double baseline, DefaultGrid& o
             return BLS_E_RESOURCE;
         }
         const int64_t len = span > 0.0 ? (int64_t)span : 0;
+        if ((int64_t)out.periods.size() + len > kMaxGridPeriods) {
+            err = "the default grid exceeds the limit of 250,000,000 trial periods";
+            return BLS_E_RESOURCE;
+        }
         if (len > 0) {
             const double v1 = start + df;
             const double delta = v1 - start;
@@ -81,6 +105,7 @@ int build_default_grid(const BlsDefaultGrid& sp, double baseline, DefaultGrid& o
     }
     return BLS_OK;
 }
+}  // namespace
 
 int64_t default_grid_size(const BlsDefaultGrid& sp, double baseline) {
     DefaultGrid g;

@@ -86,3 +86,20 @@ def test_split_default_records_the_references_failures():
     assert [k for k, _ in good] == ["o"]
     assert errors["s"].startswith("InsufficientDataError")
     assert errors["h"].startswith("GridTooLargeError")
+
+
+def test_a_grid_beyond_the_reference_limit_is_refused_not_allocated():
+    # a baseline whose default grid exceeds the reference's 250,000,000 trial
+    # samples is refused before anything is allocated (1e7 days: ~2e9 periods)
+    import time
+
+    from cuperiod_b200 import _lib
+    from cuperiod_b200.bls import default_grid_spec
+    from cuperiod_b200.errors import BackendUnavailableError
+    from cuperiod_b200.settings import BLSSettings
+    spec = default_grid_spec(BLSSettings(), 1.0e7)
+    t0 = time.perf_counter()
+    assert _lib.default_grid_sizes(spec, [1.0e7])[0] == -1
+    with pytest.raises(BackendUnavailableError, match="250,000,000"):
+        _lib.default_grid(spec, 1.0e7)
+    assert time.perf_counter() - t0 < 5.0
