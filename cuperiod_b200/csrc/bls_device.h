@@ -34,7 +34,9 @@ constexpr int kMaxDur = 32;         // deduplicated box widths per segment
 constexpr int kMaxTile = 16;        // periods per work item
 constexpr int kHalfBits = 13;       // bits per atomic half-word
 constexpr int kCountShift = 18;     // packed prefix: R * 2^18 + count
-constexpr int kMaxPoints = (1 << 17) - 1;  // per curve: 32-bit prefix words stay exact
+constexpr int kMaxExactPoints = (1 << 17) - 1;  // UNIFORM / WIDE: 32-bit prefix words
+                                                // stay exact; longer curves take GENERAL
+constexpr int kMaxPoints = 1 << 30;             // per curve (int32 indices)
 
 // One CTA folds points in chunks of kChunkThreads x kChunkPts.  The host stores
 // every full chunk lane-interleaved: memory slot chunk*2048 + r*256 + lane holds

@@ -353,6 +353,10 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
         yw[j] = (y[j] - med) * iv[j];
         uniform = uniform && iv[j] == iv[0];
     }
+    // the exact integer sums hold up to kMaxExactPoints points; a longer curve
+    // keeps FP64 sums (the reference's arithmetic, in atomic order)
+    const bool exact_ok = n <= kMaxExactPoints;
+    uniform = uniform && exact_ok;
     const double sum_y = pairwise_sum(yw, n);
     const double sum_ivar = pairwise_sum(iv, n);
     double sum_abs = 0.0;
@@ -398,7 +402,7 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
     // (the smallest weight keeps >= 2^28 steps, a relative 2^-29)
     double min_i = max_i;
     for (int64_t j = 0; j < n && !uniform; ++j) min_i = std::min(min_i, iv[j]);
-    const bool wide = !uniform && min_i > 0.0 && std::isfinite(max_i) &&
+    const bool wide = exact_ok && !uniform && min_i > 0.0 && std::isfinite(max_i) &&
                       max_i <= 256.0 * min_i && max_r > 0.0 && std::isfinite(max_r);
     if (wide) {
         int kr = 0, ki = 0;

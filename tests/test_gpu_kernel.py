@@ -162,3 +162,18 @@ def test_gappy_weighted_curve_picks_the_references_box(engine, objective, weight
     same = (got["duration"] == ref["duration"]) & \
         (np.abs(got["transit_time"] - ref["transit_time"]) <= 1e-9)
     assert same.mean() >= (0.999 if weights == "wild" else 0.99)
+
+
+@pytest.mark.parametrize("weights", ["uniform", "hetero"])
+def test_curve_beyond_the_exact_sums_matches_oracle(engine, weights):
+    # 150,000 points, past the 2^17 - 1 that the exact 32-bit sums hold: the
+    # curve keeps FP64 sums (the reference's arithmetic) and is searched, not
+    # refused
+    t, y, dy = transit_curve(150000, span=120.0, period=3.3, depth=2e-3, seed=21,
+                             weights=weights)
+    periods = np.geomspace(0.5, 12.0, 1500)
+    durations = np.array([0.04, 0.08, 0.12, 0.16])
+    ref = oracle.bls_power(t, y, dy, periods, durations, 10)
+    got = _run(engine, t, y, dy, periods, durations, 10, "snr")
+    diag = compare(ref, got, rtol=1e-6, box_agree=0.99)
+    assert diag["same_argmax"]
