@@ -40,6 +40,15 @@
  *   bls_tls_search, bls_tls_prepare / _launch / _download
  *       -- _tls_cuda / _tls_numba, the transit least squares matched filter
  *          (src/cuperiod/methods/tls.py:428-621);
+ *   bls_prepare_grids, bls_default_grid, bls_default_grid_sizes,
+ *   bls_prepare_default
+ *       -- the batch runner searching every curve over its own default grid
+ *          (src/cuperiod/batch/runner.py:187-250 -> BLSMethod.default_grid,
+ *          src/cuperiod/methods/bls.py:52-125, 327-359): the grids built on the
+ *          host cores and all curves in one launch;
+ *   bls_launch_best_noalloc, bls_time_launches
+ *       -- no counterpart: an allocation-free launch for services, and the
+ *          tile-shape autotuner's clock;
  *   bls_last_error
  *       -- the exceptions the reference raises before a launch (ValueError,
  *          BackendUnavailableError from core/backend.py:340-384).
