@@ -1559,6 +1559,57 @@ int do_download_tls(BlsEngine* e, double* out, cudaStream_t st) {
     return BLS_OK;
 }
 
+// bls_prepare_default's body: one default grid per distinct baseline, built on
+// the host cores, then one launch over all of them.
+int prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* baselines,
+                    const BlsCurves* cv, void* stream) {
+    const int nc = cv->n_curves;
+    // one grid per distinct baseline (bit pattern)
+    std::unordered_map<uint64_t, int32_t> slot;
+    std::vector<double> uniq;
+    std::vector<int32_t> gid(nc);
+    for (int c = 0; c < nc; ++c) {
+        uint64_t bits;
+        std::memcpy(&bits, baselines + c, sizeof bits);
+        auto it = slot.emplace(bits, (int32_t)uniq.size());
+        if (it.second) uniq.push_back(baselines[c]);
+        gid[c] = it.first->second;
+    }
+    const int ng = (int)uniq.size();
+    std::vector<DefaultGrid> built(ng);
+    std::vector<int> codes(ng, BLS_OK);
+    std::vector<std::string> msgs(ng);
+    parallel_for(ng, [&](int k, int) { codes[k] = build_default_grid(*spec, uniq[k], built[k], msgs[k]); });
+    std::vector<std::vector<int64_t>> dur_off(ng);
+    std::vector<std::vector<double>> dur(ng);
+    std::vector<BlsGrid> grids(ng);
+    for (int k = 0; k < ng; ++k) {
+        if (codes[k]) return fail(codes[k], "baseline %.9g: %s", uniq[k], msgs[k].c_str());
+        const DefaultGrid& g = built[k];
+        if (g.periods.empty())
+            return fail(BLS_E_INVALID,
+                        "BLS: the default grid of a %.6g-day baseline is empty (baseline too "
+                        "short for the configured period range)", uniq[k]);
+        dur_off[k].assign(1, 0);
+        for (int32_t st : g.seg_start) {
+            const int64_t d0 = spec->dur_offsets[st], d1 = spec->dur_offsets[st + 1];
+            if (d1 < d0) return fail(BLS_E_INVALID, "bad duration table");
+            dur[k].insert(dur[k].end(), spec->durations + d0, spec->durations + d1);
+            dur_off[k].push_back((int64_t)dur[k].size());
+        }
+        BlsGrid& bg = grids[k];
+        bg.n_segments = (int32_t)g.seg_start.size();
+        bg.seg_offsets = g.seg_offsets.data();
+        bg.periods = g.periods.data();
+        bg.dur_offsets = dur_off[k].data();
+        bg.durations = dur[k].data();
+        bg.oversample = spec->oversample;
+        bg.objective = spec->objective;
+    }
+    cudaSetDevice(e->device);
+    return do_prepare(e, grids.data(), ng, gid.data(), cv, pick(e, stream));
+}
+
 }  // namespace
 
 extern "C" {
@@ -1644,11 +1695,6 @@ int bls_default_grid_sizes(const BlsDefaultGrid* spec, int32_t n, const double* 
     return BLS_OK;
 }
 
-namespace {
-int prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* baselines,
-                    const BlsCurves* cv, void* stream);
-}  // namespace
-
 int bls_prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* baselines,
                         const BlsCurves* cv, void* stream) {
     if (!e) return fail(BLS_E_INVALID, "engine is NULL");
@@ -1659,56 +1705,6 @@ int bls_prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* 
     return guarded([&] { return prepare_default(e, spec, baselines, cv, stream); });
 }
 
-namespace {
-int prepare_default(BlsEngine* e, const BlsDefaultGrid* spec, const double* baselines,
-                    const BlsCurves* cv, void* stream) {
-    const int nc = cv->n_curves;
-    // one grid per distinct baseline (bit pattern)
-    std::unordered_map<uint64_t, int32_t> slot;
-    std::vector<double> uniq;
-    std::vector<int32_t> gid(nc);
-    for (int c = 0; c < nc; ++c) {
-        uint64_t bits;
-        std::memcpy(&bits, baselines + c, sizeof bits);
-        auto it = slot.emplace(bits, (int32_t)uniq.size());
-        if (it.second) uniq.push_back(baselines[c]);
-        gid[c] = it.first->second;
-    }
-    const int ng = (int)uniq.size();
-    std::vector<DefaultGrid> built(ng);
-    std::vector<int> codes(ng, BLS_OK);
-    std::vector<std::string> msgs(ng);
-    parallel_for(ng, [&](int k, int) { codes[k] = build_default_grid(*spec, uniq[k], built[k], msgs[k]); });
-    std::vector<std::vector<int64_t>> dur_off(ng);
-    std::vector<std::vector<double>> dur(ng);
-    std::vector<BlsGrid> grids(ng);
-    for (int k = 0; k < ng; ++k) {
-        if (codes[k]) return fail(codes[k], "baseline %.9g: %s", uniq[k], msgs[k].c_str());
-        const DefaultGrid& g = built[k];
-        if (g.periods.empty())
-            return fail(BLS_E_INVALID,
-                        "BLS: the default grid of a %.6g-day baseline is empty (baseline too "
-                        "short for the configured period range)", uniq[k]);
-        dur_off[k].assign(1, 0);
-        for (int32_t st : g.seg_start) {
-            const int64_t d0 = spec->dur_offsets[st], d1 = spec->dur_offsets[st + 1];
-            if (d1 < d0) return fail(BLS_E_INVALID, "bad duration table");
-            dur[k].insert(dur[k].end(), spec->durations + d0, spec->durations + d1);
-            dur_off[k].push_back((int64_t)dur[k].size());
-        }
-        BlsGrid& bg = grids[k];
-        bg.n_segments = (int32_t)g.seg_start.size();
-        bg.seg_offsets = g.seg_offsets.data();
-        bg.periods = g.periods.data();
-        bg.dur_offsets = dur_off[k].data();
-        bg.durations = dur[k].data();
-        bg.oversample = spec->oversample;
-        bg.objective = spec->objective;
-    }
-    cudaSetDevice(e->device);
-    return do_prepare(e, grids.data(), ng, gid.data(), cv, pick(e, stream));
-}
-}  // namespace
 
 int bls_launch(BlsEngine* e, void* stream) {
     if (!e) return fail(BLS_E_INVALID, "engine is NULL");
