@@ -341,15 +341,15 @@ class BLSMethod:
         base: list[float] = []
         for key, lc in keyed:
             finite = lc.finite()
+            b = finite.baseline
             try:
-                check_grid_size(_default_total(finite.baseline, settings), automatic=True,
-                                time=finite.time, baseline=finite.baseline,
-                                context="BLS default grid")
+                check_grid_size(_default_total(b, settings), automatic=True, time=finite.time,
+                                baseline=b, context="BLS default grid")
             except (CuPeriodError, ValueError) as exc:
                 errors[key] = f"{type(exc).__name__}: {exc}"
                 continue
             good.append((key, lc))
-            base.append(finite.baseline)
+            base.append(b)
         if not good:
             return good, errors
         spec = default_grid_spec(settings, max(base))
