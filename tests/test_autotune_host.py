@@ -107,3 +107,16 @@ def test_key_separates_workloads():
     dy = _lib.PackedCurves(curves.offsets, curves.t, curves.y,
                            np.linspace(1.0, 2.0, curves.t.size))
     assert k != workload_key(grid, dy, "B200")
+
+
+def test_a_corrupt_cache_file_is_ignored(tmp_path):
+    from cuperiod_b200 import autotune as mod
+    from cuperiod_b200.autotune import TileShape, autotune
+    grid, curves = _batch(6)
+    cache = tmp_path / "tune.json"
+    cache.write_text("{not json")
+    mod._memory.clear()
+    res = autotune(grid, curves, candidates=[TileShape(0, 0), TileShape(0, 4)],
+                   timer=lambda shape, g, s: 2.0 if shape.max_tile else 3.0, cache=cache)
+    assert res.shape == TileShape(0, 4) and not res.cached
+    assert json.loads(cache.read_text())[res.key]["max_tile"] == 4    # rewritten whole

@@ -68,3 +68,24 @@ def test_registry_and_multiband_refusal():
     bands = {b: LightCurve(np.arange(30.0), np.ones(30), None, Domain.FLUX) for b in "gr"}
     with pytest.raises(ValueError, match="multi-band"):
         periodogram(bands, "TLS")
+
+
+def test_shared_axis_periodograms_equal_from_spectrum():
+    # power_many sorts the shared grid once; each periodogram must equal what
+    # Periodogram.from_spectrum builds for that curve alone
+    from cuperiod_b200.lightcurve import Domain, LightCurve
+    from cuperiod_b200.tls import TLSMethod, period_grid
+    from cuperiod_b200.settings import TLSSettings
+    rng = np.random.default_rng(2)
+    t = np.sort(rng.uniform(0.0, 40.0, 500))
+    lc = LightCurve(t, 1.0 + 1e-3 * rng.normal(size=t.size), None, Domain.FLUX)
+    periods = period_grid(lc.baseline, TLSSettings())
+    res = {k: rng.normal(size=periods.size) for k in ("sde", "sr", "depth", "duration", "t0")}
+    m = TLSMethod()
+    a = m._periodogram(res, periods, lc)
+    b = m._periodogram(res, periods, lc, m._sorted_axis(periods))
+    for name in ("frequency", "period", "power"):
+        assert np.array_equal(getattr(a, name), getattr(b, name)), name
+    assert a.extras.keys() == b.extras.keys()
+    assert all(np.array_equal(a.extras[k], b.extras[k]) for k in a.extras)
+    assert (a.n_samples, a.baseline, dict(a.meta)) == (b.n_samples, b.baseline, dict(b.meta))
