@@ -354,7 +354,8 @@ def run_ours(args) -> None:
         alg_bytes = n_pts * 12 + P * 24 + 7 * 8 * n_curves * P
         achieved = alg_bytes / (kernel_ms / 1000.0) / 1e9
         # SM-pipe model: 3 native shared atomics per fold at the measured random
-        # rate, 2 FP64 ops per fold, ~10 FP32 ops per box
+        # rate, 2 FP64 ops per fold, ~10 FP32 ops per box (rates from
+        # csrc/pipe_probe.cu, profiles/pipe_rates.txt)
         f_clk = (clocks.get("sm_mhz") or 1900.0) * 1e6
         n_sm = torch.cuda.get_device_properties(local).multi_processor_count
         t_atom = info["folds"] * 3 / (16.66 * n_sm * f_clk)
