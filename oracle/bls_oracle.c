@@ -10,7 +10,8 @@
  * sums and the box objective round exactly as the reference's do.
  *
  * Only the tests, the smoke check and the benchmark's CPU-baseline leg load
- * this library, and only as the checker or the timed CPU baseline.  The
+ * this library, and only as the reference results are compared with or as the
+ * timed CPU baseline.  The
  * product path (cuperiod_b200) never calls it.
  */
 #include <math.h>

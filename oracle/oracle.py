@@ -6,7 +6,8 @@ search in plain C (``bls_oracle.c``, the numba kernel of
 ``src/cuperiod/methods/_bls_core.py:341-462`` evaluated without its screen).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
-may import this module, and only as the checker or the timed CPU baseline.  The
+may import this module, and only as the reference results are compared with or as
+the timed CPU baseline.  The
 product package ``cuperiod_b200`` never imports it.
 
 It is pinned against golden vectors produced by the reference's own numba
