@@ -17,6 +17,12 @@ plain full-grid search, one persistent launch per step.
 * ``--impl reference``: the reference's CPU search (the C port of its numba
   kernel in ``oracle/``, on every host core) on a bounded sample of the same
   workload; rank 0 only.
+* The search's tile shape is autotuned (``cuperiod_b200.autotune``) on a sample
+  of the batch before the warm-up, outside the timed region; ``--tile default``
+  skips it.  ``config`` records the shape and every candidate's time.
+* Other workloads: ``--workload long-baseline`` (512 curves of 60,000 points
+  over 4 years, 200,000 periods, with per-curve power errors against the
+  oracle), ``multiband-shared`` and ``tls``.
 
 Multi-GPU: one process per GPU (torchrun); light curves are independent, so each
 rank searches its own batch (weak scaling) and only a barrier and a max of the
