@@ -71,7 +71,16 @@ def parse_args():
     p.add_argument("--curves", type=int, default=4096, help="light curves per rank")
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--cpu-seconds", type=float, default=12.0,
-                   help="target duration of the CPU-baseline sample")
+                   help="multiband-shared / tls: target duration of the CPU-baseline sample")
+    p.add_argument("--ref-curves", type=int, default=16,
+                   help="batch: curves of the N-stratified sample one reference-arm step "
+                        "(and the cpu_baseline) searches on the host cores")
+    p.add_argument("--precision-curves", type=int, default=64,
+                   help="batch: N-stratified curves of the timed batch whose spectra are "
+                        "compared with the oracle (0: none)")
+    p.add_argument("--weights", choices=("uniform", "hetero"), default="uniform",
+                   help="batch: no errors (one weight per curve, the workload as stated) or "
+                        "per-point errors sigma x U(0.7, 1.4)")
     p.add_argument("--lb-curves", type=int, default=512,
                    help="long-baseline: light curves per rank")
     p.add_argument("--lb-check", type=int, default=2,
@@ -143,7 +152,7 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def workload(n_curves: int, seed: int, kind: str = "batch"):
+def workload(n_curves: int, seed: int, kind: str = "batch", weights: str = "uniform"):
     from cuperiod_b200 import _lib
     from cuperiod_b200.bls import _grid_segments
     from cuperiod_b200.grid import GridSpec
@@ -156,7 +165,7 @@ def workload(n_curves: int, seed: int, kind: str = "batch"):
         settings = BLSSettings(n_durations=12, max_period_days=400.0)
         periods = long_baseline_periods()
     else:
-        curves = batched_curves(n_curves, seed=seed)
+        curves = batched_curves(n_curves, seed=seed, weights=weights)
         settings = BLSSettings()
         periods = batched_periods()
     segments = _grid_segments(GridSpec(kind="period", values=periods), settings)
@@ -165,40 +174,91 @@ def workload(n_curves: int, seed: int, kind: str = "batch"):
     return curves, segments, grid, packed
 
 
-def cpu_baseline_sample(curves, segments, seconds: float) -> dict:
-    """The reference's CPU search (C port of its numba kernel, all host cores) on
-    curves chosen at spread quantiles of N until ``seconds`` have passed."""
-    from oracle import oracle
+def stratified_sample(curves, k: int) -> list[int]:
+    """``k`` curves at evenly spread quantiles of the point count, (j + 0.5) / k:
+    the sample keeps the workload's length mix, so its mean cost per curve is the
+    workload's."""
+    order = np.argsort([c.t.size for c in curves], kind="stable")
+    k = max(1, min(k, len(curves)))
+    return [int(order[int((j + 0.5) / k * len(order))]) for j in range(k)]
 
-    order = np.argsort([c.t.size for c in curves])
-    # octiles of N, near the mean first, then the midpoints between them, ... until
-    # the time is up (the sample keeps the workload's length mix at any size)
-    picks, seen = [], set()
-    for level in (8, 16, 32, 64):
-        ks = sorted(range(level), key=lambda k: abs((k + 0.5) / level - 0.5))
-        for k in ks:
-            i = int(order[int((k + 0.5) / level * len(order))])
-            if i not in seen:
-                seen.add(i)
-                picks.append(i)
+
+def cpu_reference_step(curves, segments, picks) -> float:
+    """Seconds for the reference's CPU search of the ``picks`` curves: its default
+    numba path -- the screened sweep, ``BLSMethod().power(grid, lc, settings,
+    "numba")`` segment by segment (methods/bls.py:361-395, _bls_core.py:468-500)
+    -- as the oracle's C restatement (bit-identical boxes), on every host core."""
+    from oracle import oracle
     cores = os.cpu_count() or 1
-    done, t0, npts = 0, time.perf_counter(), 0
+    t0 = time.perf_counter()
     for i in picks:
         c = curves[i]
         dy = np.ones_like(c.y) if c.dy is None else c.dy
         for periods, durations in segments:
-            oracle.bls_power(c.t, c.y, dy, periods, durations, 10, n_threads=cores)
-        done += 1
-        npts += c.t.size
-        if time.perf_counter() - t0 >= seconds:
-            break
-    dt = time.perf_counter() - t0
-    mean_n = float(np.mean([c.t.size for c in curves]))
-    # scale to the workload's mean curve length (the cost is linear in N + boxes)
-    value = done / dt * (npts / done) / mean_n
-    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{done} curves of the workload (mean N {npts / done:.0f}, rescaled to the "
-                      f"workload mean N {mean_n:.0f}) in {dt:.1f} s"}
+            oracle.bls_power(c.t, c.y, dy, periods, durations, 10, n_threads=cores, screen=True)
+    return time.perf_counter() - t0
+
+
+def cpu_sample_text(curves, picks) -> str:
+    mean_s = float(np.mean([curves[i].t.size for i in picks]))
+    mean_w = float(np.mean([c.t.size for c in curves]))
+    return (f"{len(picks)} curves of the workload at evenly spread quantiles of N (mean N "
+            f"{mean_s:.0f}; workload mean N {mean_w:.0f}), all periods and durations, searched by "
+            "the reference's screened numba sweep restated in C (oracle/bls_oracle.c; chooses the "
+            "same boxes bit for bit); light curves/s of that sample")
+
+
+def cpu_baseline_sample(curves, segments, n_sample: int) -> dict:
+    """The reference's CPU search on an N-stratified sample of the workload,
+    timed once (see ``cpu_reference_step``)."""
+    picks = stratified_sample(curves, n_sample)
+    dt = cpu_reference_step(curves, segments, picks)
+    return {"value": len(picks) / dt, "unit": UNIT, "cores": os.cpu_count() or 1,
+            "kind": "port", "sample": cpu_sample_text(curves, picks) + f", {dt:.1f} s"}
+
+
+def batch_precision(engine, curves, segments, n_check: int) -> dict | None:
+    """The timed launch's spectra of ``n_check`` N-stratified curves against the
+    oracle (the reference's unscreened FP64 search, on the host cores): argmax
+    agreement, relative power errors, the share of periods within 1e-6."""
+    from oracle import oracle
+    if n_check <= 0:
+        return None
+    picks = stratified_sample(curves, n_check)
+    got = engine.download_curves(picks)
+    cores = os.cpu_count() or 1
+    agree, raw, floored, within, at_best, box_same = 0, [], [], [], [], []
+    t0 = time.perf_counter()
+    for j, i in enumerate(picks):
+        c = curves[i]
+        dy = np.ones_like(c.y) if c.dy is None else c.dy
+        parts = [oracle.bls_power(c.t, c.y, dy, p, d, 10, n_threads=cores) for p, d in segments]
+        ref = np.concatenate([r["power"] for r in parts])
+        ref_dur = np.concatenate([r["duration"] for r in parts])
+        ref_tt = np.concatenate([r["transit_time"] for r in parts])
+        g = got[j][0]
+        fin = np.isfinite(ref)
+        err = np.abs(g[fin] - ref[fin])
+        mag = np.abs(ref[fin])
+        rel = err / np.maximum(mag, 1e-300)
+        raw.append(float(rel.max()))
+        floored.append(float(np.max(err / np.maximum(mag, 1e-3 * mag.max()))))
+        within.append(float(np.mean(rel <= 1e-6)))
+        best = int(np.argmax(np.where(fin, ref, -np.inf)))
+        at_best.append(float(abs(g[best] - ref[best]) / abs(ref[best])))
+        agree += int(best == int(np.argmax(np.where(np.isfinite(g), g, -np.inf))))
+        box_same.append(float(np.mean((got[j][4] == ref_dur) & (got[j][5] == ref_tt))))
+    return {"curves_checked": len(picks), "argmax_agree": agree,
+            "sample": "N-stratified curves of the timed batch (quantiles (j+0.5)/k of N), full grid",
+            "rel_power_err_at_best": max(at_best),
+            "max_rel_power_err_floored": max(floored),
+            "floor": "1e-3 x the curve's largest power",
+            "max_rel_power_err_raw": max(raw),
+            "periods_within_1e-6_raw": min(within),
+            "same_box_frac_min": min(box_same),
+            "reference": "oracle: the reference's unscreened FP64 numba search restated in C, "
+                         "host cores",
+            "seconds": round(time.perf_counter() - t0, 1)}
 
 
 def long_baseline_check(engine, curves, segments, grid, n_check: int):
@@ -251,18 +311,24 @@ def run_reference(args) -> None:
         return
     lb = args.workload == "long-baseline"
     n_curves = args.lb_curves if lb else args.curves
-    curves, segments, _, _ = workload(n_curves, args.seed, args.workload)
+    curves, segments, _, _ = workload(n_curves, args.seed, args.workload, args.weights)
+    # every step searches the same N-stratified sample of the workload
+    picks = stratified_sample(curves, args.ref_curves)
     for _ in range(args.warmup):
-        cpu_baseline_sample(curves, segments, args.cpu_seconds / 4)
-    vals = [cpu_baseline_sample(curves, segments, args.cpu_seconds) for _ in range(args.steps)]
-    value = statistics.mean(v["value"] for v in vals)
-    cb = dict(vals[-1], value=value)
+        cpu_reference_step(curves, segments, picks)
+    times = [cpu_reference_step(curves, segments, picks) for _ in range(args.steps)]
+    value = len(picks) * len(times) / sum(times)
+    cb = {"value": value, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+          "sample": cpu_sample_text(curves, picks)}
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * n_curves / value,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": {"workload": LB_WORKLOAD.format(n=n_curves) if lb
                                         else WORKLOAD, "curves_per_rank": n_curves,
+                                        "weights": args.weights,
+                                        "curves_per_step": len(picks),
                                         "variant": "plain full grid", "cpu": "host cores"},
         "cpu_baseline": cb,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -291,7 +357,8 @@ def run_ours(args) -> None:
 
     lb = args.workload == "long-baseline"
     n_curves = args.lb_curves if lb else args.curves
-    curves, segments, grid, packed = workload(n_curves, args.seed + rank, args.workload)
+    curves, segments, grid, packed = workload(n_curves, args.seed + rank, args.workload,
+                                              args.weights)
     tune = None
     if args.tile == "auto":
         from cuperiod_b200.autotune import tuned_engine
@@ -330,22 +397,37 @@ def run_ours(args) -> None:
     kernel_ms = max_over_ranks(statistics.mean(step_ms))
     value = world * n_curves / (ms_per_step / 1000.0)
 
-    # ---- end to end through the C ABI, host buffers in and out ------------------
+    # ---- end to end through the drop-in batch entry, host light curves in and
+    # result rows out: batch_periodograms over the workload's GridSpec (segmentation,
+    # packing, upload, one launch, peaks ranked on the device, rows read back).  The
+    # call returns only once its rows are on the host, so the host clock around it
+    # is its end-to-end time (the device is idle on both sides).
+    from cuperiod_b200.batch import batch_periodograms
+    from cuperiod_b200.grid import GridSpec
+    from cuperiod_b200.lightcurve import Domain, LightCurve
+    gspec = GridSpec(kind="period", values=np.concatenate([p for p, _ in segments]))
+    keyed = [(f"lc{i}", LightCurve(c.t, c.y, c.dy, Domain.FLUX)) for i, c in enumerate(curves)]
+    summary = batch_periodograms(keyed, "BLS", grid=gspec, engine=engine, chunk_size=n_curves)
     e2e_ms = []
     for i in range(args.steps):
         barrier()
         torch.cuda.synchronize()
-        s = torch.cuda.Event(enable_timing=True)
-        e = torch.cuda.Event(enable_timing=True)
-        s.record(stream)
-        engine.prepare(grid, packed, stream=handle)
-        engine.launch(handle)
-        idx, best, mean, std = engine.download_best(handle)
-        e.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms.append(s.elapsed_time(e))
+        t0 = time.perf_counter()
+        summary = batch_periodograms(keyed, "BLS", grid=gspec, engine=engine,
+                                     chunk_size=n_curves)
+        e2e_ms.append(1000.0 * (time.perf_counter() - t0))
     e2e_step = max_over_ranks(statistics.mean(e2e_ms))
     e2e_value = world * n_curves / (e2e_step / 1000.0)
+    e2e_h2d = engine.info()["h2d_bytes"]
+    rows = summary.rows
+    n_best = 10
+    e2e_d2h = n_curves * (4 + 8 * n_best + 8 * 8 * n_best)
+    # the rows' best periods against the timed launch's per-curve best
+    engine.prepare(grid, packed, stream=handle)
+    engine.launch(handle)
+    best_idx = engine.download_best(handle)[0]
+    all_periods = np.concatenate([p for p, _ in segments])
+    rows_agree = sum(int(r["best_period"] == all_periods[b]) for r, b in zip(rows, best_idx))
 
     if rank == 0:
         peaks = {}
@@ -374,10 +456,11 @@ def run_ours(args) -> None:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed: f64 phase and objective, exact int32 bin sums, f32 screen",
             "data": "synthetic",
             "config": {"workload": LB_WORKLOAD.format(n=n_curves) if lb else WORKLOAD,
-                       "curves_per_rank": n_curves,
+                       "curves_per_rank": n_curves, "weights": args.weights,
                        "variant": "plain full grid", "parallelism": f"replicas x{world}",
                        "l2": "inputs (~%d MB/rank) exceed L2; no flush" % (n_pts * 12 // 2**20),
                        "tile": (tune.shape.label() if tune else "default")
@@ -401,14 +484,19 @@ def run_ours(args) -> None:
                             "frac": 1000.0 * t_pipe / kernel_ms},
             "clocks": clocks,
             "gpu_launches": args.steps * n_modes,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": info["h2d_bytes"],
-                    "d2h_bytes_per_step": 32 * n_curves},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": e2e_h2d,
+                    "d2h_bytes_per_step": e2e_d2h,
+                    "api": "batch_periodograms(light curves, 'BLS', grid=GridSpec, "
+                           "chunk_size=all): result rows with 10 alias-diverse peaks",
+                    "clock": "host wall clock around the synchronous call",
+                    "rows_best_equal_launch_best": rows_agree},
         }
         if world == 1 and lb:
             out["precision"], out["cpu_baseline"] = long_baseline_check(
                 engine, curves, segments, grid, args.lb_check)
         elif world == 1:
-            out["cpu_baseline"] = cpu_baseline_sample(curves, segments, args.cpu_seconds)
+            out["precision"] = batch_precision(engine, curves, segments, args.precision_curves)
+            out["cpu_baseline"] = cpu_baseline_sample(curves, segments, args.ref_curves)
         print(json.dumps(out), flush=True)
     engine.close()
     if world > 1:

@@ -97,6 +97,7 @@ def load() -> ctypes.CDLL:
         lib.bls_prepare.argtypes = [_vp, P(BlsGrid), P(BlsCurves), _vp]
         lib.bls_launch.argtypes = [_vp, _vp]
         lib.bls_download.argtypes = [_vp, _vp, _vp]
+        lib.bls_download_curves.argtypes = [_vp, _vp, _i32, _vp, _vp]
         lib.bls_device_output.argtypes = [_vp, P(_vp)]
         lib.bls_download_best.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
         lib.bls_launch_best_noalloc.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
@@ -121,7 +122,7 @@ def load() -> ctypes.CDLL:
         lib.bls_debug_prefix.argtypes = [_vp, _vp, _vp, _vp, _i64, _dbl, _vp, _i32, _i32, _vp, _vp,
                                          _vp]
         for name in ("bls_engine_create", "bls_engine_destroy", "bls_prepare", "bls_launch",
-                     "bls_download", "bls_device_output", "bls_download_best", "bls_search",
+                     "bls_download", "bls_download_curves", "bls_device_output", "bls_download_best", "bls_search",
                      "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix",
                      "bls_launch_best_noalloc", "bls_download_rows", "bls_search_joint",
                      "bls_joint_prepare", "bls_joint_launch", "bls_joint_download",
@@ -354,6 +355,22 @@ class Engine:
         assert self._curves is not None
         out = np.empty((N_FIELDS, int(self._spec_off[-1])), dtype=np.float64)
         _check(self._lib.bls_download(self._h, out.ctypes.data, stream))
+        return out
+
+    def download_curves(self, curve_ids, stream: int | None = None) -> list[np.ndarray]:
+        """Every field of the listed curves only: one ``(7, spectrum)`` array
+        per id (``bls_download_curves``)."""
+        ids = np.ascontiguousarray(curve_ids, dtype=np.int32).reshape(-1)
+        if ids.size and (ids.min() < 0 or ids.max() >= len(self._spec_off) - 1):
+            raise ValueError("curve id outside the prepared batch")
+        lens = self._spec_off[ids + 1] - self._spec_off[ids]
+        flat = np.empty(int(N_FIELDS * lens.sum()), dtype=np.float64)
+        _check(self._lib.bls_download_curves(self._h, ids.ctypes.data, int(ids.size),
+                                             flat.ctypes.data, stream))
+        out, w = [], 0
+        for n in lens.tolist():
+            out.append(flat[w:w + N_FIELDS * n].reshape(N_FIELDS, n))
+            w += N_FIELDS * n
         return out
 
     def launch(self, stream: int | None = None) -> None:

@@ -226,6 +226,7 @@ struct BlsEngine {
     int64_t spec_total = 0;             // spectrum entries per output field, all curves
     int64_t max_periods = 0;            // the longest curve spectrum
     std::vector<int64_t> grid_pbase;    // grid k's periods: [grid_pbase[k], grid_pbase[k + 1])
+    std::vector<int64_t> spec_off;      // host: per-curve spectrum offsets (n_curves + 1)
     const int64_t* d_spec_off = nullptr;    // device: per-curve spectrum offsets (n_curves + 1)
     const int64_t* d_grid_base = nullptr;   // device: per-curve first period of its grid
     int n_items_mode[kModes] = {0, 0, 0};
@@ -966,6 +967,7 @@ int do_prepare(BlsEngine* e, const BlsGrid* grids, int n_grids, const int32_t* g
     e->spec_total = spec_total;
     e->max_periods = max_periods;
     e->grid_pbase = pbase;
+    e->spec_off = spec_off;
     e->d_spec_off = dspec;
     e->d_grid_base = dgbase;
     BlsBatchInfo& in = e->info;
@@ -991,7 +993,9 @@ int do_prepare(BlsEngine* e, const BlsGrid* grids, int n_grids, const int32_t* g
 
 // Enqueue one search (both accumulation modes) on `st`.
 int enqueue_search(BlsEngine* e, cudaStream_t st) {
-    CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, kModes * sizeof(int32_t), st), "reset work counters");
+    // the work counters (words 0..kModes-1) and the error flag (word 8): every
+    // search starts clean, so BLS_E_DEVICE reports this search's descriptors only
+    CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, 64, st), "reset work counters and error flag");
     for (int m = 0; m < kModes; ++m) {
         if (e->args[m].n_items <= 0) continue;
         CUDA_TRY(launch_search(e->args[m], m, e->ctas_mode[m], e->smem_mode[m], st),
@@ -1774,6 +1778,32 @@ int bls_download(BlsEngine* e, double* out, void* stream) {
     const size_t bytes = sizeof(double) * kFields * (size_t)e->spec_total;
     if (bytes) CUDA_TRY(cudaMemcpyAsync(out, e->d_out.p, bytes, cudaMemcpyDeviceToHost, st),
                         "download outputs");
+    return check_device_flag(e, st);
+}
+
+int bls_download_curves(BlsEngine* e, const int32_t* curve_ids, int32_t n_ids, double* out,
+                        void* stream) {
+    if (!e || (n_ids > 0 && (!curve_ids || !out)) || n_ids < 0)
+        return fail(BLS_E_INVALID, "engine, curve ids and output are required");
+    if (!e->prepared) return fail(BLS_E_STATE, "bls_download_curves before bls_prepare");
+    for (int32_t k = 0; k < n_ids; ++k)
+        if (curve_ids[k] < 0 || curve_ids[k] >= e->n_curves)
+            return fail(BLS_E_INVALID, "curve id %d outside the prepared batch of %d curves",
+                        (int)curve_ids[k], e->n_curves);
+    cudaSetDevice(e->device);
+    cudaStream_t st = pick(e, stream);
+    const double* d = e->d_out.as<double>();
+    size_t w = 0;
+    for (int32_t k = 0; k < n_ids; ++k) {
+        const int64_t b = e->spec_off[curve_ids[k]], len = e->spec_off[curve_ids[k] + 1] - b;
+        for (int f = 0; f < kFields; ++f) {
+            if (len > 0)
+                CUDA_TRY(cudaMemcpyAsync(out + w, d + (size_t)f * e->spec_total + b,
+                                         sizeof(double) * (size_t)len, cudaMemcpyDeviceToHost, st),
+                         "download a curve's field");
+            w += (size_t)len;
+        }
+    }
     return check_device_flag(e, st);
 }
 

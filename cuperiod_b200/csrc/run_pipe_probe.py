@@ -1,5 +1,5 @@
-"""Run the pipe-rate probe (libbls_probe.so, built from pipe_probe.cu by the
-Makefile) on the current CUDA device and print one line per probe: name,
+"""Run the pipe-rate probe (libbls_probe.so, built from pipe_probe.cu by
+`make -C cuperiod_b200/csrc probe`) on the current CUDA device and print one line per probe: name,
 operations per SM clock for a whole SM, and the SM clock in MHz seen during it.
 
 These rates are the denominators of the engine's SM-pipe roofline (shared-memory

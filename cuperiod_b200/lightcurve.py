@@ -102,6 +102,23 @@ class LightCurve:
             mask &= np.isfinite(self.error) & (self.error > 0.0)
         return mask
 
+    def unusable_reason(self) -> str | None:
+        """Why the errors leave no usable point, or ``None`` when they do not
+        (lightcurve.py:306-326).  ``finite`` drops every point whose error is
+        non-finite or ``<= 0``, so a placeholder error column (all 0, -1 or NaN)
+        empties the curve; this names that cause.  ``None`` when there are no
+        errors, when a point survives, or when no point has a finite time and
+        value (a different problem, left to the caller)."""
+        if self.error is None:
+            return None
+        data = np.isfinite(self.time) & np.isfinite(self.value)
+        n_data = int(np.count_nonzero(data))
+        if n_data == 0 or self._usable().any():
+            return None
+        return (f"none of the {n_data} points with a finite time and value has a usable "
+                "error (all are zero, negative or non-finite), so every point would be "
+                "dropped; drop the error column (error=None) to run unweighted")
+
     def finite(self) -> "LightCurve":
         """Drop non-finite points and non-positive errors (lightcurve.py:240-255)."""
         mask = self._usable()
@@ -222,6 +239,21 @@ class MultiBandLightCurve:
         """Each band's non-finite points removed (lightcurve.py:520-524)."""
         return MultiBandLightCurve({k: lc.finite() for k, lc in self.bands.items()}, self.meta)
 
+    def unusable_reason(self) -> str | None:
+        """Why the errors leave no usable point in any band, or ``None``
+        (lightcurve.py:526-542): each band whose error column is unusable is
+        named, and only when no band keeps a point."""
+        reasons: dict[str, str] = {}
+        for name, lc in self.bands.items():
+            reason = lc.unusable_reason()
+            if reason is not None:
+                reasons[name] = reason
+            elif lc._usable().any():
+                return None
+        if not reasons:
+            return None
+        return "; ".join(f"band {name!r}: {why}" for name, why in reasons.items())
+
     def stacked(self):
         """All bands in ascending time: ``(time, value, error or None, band)``;
         ``error`` is None when a band has none (lightcurve.py:544-575)."""
@@ -243,4 +275,15 @@ class MultiBandLightCurve:
         return time[order], value[order], None if error is None else error[order], band[order]
 
 
-__all__ = ["Domain", "LightCurve", "MultiBandLightCurve"]
+def raise_if_unusable(data: "LightCurve | MultiBandLightCurve", label: str) -> None:
+    """Raise ``InsufficientDataError(f"{label}: {reason}")`` when an unusable error
+    column would empty ``data`` (lightcurve.py:625-646).  Called before a grid is
+    built, so the cause is named instead of surfacing as "no usable time
+    baseline" from the emptied curve."""
+    from .errors import InsufficientDataError
+    reason = data.unusable_reason()
+    if reason is not None:
+        raise InsufficientDataError(f"{label}: {reason}")
+
+
+__all__ = ["Domain", "LightCurve", "MultiBandLightCurve", "raise_if_unusable"]

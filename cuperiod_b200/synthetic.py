@@ -5,9 +5,10 @@ cadences, lengths and value distributions:
 
 * :func:`batched_curves` -- light curves of N ~ U[500, 20000] points over a 27 d
   baseline at 2-minute cadence with a 1 d gap in the middle and 5% random
-  dropouts; flux 1 + N(0, sigma), sigma log-uniform in [2e-4, 5e-3]; half of
-  them carry box transits (depth log-uniform [1e-4, 1e-2], period log-uniform
-  [0.5, 13] d, duration U[0.02, 0.25] d); unit errors.  Searched over 50,000
+  dropouts; FP32 flux 1 + N(0, sigma), sigma log-uniform in [2e-4, 5e-3]; half
+  of them carry box transits (depth log-uniform [1e-4, 1e-2], period log-uniform
+  [0.5, 13] d, duration U[0.02, 0.25] d); no errors (one weight per curve), or
+  per-point errors sigma x U(0.7, 1.4).  Searched over 50,000
   log-spaced periods in [0.3, 13] d with the default 8 durations per segment.
 * :func:`single_curve` -- 2000 points uniform over 90 d, a 2e-3 transit at 3.7 d
   lasting 0.1 d, 1e-3 noise, unit errors; 10,000 log periods in [0.5, 30] d with
@@ -52,8 +53,12 @@ def _box(t, rng, period, duration, depth, y):
     y[np.mod(t - t0, period) < duration] -= depth
 
 
-def batched_curves(n_curves: int, *, seed: int = 0, n_range=(500, 20000)) -> list[Curve]:
-    """The batched workload's light curves (see the module docstring)."""
+def batched_curves(n_curves: int, *, seed: int = 0, n_range=(500, 20000),
+                   weights: str = "uniform") -> list[Curve]:
+    """The batched workload's light curves (see the module docstring).  Flux is
+    rounded to FP32 (survey photometry is stored in single precision).
+    ``weights="hetero"`` gives every point an error sigma x U(0.7, 1.4) (per-point
+    photometric errors) instead of none."""
     rng = np.random.default_rng(seed)
     cadence = 2.0 / 1440.0
     base = np.arange(0.0, 27.0, cadence)
@@ -73,7 +78,11 @@ def batched_curves(n_curves: int, *, seed: int = 0, n_range=(500, 20000)) -> lis
             depth = 10.0 ** rng.uniform(-4.0, -2.0)
             _box(keep, rng, period, duration, depth, y)
             transit = (period, duration, depth)
-        out.append(Curve(keep + 2460000.0, y, None, transit))
+        dy = None
+        if weights == "hetero":
+            dy = sigma * rng.uniform(0.7, 1.4, keep.size)
+        y = y.astype(np.float32).astype(np.float64)
+        out.append(Curve(keep + 2460000.0, y, dy, transit))
     return out
 
 

@@ -68,7 +68,7 @@ enum {
     BLS_E_CUDA = 2,         /* CUDA runtime failure */
     BLS_E_RESOURCE = 3,     /* a segment too wide for shared memory (BackendUnavailableError) */
     BLS_E_NOMEM = 4,        /* device or pinned host allocation failed */
-    BLS_E_DEVICE = 5,       /* a kernel reported an impossible work descriptor */
+    BLS_E_DEVICE = 5,       /* a kernel of the latest search met an impossible work descriptor */
     BLS_E_STATE = 6         /* call out of order (e.g. launch before prepare) */
 };
 
@@ -211,6 +211,14 @@ int bls_time_launches(BlsEngine* engine, int32_t reps, double* ms_per_launch, vo
  * f < BLS_N_FIELDS, c < n_curves, p < n_periods (grid order); after
  * bls_prepare_grids, out[f * spectrum + spec(c) + p].  Waits for the stream. */
 int bls_download(BlsEngine* engine, double* out, void* stream);
+
+/* No counterpart in the reference (its per-curve calls return whole spectra).
+ * Copy every field of the listed curves of the prepared batch: for each id in
+ * turn, its BLS_N_FIELDS fields of its own spectrum length, field after field
+ * (one grid: out[(k * BLS_N_FIELDS + f) * n_periods + p]).  Ids outside the
+ * batch are refused (BLS_E_INVALID).  Waits for the stream. */
+int bls_download_curves(BlsEngine* engine, const int32_t* curve_ids, int32_t n_ids, double* out,
+                        void* stream);
 
 /* Device address of the output fields (layout as bls_download), valid until the
  * next bls_prepare. */

@@ -2,8 +2,11 @@
  * TEST INFRASTRUCTURE ONLY -- the CPU oracle of the BLS parity tests.
  *
  * A plain-C restatement of cuPeriod's numba box-least-squares kernel
- * (src/cuperiod/methods/_bls_core.py:341-462) in its exact, unscreened form
- * (_bls_search_numba(..., screen=False), _bls_core.py:468-500).  Every
+ * (src/cuperiod/methods/_bls_core.py:341-462): its exact, unscreened form
+ * (_bls_search_numba(..., screen=False), _bls_core.py:468-500) is the parity
+ * checker, and its screened form (screen=True, the reference's default CPU
+ * path, _bls_core.py:315-329, 395-440), which chooses the same box bit for bit,
+ * is the timed CPU baseline.  Every
  * operation keeps the reference's order and IEEE rounding: the translation unit
  * is built with -ffp-contract=off (no fused multiply-add) and without fast-math,
  * like numba's fastmath=False, so the phase fold, the bin sums, the cumulative
@@ -62,6 +65,8 @@ typedef struct {
     int64_t n_points, n_periods, n_dur, oversample, width;
     double bin_duration, sum_y, sum_ivar, t_min, ivar_floor;
     int obj_flag;
+    int screened;           /* 1: the reference's two-pass screened sweep */
+    double inv_a, inv_s, slack;     /* its normalisations and slack */
     double* out;
     atomic_long next;       /* next unclaimed period block */
     atomic_int failed;
@@ -69,8 +74,17 @@ typedef struct {
 
 #define PERIOD_BLOCK 16
 
-/* One trial period: _bls_core.py:357-460 with screen=False. */
-static void search_period(const search_args* a, int64_t pidx, double* my, double* mi)
+/* One trial period: _bls_core.py:357-460 (num, den: the screen's per-start
+ * bounds, used when a->screened).  Built twice, for AVX2 and for any x86-64,
+ * and chosen at load time: the vector build runs the screen's elementwise first
+ * pass several points at a time, as the reference's JIT-compiled loop does on
+ * the host CPU; every operation still rounds on its own (no contraction), so
+ * both builds give the same bits. */
+#if defined(__x86_64__)
+__attribute__((target_clones("avx2", "default")))
+#endif
+static void search_period(const search_args* a, int64_t pidx, double* my, double* mi,
+                          double* num, double* den)
 {
     const int64_t n_periods = a->n_periods, width = a->width, oversample = a->oversample;
     const double bin_duration = a->bin_duration, sum_y = a->sum_y, sum_ivar = a->sum_ivar;
@@ -102,6 +116,49 @@ static void search_period(const search_args* a, int64_t pidx, double* my, double
     }
     double loc = -INFINITY;
     int64_t ln = 0, ld = 0;
+    if (a->screened) {                                    /* screened sweep, 389-440 */
+        const double ybar = sum_ivar > 0.0 ? sum_y / sum_ivar : 0.0;
+        const double inv_a = a->inv_a, inv_s = a->inv_s, slack = a->slack;
+        double best_t2 = 0.0, best_den = 1.0;
+        for (int64_t di = 0; di < a->n_dur; ++di) {
+            const int64_t d = a->dur_bins[di];
+            if (d < 1 || d >= n_bins) continue;
+            const int64_t m = n_bins - d + 1;
+            for (int64_t n = 0; n < m; ++n) {             /* pass 1: optimistic bounds */
+                const double y_in = my[n + d] - my[n];
+                const double iv_in = mi[n + d] - mi[n];
+                const double iv_out = sum_ivar - iv_in;
+                const double t = (y_in - ybar * iv_in) * inv_a;
+                const double t_hi = fabs(t) + slack;
+                double dn = (iv_in * inv_s) * (iv_out * inv_s);
+                if (a->obj_flag != 0) dn = dn * (iv_out * inv_s);
+                const int ok = (iv_in >= ivar_floor) & (iv_out >= ivar_floor) & (t <= slack);
+                num[n] = ok ? t_hi * t_hi : -1.0;
+                den[n] = ok ? dn : 1.0;
+            }
+            for (int64_t n = 0; n < m; ++n) {             /* pass 2: exact where it can win */
+                if (num[n] * best_den < best_t2 * den[n]) continue;
+                const double y_in = my[n + d] - my[n];
+                const double iv_in = mi[n + d] - mi[n];
+                const double iv_out = sum_ivar - iv_in;
+                if (iv_in < ivar_floor || iv_out < ivar_floor) continue;
+                const double yin = y_in / iv_in;
+                const double yout = (sum_y - y_in) / iv_out;
+                if (yout < yin) continue;
+                const double depth = yout - yin;
+                double obj;
+                if (a->obj_flag == 0) obj = depth / sqrt(1.0 / iv_in + 1.0 / iv_out);
+                else obj = 0.5 * iv_in * depth * depth;
+                if (obj > loc) {
+                    loc = obj; ln = n; ld = d;
+                    double t_lo = fabs((y_in - ybar * iv_in) * inv_a) - slack;
+                    if (!(t_lo > 0.0)) t_lo = 0.0;
+                    best_t2 = t_lo * t_lo;
+                    best_den = den[n];
+                }
+            }
+        }
+    } else
     for (int64_t di = 0; di < a->n_dur; ++di) {           /* exact sweep, 395-440 */
         const int64_t d = a->dur_bins[di];
         if (d < 1 || d >= n_bins) continue;
@@ -151,30 +208,37 @@ static void* search_worker(void* arg)
     search_args* a = (search_args*)arg;
     double* my = (double*)malloc(sizeof(double) * (size_t)a->width);
     double* mi = (double*)malloc(sizeof(double) * (size_t)a->width);
-    if (!my || !mi) {
+    double* num = (double*)malloc(sizeof(double) * (size_t)a->width);
+    double* den = (double*)malloc(sizeof(double) * (size_t)a->width);
+    if (!my || !mi || !num || !den) {
         atomic_store(&a->failed, 1);
     } else {
         for (;;) {
             const int64_t p0 = atomic_fetch_add(&a->next, PERIOD_BLOCK);
             if (p0 >= a->n_periods) break;
             const int64_t p1 = p0 + PERIOD_BLOCK < a->n_periods ? p0 + PERIOD_BLOCK : a->n_periods;
-            for (int64_t p = p0; p < p1; ++p) search_period(a, p, my, mi);
+            for (int64_t p = p0; p < p1; ++p) search_period(a, p, my, mi, num, den);
         }
     }
     free(my);
     free(mi);
+    free(num);
+    free(den);
     return NULL;
 }
 
 /* The box search over every period (the numba kernel's prange loop, 356). The
  * periods are independent, so n_threads workers share them; the result does
- * not depend on the thread count. */
-int bls_oracle_search(const double* tau, const double* yw, const double* wv, int64_t n_points,
-                      const double* periods, int64_t n_periods,
-                      const int64_t* dur_bins, int64_t n_dur,
-                      double bin_duration, int64_t oversample, int64_t width,
-                      double sum_y, double sum_ivar, double t_min, int obj_flag,
-                      double ivar_floor, double* out, int n_threads)
+ * not depend on the thread count.  screened = 0 is screen=False; screened = 1
+ * runs the reference's screen with its normalisations inv_a = 1/sum|y*ivar|,
+ * inv_s = 1/sum_ivar and slack (_bls_core.py:484-491). */
+int bls_oracle_search_screened(const double* tau, const double* yw, const double* wv,
+                               int64_t n_points, const double* periods, int64_t n_periods,
+                               const int64_t* dur_bins, int64_t n_dur,
+                               double bin_duration, int64_t oversample, int64_t width,
+                               double sum_y, double sum_ivar, double t_min, int obj_flag,
+                               double ivar_floor, int screened, double inv_a, double inv_s,
+                               double slack, double* out, int n_threads)
 {
     if (width < 2 || n_periods < 0 || n_points < 0) return 1;
     search_args a = {
@@ -182,7 +246,8 @@ int bls_oracle_search(const double* tau, const double* yw, const double* wv, int
         .n_points = n_points, .n_periods = n_periods, .n_dur = n_dur,
         .oversample = oversample, .width = width, .bin_duration = bin_duration,
         .sum_y = sum_y, .sum_ivar = sum_ivar, .t_min = t_min, .ivar_floor = ivar_floor,
-        .obj_flag = obj_flag, .out = out,
+        .obj_flag = obj_flag, .screened = screened != 0, .inv_a = inv_a, .inv_s = inv_s,
+        .slack = slack, .out = out,
     };
     atomic_init(&a.next, 0);
     atomic_init(&a.failed, 0);
@@ -197,6 +262,19 @@ int bls_oracle_search(const double* tau, const double* yw, const double* wv, int
     search_worker(&a);
     for (int i = 0; i < started; ++i) pthread_join(th[i], NULL);
     return atomic_load(&a.failed) ? 2 : 0;
+}
+
+/* The unscreened search (_bls_search_numba(..., screen=False)): the parity checker. */
+int bls_oracle_search(const double* tau, const double* yw, const double* wv, int64_t n_points,
+                      const double* periods, int64_t n_periods,
+                      const int64_t* dur_bins, int64_t n_dur,
+                      double bin_duration, int64_t oversample, int64_t width,
+                      double sum_y, double sum_ivar, double t_min, int obj_flag,
+                      double ivar_floor, double* out, int n_threads)
+{
+    return bls_oracle_search_screened(tau, yw, wv, n_points, periods, n_periods, dur_bins, n_dur,
+                                      bin_duration, oversample, width, sum_y, sum_ivar, t_min,
+                                      obj_flag, ivar_floor, 0, 0.0, 0.0, INFINITY, out, n_threads);
 }
 
 /* ---- joint multi-band search ------------------------------------------------

@@ -3,7 +3,8 @@
 A restatement of cuPeriod's BLS path on the CPU: the host-side steps in numpy
 (each function cites the reference file:line it follows) and the per-period box
 search in plain C (``bls_oracle.c``, the numba kernel of
-``src/cuperiod/methods/_bls_core.py:341-462`` evaluated without its screen).
+``src/cuperiod/methods/_bls_core.py:341-462``: without its screen as the parity
+checker, with it as the timed CPU baseline).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
 may import this module, and only as the reference results are compared with or as
@@ -29,6 +30,10 @@ _LIB_PATH = os.path.join(_HERE, "liboracle_bls.so")
 _lib: ctypes.CDLL | None = None
 
 F64_EPS = float(np.finfo(np.float64).eps)
+# The numba sweep's screen (_bls_core.py:67-72): slack in units of eps of
+# sum|y*ivar|, and the range of sums inside which its normalisation is exact.
+SCREEN_SLACK_EPS = 256.0
+SCREEN_SCALE_RANGE = (1e-150, 1e150)
 OUTPUT_NAMES = ("power", "depth", "depth_err", "depth_snr", "duration",
                 "transit_time", "log_likelihood")
 SEGMENT_FIELDS = ("period", "power", "depth", "depth_snr", "duration", "transit_time")
@@ -51,6 +56,9 @@ def _load() -> ctypes.CDLL:
         lib.bls_oracle_search.argtypes = [p, p, p, i64, p, i64, p, i64, d, i64, i64,
                                           d, d, d, i32, d, p, i32]
         lib.bls_oracle_search.restype = i32
+        lib.bls_oracle_search_screened.argtypes = [p, p, p, i64, p, i64, p, i64, d, i64, i64,
+                                                   d, d, d, i32, d, i32, d, d, d, p, i32]
+        lib.bls_oracle_search_screened.restype = i32
         lib.bls_oracle_fold_bins.argtypes = [p, i64, d, d, i64, p]
         lib.bls_oracle_fold_bins.restype = i32
         lib.bls_oracle_joint.argtypes = [p, p, p, p, i64, p, p, p, p, i64, p, i64, d, i64,
@@ -125,8 +133,12 @@ def objective_flag(objective: str) -> int:
 
 
 def search(t, y, ivar, periods, *, bin_duration, dur_bins, oversample, width,
-           obj_flag, n_threads: int | None = None) -> dict[str, np.ndarray]:
-    """``_bls_search_numba(..., screen=False)``, ``_bls_core.py:468-500``."""
+           obj_flag, n_threads: int | None = None,
+           screen: bool = False) -> dict[str, np.ndarray]:
+    """``_bls_search_numba(..., screen=screen)``, ``_bls_core.py:468-500``:
+    ``screen=False`` (the default here) evaluates every box, the parity
+    checker; ``screen=True`` is the reference's default CPU path, which
+    chooses the same boxes bit for bit and is the timed CPU baseline."""
     lib = _load()
     t = np.ascontiguousarray(t, dtype=np.float64)
     ivar = np.ascontiguousarray(ivar, dtype=np.float64)
@@ -140,10 +152,17 @@ def search(t, y, ivar, periods, *, bin_duration, dur_bins, oversample, width,
     out = np.empty((7, per.size), dtype=np.float64)
     if n_threads is None:
         n_threads = os.cpu_count() or 1
-    rc = lib.bls_oracle_search(
+    sum_abs = float(np.abs(yw).sum())
+    lo, hi = SCREEN_SCALE_RANGE
+    if screen and lo <= sum_abs <= hi and lo <= sum_ivar <= hi:
+        inv_a, inv_s, slack = 1.0 / sum_abs, 1.0 / sum_ivar, SCREEN_SLACK_EPS * F64_EPS
+    else:
+        inv_a, inv_s, slack = 0.0, 0.0, math.inf
+    rc = lib.bls_oracle_search_screened(
         _ptr(tau), _ptr(yw), _ptr(ivar), tau.size, _ptr(per), per.size, _ptr(db), db.size,
         float(bin_duration), int(oversample), int(width), sum_y, sum_ivar, t_min,
-        int(obj_flag), ivar_floor(int(tau.size), sum_ivar), _ptr(out), int(n_threads))
+        int(obj_flag), ivar_floor(int(tau.size), sum_ivar), int(bool(screen)), inv_a, inv_s,
+        slack, _ptr(out), int(n_threads))
     if rc != 0:
         raise RuntimeError(f"oracle search failed ({rc})")
     return dict(zip(OUTPUT_NAMES, out))
@@ -181,8 +200,9 @@ def padded_cumsums(t, y, dy, period: float, durations, oversample: int):
 
 
 def bls_power(t, y, dy, periods, durations, oversample: int, *, objective: str = "snr",
-              n_threads: int | None = None) -> dict[str, np.ndarray]:
-    """``bls_power(..., backend="numba")``, ``_bls_core.py:882-1028``."""
+              n_threads: int | None = None, screen: bool = False) -> dict[str, np.ndarray]:
+    """``bls_power(..., backend="numba")``, ``_bls_core.py:882-1028`` (``screen``
+    as in :func:`search`)."""
     obj_flag = objective_flag(objective)
     periods_host = np.ascontiguousarray(periods, dtype=np.float64)
     if periods_host.size == 0:
@@ -193,7 +213,7 @@ def bls_power(t, y, dy, periods, durations, oversample: int, *, objective: str =
     th, yh, ih = host_inputs(t, y, dy)
     out = search(th, yh, ih, periods_host, bin_duration=spec.bin_duration,
                  dur_bins=spec.dur_bins, oversample=oversample, width=spec.width,
-                 obj_flag=obj_flag, n_threads=n_threads)
+                 obj_flag=obj_flag, n_threads=n_threads, screen=screen)
     out["period"] = periods_host
     return out
 

@@ -25,7 +25,7 @@ def _run(args, env_extra=None):
                           cwd=ROOT)
 
 
-@pytest.mark.parametrize("args", [["--curves", "16"], ["--workload", "tls", "--tls-curves", "2"],
+@pytest.mark.parametrize("args", [["--curves", "16", "--ref-curves", "2"], ["--workload", "tls", "--tls-curves", "2"],
                                   ["--workload", "multiband-shared", "--stars", "2"]])
 def test_reference_arm_prints_one_contract_line(args):
     res = _run(args)
@@ -42,6 +42,6 @@ def test_reference_arm_prints_one_contract_line(args):
 
 
 def test_reference_arm_runs_on_rank_0_only():
-    res = _run(["--curves", "16"], {"RANK": "1", "WORLD_SIZE": "2"})
+    res = _run(["--curves", "16", "--ref-curves", "2"], {"RANK": "1", "WORLD_SIZE": "2"})
     assert res.returncode == 0, res.stderr[-2000:]
     assert not [l for l in res.stdout.splitlines() if l.startswith("{")]

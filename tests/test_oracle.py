@@ -23,6 +23,20 @@ def test_oracle_bit_exact_on_golden(meta_arrays):
     assert np.array_equal(got, a["out"], equal_nan=True)
 
 
+@pytest.mark.parametrize("meta_arrays", kernel_golden(), ids=lambda c: c[0]["name"])
+def test_screened_oracle_bit_exact_on_golden(meta_arrays):
+    """The screened sweep (the reference's default CPU path, timed as the CPU
+    baseline) chooses the unscreened sweep's boxes bit for bit, as the
+    reference's own test asserts of its numba kernel (tests/test_bls.py:397-424)."""
+    meta, a = meta_arrays
+    with np.errstate(over="ignore", divide="ignore", invalid="ignore"):
+        out = oracle.bls_power(a["t"], a["y"], a["dy"], a["periods"], a["durations"],
+                               meta["oversample"], objective=meta["objective"], n_threads=4,
+                               screen=True)
+    got = np.stack([out[f] for f in FIELDS])
+    assert np.array_equal(got, a["out"], equal_nan=True)
+
+
 def _method_cases():
     index = json.load(open(os.path.join(GOLDEN, "method_cases.json")))
     z = np.load(os.path.join(GOLDEN, "method_cases.npz"))

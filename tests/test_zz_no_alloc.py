@@ -52,15 +52,20 @@ def test_no_alloc_matches_the_allocating_path_twice(lib):
         eng.prepare(grid, curves)
         eng.launch()
         ref = eng.download_best()
-        free = []
+        torch.cuda.synchronize()
+        # every buffer of the allocating path exists now; from here on neither the
+        # device's free memory nor torch's allocator may move, the first call (which
+        # looks up the static array's address) included
+        free0 = torch.cuda.mem_get_info()[0]
+        torch0 = torch.cuda.memory_allocated()
         for _ in range(2):                      # the counters must be zeroed again
             got = eng.launch_best_noalloc()
             torch.cuda.synchronize()
-            free.append(torch.cuda.mem_get_info()[0])
+            assert torch.cuda.mem_get_info()[0] == free0
+            assert torch.cuda.memory_allocated() == torch0
             np.testing.assert_array_equal(got[0], ref[0])
             for g, r in zip(got[1:], ref[1:]):
                 np.testing.assert_allclose(g, r, rtol=RTOL, atol=0.0)
-        assert free[0] == free[1]               # the second call allocated nothing
     finally:
         eng.close()
 
