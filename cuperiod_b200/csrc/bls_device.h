@@ -91,6 +91,13 @@ struct CurveDesc {
     // which grew with the box instead of its square root).
     double center;          // the per-point centring, reference units
     double center_frac;     // ybar*ivar*2^e_r minus that whole number (|.| <= 1/2)
+    // WIDE: the exact sums of every point's quantised centred flux*weight and
+    // weight.  A box's outside sums are these minus its inside sums, so a box
+    // holding every point has exactly zero weight outside and fails the floor
+    // test as the reference's does (sum_ivar minus a quantised inside sum would
+    // leave the quantisation residual, far above the floor).
+    long long rq_total;
+    long long iq_total;
 };
 
 struct WorkItem {

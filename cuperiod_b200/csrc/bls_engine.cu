@@ -399,6 +399,7 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
     }
     int e_i = 0;
     double i_total = 0.0;
+    long long rq_total = 0, iq_total = 0;
     // per-point weights within a factor 2^8 of each other: 38-bit fixed point
     // (the smallest weight keeps >= 2^28 steps, a relative 2^-29)
     double min_i = max_i;
@@ -410,7 +411,7 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
         std::frexp(max_r, &kr);            // max_r < 2^kr
         std::frexp(max_i, &ki);
         const int e_rw = 37 - kr, e_iw = 37 - ki;       // |v| < 2^37
-        int64_t total = 0;
+        int64_t total = 0, rtotal = 0;
         for (int64_t j = 0; j < n; ++j) {
             const int64_t m = point_slot(j, n);
             const long long rq = std::llrint(std::ldexp(r[j], e_rw));
@@ -418,10 +419,13 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
             std::memcpy(&r64[m], &rq, sizeof(rq));
             std::memcpy(&iv64[m], &iq, sizeof(iq));
             total += iq;
+            rtotal += rq;
         }
         e_r = e_rw;
         e_i = e_iw;
         i_total = (double)total;
+        rq_total = rtotal;
+        iq_total = total;
     } else if (!uniform) {
         // per-point weights: FP64 values scaled by powers of two (exact)
         if (max_i > 0.0 && std::isfinite(max_i)) {
@@ -453,6 +457,8 @@ void pack_curve(const BlsCurves* cv, int c, int64_t off, double* tau, uint32_t* 
     d.e_i = e_i;
     d.center = std::ldexp((double)cq, -e_r);
     d.center_frac = c_frac;
+    d.rq_total = rq_total;
+    d.iq_total = iq_total;
     ch.tau_max = tau_max;
 }
 

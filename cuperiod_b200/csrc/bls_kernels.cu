@@ -161,18 +161,20 @@ __device__ __forceinline__ bool better(double v, int di, int n, double w, int dj
     return di < dj || (di == dj && n < m);
 }
 
-// Exact sums of one box, in the reference's units.
+// Sums of one box inside and outside, in the reference's units: the reference
+// forms the outside as sum_y - y_in and sum_ivar - iv_in; WIDE curves take them
+// from the exact quantised totals instead (CurveDesc::rq_total).
 struct BoxSums {
-    double y_in, iv_in;
+    double y_in, iv_in, y_out, iv_out;
 };
 
 // The reference's objective of one box (_bls_core.py:410-426); -inf when the box
 // is not admissible.
 __device__ __forceinline__ double box_objective(const BoxSums& s, const CurveDesc& c, int obj) {
-    const double iv_out = c.sum_ivar - s.iv_in;
+    const double iv_out = s.iv_out;
     if (!(s.iv_in >= c.ivar_floor) || !(iv_out >= c.ivar_floor)) return -CUDART_INF;
     const double yin = s.y_in / s.iv_in;
-    const double yout = (c.sum_y - s.y_in) / iv_out;
+    const double yout = s.y_out / iv_out;
     if (yout < yin) return -CUDART_INF;
     const double depth = yout - yin;
     if (obj == 0) return depth / sqrt(1.0 / s.iv_in + 1.0 / iv_out);
@@ -378,14 +380,20 @@ __device__ __forceinline__ BoxSums box_sums(uint32_t hq, const CurveDesc& cv, in
         b.y_in = ldexp((double)(prefix_r(hq, n + d) - prefix_r(hq, n)), -cv.e_r) +
                  cv.center * cnt;
     } else if (MODE == MODE_WIDE) {
-        b.iv_in = ldexp((double)(wide_prefix_i(hq, n + d) - wide_prefix_i(hq, n)), -cv.e_i);
-        b.y_in = ldexp((double)(wide_prefix_r(hq, n + d) - wide_prefix_r(hq, n)), -cv.e_r) +
-                 cv.ybar * b.iv_in;
+        const long long qi = wide_prefix_i(hq, n + d) - wide_prefix_i(hq, n);
+        const long long qr = wide_prefix_r(hq, n + d) - wide_prefix_r(hq, n);
+        b.iv_in = ldexp((double)qi, -cv.e_i);
+        b.y_in = ldexp((double)qr, -cv.e_r) + cv.ybar * b.iv_in;
+        b.iv_out = ldexp((double)(cv.iq_total - qi), -cv.e_i);
+        b.y_out = ldexp((double)(cv.rq_total - qr), -cv.e_r) + cv.ybar * b.iv_out;
+        return b;
     } else {
         const uint32_t r1 = hq + (uint32_t)(n + d) * 16u, r0 = hq + (uint32_t)n * 16u;
         b.iv_in = ldexp(ld_f64(r1 + 8) - ld_f64(r0 + 8), -cv.e_i);
         b.y_in = ldexp(ld_f64(r1) - ld_f64(r0), -cv.e_r) + cv.ybar * b.iv_in;
     }
+    b.iv_out = cv.sum_ivar - b.iv_in;
+    b.y_out = cv.sum_y - b.y_in;
     return b;
 }
 
@@ -993,9 +1001,9 @@ __global__ void __launch_bounds__(kThreads, MODE == MODE_UNIFORM ? 3 : 2)
                 const int vn = s.win_n[q];
                 const int d = s.dur[s.win_di[q]];
                 const BoxSums b = box_sums<MODE>(hq, cv, vn, d);
-                const double iv_out = cv.sum_ivar - b.iv_in;
+                const double iv_out = b.iv_out;
                 const double yin = b.y_in / b.iv_in;
-                const double yout = (cv.sum_y - b.y_in) / iv_out;
+                const double yout = b.y_out / iv_out;
                 const double depth = yout - yin;
                 const double derr = sqrt(1.0 / b.iv_in + 1.0 / iv_out);
                 const double dsnr = depth / derr;

@@ -177,3 +177,31 @@ def test_curve_beyond_the_exact_sums_matches_oracle(engine, weights):
     got = _run(engine, t, y, dy, periods, durations, 10, "snr")
     diag = compare(ref, got, rtol=1e-6, box_agree=0.99)
     assert diag["same_argmax"]
+
+
+@pytest.mark.parametrize("weights", ["uniform", "hetero", "wild"])
+@pytest.mark.parametrize("objective", ["snr", "likelihood"])
+def test_box_holding_every_point_is_not_admissible(engine, objective, weights):
+    # Two short runs of observations a year apart and periods far longer than a
+    # run: at many periods every point folds into a few days of phase, and the
+    # widest boxes hold every point.  Such a box leaves no weight outside and the
+    # reference rejects it (its outside weight is a rounding residual, below the
+    # floor); with per-point weights within 2^8 the engine sums quantised
+    # weights, and an outside weight of sum_ivar minus a quantised inside sum
+    # would leave the quantisation residual -- far above the floor -- and admit it.
+    rng = np.random.default_rng(5)
+    t = np.concatenate([np.sort(rng.uniform(0.0, 3.0, 150)),
+                        np.sort(rng.uniform(365.0, 368.0, 150))]) + 2458000.0
+    y = 1.0 + rng.normal(0.0, 4e-3, t.size)
+    if weights == "uniform":
+        dy = np.full(t.size, 4e-3)
+    elif weights == "hetero":
+        dy = 4e-3 * rng.uniform(0.75, 2.0, t.size)
+    else:
+        dy = 4e-3 * 10.0 ** rng.uniform(-1.5, 1.5, t.size)
+    periods = np.geomspace(20.0, 90.0, 600)
+    durations = np.geomspace(0.4, 4.8, 8)
+    ref = oracle.bls_power(t, y, dy, periods, durations, 10, objective=objective)
+    got = _run(engine, t, y, dy, periods, durations, 10, objective)
+    diag = compare(ref, got, rtol=1e-6, box_agree=0.98)
+    assert diag["same_argmax"]
