@@ -75,6 +75,15 @@ def parse_args():
     p.add_argument("--ref-curves", type=int, default=16,
                    help="batch: curves of the N-stratified sample one reference-arm step "
                         "(and the cpu_baseline) searches on the host cores")
+    p.add_argument("--pruned-steps", type=int, default=2,
+                   help="batch: timed steps of the learned-pruned search of the same batch "
+                        "(0: skip)")
+    p.add_argument("--proposal-weights", default=os.path.join(ROOT, "cuperiod_b200",
+                                                               "proposal_weights.npz"),
+                   help="trained proposal network (cuperiod_b200.proposal_train)")
+    p.add_argument("--ref-gpu-curves", type=int, default=8,
+                   help="batch, --impl reference: N-stratified curves searched by the "
+                        "reference's own GPU kernel (0: skip)")
     p.add_argument("--precision-curves", type=int, default=64,
                    help="batch: N-stratified curves of the timed batch whose spectra are "
                         "compared with the oracle (0: none)")
@@ -85,7 +94,12 @@ def parse_args():
                    help="long-baseline: light curves per rank")
     p.add_argument("--lb-check", type=int, default=2,
                    help="long-baseline: curves checked against the oracle (rank 0)")
-    p.add_argument("--workload", choices=("batch", "long-baseline", "multiband-shared", "tls"),
+    p.add_argument("--catalogue-curves", type=int, default=65536,
+                   help="catalogue: curves per rank (the full sweep is 262144)")
+    p.add_argument("--catalogue-chunk", type=int, default=16384,
+                   help="catalogue: curves per streamed chunk")
+    p.add_argument("--workload", choices=("batch", "long-baseline", "multiband-shared", "tls",
+                                          "catalogue"),
                    default="batch",
                    help="batch: the headline batched search; long-baseline: the 4-year "
                         "precision stress search of --lb-curves curves with an oracle check; "
@@ -230,7 +244,7 @@ def batch_precision(engine, curves, segments, n_check: int, rows=None) -> dict |
     got = engine.download_curves(picks)
     cores = os.cpu_count() or 1
     agree, raw, floored, within, at_best, box_same = 0, [], [], [], [], []
-    bp_agree = 0
+    bp_agree, bp_ties = 0, 0
     all_periods = np.concatenate([p for p, _ in segments])
     t0 = time.perf_counter()
     for j, i in enumerate(picks):
@@ -258,7 +272,15 @@ def batch_precision(engine, curves, segments, n_check: int, rows=None) -> dict |
             pw = np.nan_to_num(ref, nan=0.0, posinf=0.0, neginf=0.0)[order]
             ref_bp = 1.0 / freq[order][oracle.best_index(pw)]
             row_bp = rows[i]["best_period"]
-            bp_agree += int(abs(row_bp - ref_bp) <= 1e-12 * ref_bp)
+            if abs(row_bp - ref_bp) <= 1e-12 * ref_bp:
+                bp_agree += 1
+            else:
+                # two separate peak candidates of exactly equal power: the reference
+                # orders them with numpy's unstable argsort (core/peaks.py:215), the
+                # device ranks the later candidate first
+                fo = freq[order]
+                j_row = int(np.argmin(np.abs(1.0 / fo - row_bp)))
+                bp_ties += int(pw[j_row] == pw[oracle.best_index(pw)])
     return {"curves_checked": len(picks), "argmax_agree": agree,
             "sample": "N-stratified curves of the timed batch (quantiles (j+0.5)/k of N), full grid",
             "rel_power_err_at_best": max(at_best),
@@ -268,6 +290,7 @@ def batch_precision(engine, curves, segments, n_check: int, rows=None) -> dict |
             "periods_within_1e-6_raw": min(within),
             "same_box_frac_min": min(box_same),
             "row_best_period_agree": None if rows is None else bp_agree,
+            "row_best_period_exact_power_ties": None if rows is None else bp_ties,
             "reference": "oracle: the reference's unscreened FP64 numba search restated in C, "
                          "host cores",
             "seconds": round(time.perf_counter() - t0, 1)}
@@ -318,6 +341,89 @@ def long_baseline_check(engine, curves, segments, grid, n_check: int):
     return precision, cpu
 
 
+def pruned_check(engine, curves, segments, grid, packed, plain_best, steps: int,
+                 weights_path: str) -> dict:
+    """The learned-pruned search of the same batch (``cuperiod_b200.proposal``):
+    light curves/s end to end (host arrays in, each curve's best period out: the
+    binning and the network on the tensor cores, the windows built on the host,
+    one engine launch over every curve's windows or, below the confidence
+    threshold, its full grid), agreement of its best period with the timed
+    plain search's, and the plain search timed the same way."""
+    from cuperiod_b200.proposal import Proposer, Weights
+    if not os.path.exists(weights_path):
+        return {"unavailable": "no trained proposal weights at " + os.path.relpath(weights_path, ROOT)}
+    w = Weights.load(weights_path)
+    prop = Proposer(w, segments)
+    host = [(c.t, c.y, c.dy) for c in curves]
+    prop.search(host[:256], engine)                        # warm-up
+    times, res = [], None
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        res = prop.search(host, engine)
+        times.append(time.perf_counter() - t0)
+    plain_times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        engine.prepare(grid, packed)
+        engine.launch()
+        engine.download_best()
+        plain_times.append(time.perf_counter() - t0)
+    n = len(curves)
+    agree = res.best_index == np.asarray(plain_best)
+    conf = res.confident
+    value = n * len(times) / sum(times)
+    plain = n * len(plain_times) / sum(plain_times)
+    has_transit = np.array([c.transit is not None for c in curves])
+    return {"value": value, "unit": UNIT, "agreement": float(agree.mean()),
+            "agreement_transit_curves": float(agree[has_transit].mean()),
+            "agreement_noise_curves": float(agree[~has_transit].mean()),
+            "confident_frac": float(conf.mean()),
+            "confident_agreement": float(agree[conf].mean()) if conf.any() else None,
+            "periods_searched_frac": res.periods_searched / float(n * grid.n_periods),
+            "plain_best_e2e": plain, "speedup_vs_plain": value / plain,
+            "threshold": prop.threshold, "k": prop.k, "widen": prop.widen,
+            "training": {k: w.meta.get(k) for k in ("train_curves", "epochs", "val_top1",
+                                                     "val_window_recall", "val_confident_frac",
+                                                     "val_agreement_bound")},
+            "clock": "host wall clock around the synchronous call, both searches"}
+
+
+def ref_gpu_kernel_sample(curves, segments, n_sample: int) -> dict | None:
+    """The reference's own GPU kernel (``bls_block`` compiled from its source for
+    sm_100a, ``oracle/_ref``) on an N-stratified sample of the workload, one curve
+    per call as ``_bls_search_cuda_specs`` runs it (upload, one launch per segment,
+    download), in its FP64 default and its FP32 opt-in: light curves/s by the host
+    clock around each call, and by the device time of its launches alone."""
+    from oracle import ref_gpu
+    if n_sample <= 0 or not ref_gpu.available():
+        return None
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except ImportError:
+        return None
+    picks = stratified_sample(curves, n_sample)
+    out = {"sample": cpu_sample_text(curves, picks).split(", all periods")[0],
+           "kernel": "cuPeriod bls_block (_bls_core.py:505-656), 128 threads per period, "
+                     "one launch per segment, per-curve upload and download"}
+    for precision in ("float64", "float32"):
+        c0 = curves[picks[0]]
+        ref_gpu.search_curve(c0.t, c0.y, np.ones_like(c0.y) if c0.dy is None else c0.dy,
+                             segments[:1], 10, precision=precision)          # warm-up
+        wall, dev = 0.0, 0.0
+        for i in picks:
+            c = curves[i]
+            t0 = time.perf_counter()
+            _, ms = ref_gpu.search_curve(c.t, c.y, np.ones_like(c.y) if c.dy is None else c.dy,
+                                         segments, 10, precision=precision)
+            wall += time.perf_counter() - t0
+            dev += ms / 1000.0
+        out[precision] = {"value": len(picks) / wall, "device_only_value": len(picks) / dev,
+                          "unit": UNIT, "seconds": round(wall, 2)}
+    return out
+
+
 def run_reference(args) -> None:
     if int(os.environ.get("RANK", "0")) != 0:
         return
@@ -330,6 +436,7 @@ def run_reference(args) -> None:
         cpu_reference_step(curves, segments, picks)
     times = [cpu_reference_step(curves, segments, picks) for _ in range(args.steps)]
     value = len(picks) * len(times) / sum(times)
+    ref_gpu = None if lb else ref_gpu_kernel_sample(curves, segments, args.ref_gpu_curves)
     cb = {"value": value, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
           "sample": cpu_sample_text(curves, picks)}
     print(json.dumps({
@@ -344,6 +451,7 @@ def run_reference(args) -> None:
                                         "variant": "plain full grid", "cpu": "host cores"},
         "cpu_baseline": cb,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "ref_gpu_kernel": ref_gpu,
     }), flush=True)
 
 
@@ -437,6 +545,7 @@ def run_ours(args) -> None:
     # the timed batch again, for the precision check of its spectra
     engine.prepare(grid, packed, stream=handle)
     engine.launch(handle)
+    plain_best = engine.download_best(handle)[0]
     torch.cuda.synchronize()
 
     if rank == 0:
@@ -506,6 +615,9 @@ def run_ours(args) -> None:
         elif world == 1:
             out["precision"] = batch_precision(engine, curves, segments, args.precision_curves,
                                                rows)
+            if args.pruned_steps > 0 and args.weights == "uniform":
+                out["pruned"] = pruned_check(engine, curves, segments, grid, packed, plain_best,
+                                             args.pruned_steps, args.proposal_weights)
             out["cpu_baseline"] = cpu_baseline_sample(curves, segments, args.ref_curves)
         print(json.dumps(out), flush=True)
     engine.close()
@@ -909,8 +1021,113 @@ def run_tls_ours(args) -> None:
         dist.destroy_process_group()
 
 
+# ---- the streamed catalogue sweep ------------------------------------------------
+
+CAT_WORKLOAD = ("catalogue sweep: {n} curves streamed from pinned host memory in {chunk}-curve "
+                "chunks, N lognormal (median 3000, 200-60,000), mixed 2-min/27 d and "
+                "30-min/4 yr cadences, 50,000 log periods 0.3-13 d, learned-pruned BLS with a "
+                "full-grid audit of a seeded 1% of confident curves and of every "
+                "low-confidence curve")
+
+
+def run_catalogue(args) -> None:
+    """The catalogue sweep (``cuperiod_b200.catalogue``) of a seeded catalogue:
+    learned-pruned, then plain, over the same pinned arrays; rank 0 reports both
+    (each rank sweeps its own catalogue)."""
+    import torch
+
+    from cuperiod_b200.catalogue import pin, sweep
+    from cuperiod_b200.proposal import Weights
+    from cuperiod_b200.proposal_train import grid_segments
+    from cuperiod_b200.sharding import max_over_ranks
+    from cuperiod_b200.synthetic import catalogue_curves
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    t_gen = time.perf_counter()
+    t, y, off, kind = catalogue_curves(args.catalogue_curves, seed=args.seed + rank)
+    t, y, keep = pin(t, y)
+    t_gen = time.perf_counter() - t_gen
+    segments = grid_segments()
+    w = Weights.load(args.proposal_weights)
+    n = args.catalogue_curves
+    # warm-up: one small chunk through both paths
+    wn = min(n, 512)
+    sweep(t, y, off[:wn + 1], w, segments, chunk=wn, workers=1)
+    sweep(t, y, off[:wn + 1], w, segments, chunk=wn, workers=1, plain=True)
+    torch.cuda.synchronize()
+    pruned = sweep(t, y, off, w, segments, chunk=args.catalogue_chunk, workers=2,
+                   seed=args.seed)
+    plain = sweep(t, y, off, w, segments, chunk=args.catalogue_chunk, workers=2, plain=True)
+    p_s = max_over_ranks(pruned.seconds)
+    q_s = max_over_ranks(plain.seconds)
+    agree_all = float(np.mean(pruned.best_index == plain.best_index))
+    if rank == 0:
+        clocks_mhz = 1965.0
+        n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+        folds = sum(r["folds"] for r in pruned.chunks)
+        boxes = sum(r["boxes"] for r in pruned.chunks)
+        t_atom = folds * 3 / (16.66 * n_sm * clocks_mhz * 1e6)
+        t_fp32 = boxes * 10 / (188.0 * n_sm * clocks_mhz * 1e6)
+        h2d = sum(r["h2d_bytes"] for r in pruned.chunks)
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        value = world * n / p_s
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1,
+            "warmup": 1, "ms_per_step": 1000.0 * p_s, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed: bf16 network (fp32 accumulate); f64 phase, exact int32 bin sums, "
+                     "f32 screen",
+            "data": "synthetic",
+            "config": {"workload": CAT_WORKLOAD.format(n=n, chunk=args.catalogue_chunk),
+                       "curves_per_rank": n, "variant": "learned-pruned + audit",
+                       "long_cadence_frac": float(kind.mean()),
+                       "points": int(off[-1]), "generation_s": round(t_gen, 1)},
+            "pruned": {"value": value, "confident_frac": float(pruned.confident.mean()),
+                       "audited": int(pruned.audited.sum()),
+                       "audit_agreement": pruned.audit_agreement,
+                       "agreement_with_plain_all_curves": agree_all,
+                       "periods_searched_frac": sum(r["periods_searched"] for r in pruned.chunks)
+                       / float(n * 50000)},
+            "plain": {"value": world * n / q_s, "seconds": q_s},
+            "speedup_vs_plain": q_s / p_s,
+            "roofline": {"bound": "hbm", "achieved": h2d / p_s / 1e9, "peak": hbm,
+                         "unit": "GB/s", "frac": h2d / p_s / 1e9 / hbm, "traffic": None,
+                         "note": "host-to-device staging of the chunks; the search is SM-bound"},
+            "sm_roofline": {"bound": "smem_atomic" if t_atom >= t_fp32 else "fp32",
+                            "model_ms": 1000.0 * max(t_atom, t_fp32), "kernel_ms": 1000.0 * p_s,
+                            "frac": max(t_atom, t_fp32) / p_s,
+                            "note": "model at 1965 MHz over the whole sweep wall clock"},
+            "gpu_launches": len(pruned.chunks) * 30,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": n * 32},
+        }), flush=True)
+    del keep
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main() -> None:
     args = parse_args()
+    if args.workload == "catalogue":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the catalogue sweep's "
+                                  "reference is the batch workload's CPU baseline"}))
+            return
+        run_catalogue(args)
+        return
     if args.workload == "tls":
         run_tls_reference(args) if args.impl == "reference" else run_tls_ours(args)
         return

@@ -10,6 +10,13 @@ cadences, lengths and value distributions:
   [0.5, 13] d, duration U[0.02, 0.25] d); no errors (one weight per curve), or
   per-point errors sigma x U(0.7, 1.4).  Searched over 50,000
   log-spaced periods in [0.3, 13] d with the default 8 durations per segment.
+* :func:`proposal_curves` -- training curves of the period-proposal network:
+  the same cadence and noise, 60% with box transits, 40% noise (half with a
+  sinusoid of amplitude log-uniform in [1e-4, 1e-2], period log-uniform in
+  [0.1, 20] d).
+* :func:`catalogue_curves` -- a packed catalogue for the streamed sweep:
+  lognormal point counts (median 3000, 200-60,000), mixed 2-minute / 27 d and
+  30-minute / 4-year cadences, half with box transits.
 * :func:`single_curve` -- 2000 points uniform over 90 d, a 2e-3 transit at 3.7 d
   lasting 0.1 d, 1e-3 noise, unit errors; 10,000 log periods in [0.5, 30] d with
   durations {0.05, 0.08, 0.12, 0.16, 0.2} d and the likelihood objective.
@@ -84,6 +91,75 @@ def batched_curves(n_curves: int, *, seed: int = 0, n_range=(500, 20000),
         y = y.astype(np.float32).astype(np.float64)
         out.append(Curve(keep + 2460000.0, y, dy, transit))
     return out
+
+
+def proposal_curves(n_curves: int, *, seed: int = 0, n_range=(500, 20000)) -> list[Curve]:
+    """Training curves of the period-proposal network: the batched workload's
+    cadence, lengths and noise, with box transits (as there) on 60% of the
+    curves; the other 40% are noise, half of them with a sinusoid of amplitude
+    log-uniform in [1e-4, 1e-2] and period log-uniform in [0.1, 20] d."""
+    rng = np.random.default_rng(seed)
+    cadence = 2.0 / 1440.0
+    base = np.arange(0.0, 27.0, cadence)
+    base = base[(base < 13.0) | (base >= 14.0)]
+    out = []
+    for _ in range(n_curves):
+        keep = base[rng.random(base.size) > 0.05]
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        if keep.size > n:
+            keep = np.sort(rng.choice(keep, n, replace=False))
+        sigma = 10.0 ** rng.uniform(np.log10(2e-4), np.log10(5e-3))
+        y = 1.0 + rng.normal(0.0, sigma, keep.size)
+        transit = None
+        if rng.random() < 0.6:
+            period = 10.0 ** rng.uniform(np.log10(0.5), np.log10(13.0))
+            duration = rng.uniform(0.02, 0.25)
+            depth = 10.0 ** rng.uniform(-4.0, -2.0)
+            _box(keep, rng, period, duration, depth, y)
+            transit = (period, duration, depth)
+        elif rng.random() < 0.5:
+            amp = 10.0 ** rng.uniform(-4.0, -2.0)
+            ps = 10.0 ** rng.uniform(-1.0, np.log10(20.0))
+            y += amp * np.sin(2.0 * np.pi * keep / ps + rng.uniform(0.0, 2.0 * np.pi))
+        out.append(Curve(keep + 2460000.0, y.astype(np.float32).astype(np.float64), None,
+                         transit))
+    return out
+
+
+def catalogue_curves(n_curves: int, *, seed: int = 0):
+    """A catalogue of light curves, packed: ``(t, y, offsets, kind)`` with curve c
+    at ``[offsets[c], offsets[c + 1])`` of the FP64 arrays ``t`` and ``y`` (FP32
+    flux values).  Point counts are lognormal (median 3000, clipped to
+    200-60,000); cadences are mixed: ``kind`` 0 is the batched workload's 2-minute
+    cadence over 27 d (5% dropouts, a 1 d gap), ``kind`` 1 the long-baseline
+    workload's 30-minute cadence over four years (two curves in ten); noise
+    sigma log-uniform in [2e-4, 5e-3]; half carry box transits (depth log-uniform
+    [1e-4, 1e-2], period log-uniform [0.5, 13] d, duration U[0.02, 0.25] d).  A
+    curve's count is capped at its cadence's samples."""
+    rng = np.random.default_rng(seed)
+    short = np.arange(0.0, 27.0, 2.0 / 1440.0)
+    short = short[(short < 13.0) | (short >= 14.0)]
+    long_ = np.arange(60000) * (30.0 / 1440.0)
+    long_ = long_ * (1461.0 / long_[-1])
+    ts, ys, sizes = [], [], np.empty(n_curves, dtype=np.int64)
+    kind = (rng.random(n_curves) < 0.2).astype(np.int8)
+    for c in range(n_curves):
+        base = long_ if kind[c] else short
+        keep = base[rng.random(base.size) > 0.05]
+        n = int(np.clip(np.exp(rng.normal(np.log(3000.0), 0.8)), 200, 60000))
+        if keep.size > n:
+            keep = np.sort(rng.choice(keep, n, replace=False))
+        sigma = 10.0 ** rng.uniform(np.log10(2e-4), np.log10(5e-3))
+        y = 1.0 + rng.normal(0.0, sigma, keep.size)
+        if rng.random() < 0.5:
+            period = 10.0 ** rng.uniform(np.log10(0.5), np.log10(13.0))
+            _box(keep, rng, period, rng.uniform(0.02, 0.25), 10.0 ** rng.uniform(-4.0, -2.0), y)
+        ts.append(keep + (2460000.0 if not kind[c] else 1400.0))
+        ys.append(y.astype(np.float32).astype(np.float64))
+        sizes[c] = keep.size
+    offsets = np.zeros(n_curves + 1, dtype=np.int64)
+    offsets[1:] = np.cumsum(sizes)
+    return np.concatenate(ts), np.concatenate(ys), offsets, kind
 
 
 def batched_periods() -> np.ndarray:
@@ -185,6 +261,7 @@ def tls_curves(n_curves: int, *, seed: int = 0, n_range=(10000, 30000)) -> list[
     return out
 
 
-__all__ = ["Curve", "MULTIBAND_BANDS", "batched_curves", "batched_periods",
+__all__ = ["Curve", "MULTIBAND_BANDS", "batched_curves", "batched_periods", "catalogue_curves",
+           "proposal_curves",
            "long_baseline_curves", "long_baseline_periods", "multiband_stars", "single_curve",
            "tls_curves"]
