@@ -72,6 +72,12 @@ def _ptr(t) -> int | None:
     return None if t is None else int(t.data_ptr())
 
 
+def _bf16_bits(a: np.ndarray) -> np.ndarray:
+    """fp32 values rounded to bf16 (nearest, ties to even), as uint16 bits."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
 class _null:
     def __enter__(self):
         return None
@@ -168,16 +174,26 @@ class Weights:
     def arrays(self) -> list:
         return [*self.conv_w, *self.conv_b, self.w1, self.b1, self.w2, self.b2]
 
-    def save(self, path: str) -> None:
+    def save(self, path: str, *, compact: bool = False) -> None:
+        """npz of the arrays (fp32) and the meta record; ``compact`` stores the
+        weight matrices as their bf16 bit patterns (what the GEMMs read; half
+        the size, biases stay fp32)."""
         import json
-        np.savez_compressed(path, meta=np.array(json.dumps(self.meta)),
-                            **{f"p{i}": a for i, a in enumerate(self.arrays())})
+        arrays = {}
+        for i, a in enumerate(self.arrays()):
+            if compact and a.ndim == 2:
+                arrays[f"h{i}"] = _bf16_bits(a)
+            else:
+                arrays[f"p{i}"] = a
+        np.savez_compressed(path, meta=np.array(json.dumps(self.meta)), **arrays)
 
     @classmethod
     def load(cls, path: str) -> "Weights":
         import json
         z = np.load(path)
-        a = [z[f"p{i}"].astype(np.float32) for i in range(2 * N_CONV + 4)]
+        a = [z[f"p{i}"].astype(np.float32) if f"p{i}" in z else
+             (z[f"h{i}"].astype(np.uint32) << 16).view(np.float32)
+             for i in range(2 * N_CONV + 4)]
         meta = json.loads(str(z["meta"])) if "meta" in z else {}
         return cls(a[:N_CONV], a[N_CONV:2 * N_CONV], *a[2 * N_CONV:], meta=meta)
 
