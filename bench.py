@@ -368,6 +368,11 @@ def pruned_check(engine, curves, segments, grid, packed, plain_best, steps: int,
         engine.launch()
         engine.download_best()
         plain_times.append(time.perf_counter() - t0)
+    # the other end of the trade: every curve searched over its windows only
+    prop_all = Proposer(w, segments, threshold=0.0)
+    t0 = time.perf_counter()
+    res_all = prop_all.search(host, engine)
+    t_all = time.perf_counter() - t0
     n = len(curves)
     agree = res.best_index == np.asarray(plain_best)
     conf = res.confident
@@ -382,6 +387,11 @@ def pruned_check(engine, curves, segments, grid, packed, plain_best, steps: int,
             "periods_searched_frac": res.periods_searched / float(n * grid.n_periods),
             "plain_best_e2e": plain, "speedup_vs_plain": value / plain,
             "threshold": prop.threshold, "k": prop.k, "widen": prop.widen,
+            "all_pruned": {"value": len(curves) / t_all,
+                           "agreement": float(np.mean(res_all.best_index ==
+                                                      np.asarray(plain_best))),
+                           "periods_searched_frac":
+                               res_all.periods_searched / float(n * grid.n_periods)},
             "training": {k: w.meta.get(k) for k in ("train_curves", "epochs", "val_top1",
                                                      "val_window_recall", "val_confident_frac",
                                                      "val_agreement_bound")},
