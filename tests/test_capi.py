@@ -11,15 +11,18 @@ from conftest import ROOT
 
 
 def _declared():
-    text = open(os.path.join(ROOT, "include", "bls_b200.h")).read()
-    return sorted(set(re.findall(r"^(?:int|const char\*)\s+(bls_\w+)\(", text, re.M)))
+    inc = os.path.join(ROOT, "include")
+    text = "\n".join(open(os.path.join(inc, f)).read() for f in sorted(os.listdir(inc))
+                     if f.endswith(".h"))
+    return sorted(set(re.findall(r"^(?:int|const char\*)\s+((?:bls|pn)_\w+)\(", text, re.M)))
 
 
 def test_header_declares_the_entry_points():
     names = _declared()
     for must in ("bls_engine_create", "bls_engine_destroy", "bls_last_error", "bls_prepare",
                  "bls_launch", "bls_download", "bls_download_best", "bls_search",
-                 "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix"):
+                 "bls_batch_info", "bls_debug_fold_bins", "bls_debug_prefix",
+                 "bls_download_curves", "pn_gemm", "pn_bin_curves", "pn_topk"):
         assert must in names
 
 
