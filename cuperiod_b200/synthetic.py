@@ -190,11 +190,13 @@ def long_baseline_curves(n_curves: int, *, seed: int = 0) -> list[Curve]:
     out = []
     for _ in range(n_curves):
         sigma = 10.0 ** rng.uniform(np.log10(2e-4), np.log10(5e-3))
-        y = (1.0 + rng.normal(0.0, sigma, t.size)).astype(np.float32).astype(np.float64)
+        y = 1.0 + rng.normal(0.0, sigma, t.size)
         period = 10.0 ** rng.uniform(np.log10(0.5), np.log10(400.0))
         duration = rng.uniform(0.02, 0.25)
         depth = 10.0 ** rng.uniform(np.log10(5e-5), -2.0)
         _box(t, rng, period, duration, depth, y)
+        # FP32 flux, transits included (the photometry is stored in single precision)
+        y = y.astype(np.float32).astype(np.float64)
         out.append(Curve(t.copy(), y, None, (period, duration, depth)))
     return out
 
