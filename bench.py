@@ -99,7 +99,7 @@ def parse_args():
     p.add_argument("--catalogue-chunk", type=int, default=16384,
                    help="catalogue: curves per streamed chunk")
     p.add_argument("--workload", choices=("batch", "long-baseline", "multiband-shared", "tls",
-                                          "catalogue"),
+                                          "catalogue", "single"),
                    default="batch",
                    help="batch: the headline batched search; long-baseline: the 4-year "
                         "precision stress search of --lb-curves curves with an oracle check; "
@@ -560,6 +560,19 @@ def run_ours(args) -> None:
     e2e_step = max_over_ranks(statistics.mean(e2e_ms))
     e2e_value = world * n_curves / (e2e_step / 1000.0)
     e2e_h2d = engine.info()["h2d_bytes"]
+    # the same call left to its own worker threads (4 engines and streams, chunks
+    # of 1024 curves): one chunk's host steps overlap another's search
+    batch_periodograms(keyed[:1024], "BLS", grid=gspec, chunk_size=1024, workers=4)
+    ovl_ms = []
+    for i in range(args.steps):
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        summary_o = batch_periodograms(keyed, "BLS", grid=gspec, chunk_size=1024, workers=4)
+        ovl_ms.append(1000.0 * (time.perf_counter() - t0))
+    ovl_value = world * n_curves / (max_over_ranks(statistics.mean(ovl_ms)) / 1000.0)
+    ovl_same = sum(int(a["best_period"] == b["best_period"])
+                   for a, b in zip(summary.rows, summary_o.rows))
     rows = summary.rows
     n_best = 10
     e2e_d2h = n_curves * (4 + 8 * n_best + 8 * 8 * n_best)
@@ -628,7 +641,12 @@ def run_ours(args) -> None:
                     "d2h_bytes_per_step": e2e_d2h,
                     "api": "batch_periodograms(light curves, 'BLS', grid=GridSpec, "
                            "chunk_size=all): result rows with 10 alias-diverse peaks",
-                    "clock": "host wall clock around the synchronous call"},
+                    "clock": "host wall clock around the synchronous call",
+                    "overlapped": {"value": ovl_value, "unit": UNIT,
+                                   "api": "batch_periodograms(..., chunk_size=1024, workers=4): "
+                                          "four engines and streams, host steps of one chunk "
+                                          "overlapping another's search",
+                                   "rows_equal_best_period": ovl_same}},
         }
         if world == 1 and lb:
             out["precision"], out["cpu_baseline"] = long_baseline_check(
@@ -1042,6 +1060,88 @@ def run_tls_ours(args) -> None:
         dist.destroy_process_group()
 
 
+# ---- single-curve latency (benchmark configuration 1) ------------------------------
+
+SINGLE_WORKLOAD = ("single-curve BLS: 2000 points over 90 d, 10,000 log periods 0.5-30 d, "
+                   "durations {0.05, 0.08, 0.12, 0.16, 0.2} d, likelihood objective, full "
+                   "spectrum + best period (bls_power)")
+
+
+def run_single(args) -> None:
+    """One curve at a time through the kernel-level drop-in ``bls_power`` (host
+    arrays in, the eight fields of the full spectrum out), the reference's
+    ``bls_power(..., backend="numba")`` call (``_bls_core.py:882-1028``)."""
+    from cuperiod_b200.synthetic import SINGLE_DURATIONS, SINGLE_PERIODS, single_curve
+
+    c = single_curve(args.seed)
+    periods = np.geomspace(*SINGLE_PERIODS)
+    durations = np.asarray(SINGLE_DURATIONS)
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        from oracle import oracle
+        cores = os.cpu_count() or 1
+        for _ in range(args.warmup):
+            oracle.bls_power(c.t, c.y, c.dy, periods, durations, 10, objective="likelihood",
+                             n_threads=cores, screen=True)
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            oracle.bls_power(c.t, c.y, c.dy, periods, durations, 10, objective="likelihood",
+                             n_threads=cores, screen=True)
+            times.append(time.perf_counter() - t0)
+        value = len(times) / sum(times)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": SINGLE_WORKLOAD, "curves_per_rank": 1, "cpu": "host cores"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "the whole workload, the reference's screened numba "
+                                       "sweep restated in C"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+
+    from cuperiod_b200 import _lib
+    from cuperiod_b200.core import bls_power
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    engine = _lib.Engine(device=local)
+    for _ in range(max(args.warmup, 3)):
+        bls_power(c.t, c.y, c.dy, periods, durations, 10, objective="likelihood", engine=engine)
+    times = []
+    with ClockSampler(local) as sampler:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = bls_power(c.t, c.y, c.dy, periods, durations, 10, objective="likelihood",
+                            engine=engine)
+            times.append(time.perf_counter() - t0)
+    clocks = sampler.summary()
+    dev_ms = engine.time_launches(reps=10)
+    best = float(periods[int(np.argmax(res.power))])
+    value = len(times) / sum(times)
+    print(json.dumps({
+        "metric": METRIC, "value": 1000.0 / dev_ms, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "mixed: f64 phase and objective, exact int32 bin sums, f32 screen",
+        "data": "synthetic",
+        "config": {"workload": SINGLE_WORKLOAD, "curves_per_rank": 1, "best_period": best,
+                   "l2": "one curve (48 KB) lives in L2; device time of one launch"},
+        "clocks": clocks, "gpu_launches": args.steps,
+        "e2e": {"value": value, "unit": UNIT, "latency_ms": 1000.0 / value,
+                "h2d_bytes_per_step": c.t.size * 12 + periods.size * 24,
+                "d2h_bytes_per_step": periods.size * 7 * 8,
+                "api": "cuperiod_b200.bls_power(t, y, dy, periods, durations, 10, "
+                       "objective='likelihood')"},
+    }), flush=True)
+    engine.close()
+
+
 # ---- the streamed catalogue sweep ------------------------------------------------
 
 CAT_WORKLOAD = ("catalogue sweep: {n} curves streamed from pinned host memory in {chunk}-curve "
@@ -1141,6 +1241,9 @@ def run_catalogue(args) -> None:
 
 def main() -> None:
     args = parse_args()
+    if args.workload == "single":
+        run_single(args)
+        return
     if args.workload == "catalogue":
         if args.impl == "reference":
             if int(os.environ.get("RANK", "0")) == 0:
