@@ -1221,6 +1221,9 @@ def run_catalogue(args) -> None:
                        "periods_searched_frac": sum(r["periods_searched"] for r in pruned.chunks)
                        / float(n * 50000)},
             "plain": {"value": world * n / q_s, "seconds": q_s},
+            "chunks": {"pruned_search_s": [round(r["search_s"], 2) for r in pruned.chunks],
+                       "pruned_audit_s": [round(r["audit_s"], 2) for r in pruned.chunks],
+                       "plain_search_s": [round(r["search_s"], 2) for r in plain.chunks]},
             "speedup_vs_plain": q_s / p_s,
             "roofline": {"bound": "hbm", "achieved": h2d / p_s / 1e9, "peak": hbm,
                          "unit": "GB/s", "frac": h2d / p_s / 1e9 / hbm, "traffic": None,

@@ -283,8 +283,34 @@ __device__ __forceinline__ void fold_points(const TileShared& s, uint32_t hist_s
                 rec[r] = hq + kB + (v >> fb) * kB;
             }
             if (all_ok) {
+                if (MODE == MODE_UNIFORM) {
+                    // a lane's points are consecutive in time, so dense curves in
+                    // the wide-bin segments put several in one bin: each run of
+                    // equal bins adds its exact sums once (low parts of at most 8
+                    // points stay below 2^16), and lanes without a flush at a
+                    // step sit out that step's atomics and their bank conflicts
+                    uint32_t s_lo = p.lo[0], s_hi = p.hi[0], s_c = 1u;
 #pragma unroll
-                for (int r = 0; r < kPts; ++r) add_point<MODE>(rec[r], p, r, flag);
+                    for (int r = 1; r < kPts; ++r) {
+                        if (rec[r] != rec[r - 1]) {
+                            red_add_u32<0>(rec[r - 1], s_lo);
+                            red_add_u32<4>(rec[r - 1], s_hi);
+                            red_add_u32<8>(rec[r - 1], s_c);
+                            s_lo = 0u;
+                            s_hi = 0u;
+                            s_c = 0u;
+                        }
+                        s_lo += p.lo[r];
+                        s_hi += p.hi[r];
+                        s_c += 1u;
+                    }
+                    red_add_u32<0>(rec[kPts - 1], s_lo);
+                    red_add_u32<4>(rec[kPts - 1], s_hi);
+                    red_add_u32<8>(rec[kPts - 1], s_c);
+                } else {
+#pragma unroll
+                    for (int r = 0; r < kPts; ++r) add_point<MODE>(rec[r], p, r, flag);
+                }
                 continue;
             }
         }
