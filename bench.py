@@ -355,11 +355,12 @@ def long_baseline_check(engine, curves, segments, grid, n_check: int):
 def pruned_check(engine, curves, segments, grid, packed, plain_best, steps: int,
                  weights_path: str) -> dict:
     """The learned-pruned search of the same batch (``cuperiod_b200.proposal``):
-    light curves/s end to end (host arrays in, each curve's best period out: the
-    binning and the network on the tensor cores, the windows built on the host,
-    one engine launch over every curve's windows or, below the confidence
-    threshold, its full grid), agreement of its best period with the timed
-    plain search's, and the plain search timed the same way."""
+    light curves/s end to end (the packed host batch in, each curve's best period
+    out: the binning and the network on the tensor cores, the windows built on
+    the host, one engine launch over every curve's windows or, below the
+    confidence threshold, its full grid), agreement of its best period with the
+    timed plain search's, and the plain search of the same packed batch timed
+    the same way."""
     from cuperiod_b200.proposal import Proposer, Weights
     if not os.path.exists(weights_path):
         return {"unavailable": "no trained proposal weights at " + os.path.relpath(weights_path, ROOT)}
@@ -370,7 +371,7 @@ def pruned_check(engine, curves, segments, grid, packed, plain_best, steps: int,
     times, res = [], None
     for _ in range(steps):
         t0 = time.perf_counter()
-        res = prop.search(host, engine)
+        res = prop.search_packed(packed, engine)
         times.append(time.perf_counter() - t0)
     plain_times = []
     for _ in range(steps):
@@ -382,7 +383,7 @@ def pruned_check(engine, curves, segments, grid, packed, plain_best, steps: int,
     # the other end of the trade: every curve searched over its windows only
     prop_all = Proposer(w, segments, threshold=0.0)
     t0 = time.perf_counter()
-    res_all = prop_all.search(host, engine)
+    res_all = prop_all.search_packed(packed, engine)
     t_all = time.perf_counter() - t0
     n = len(curves)
     agree = res.best_index == np.asarray(plain_best)

@@ -420,8 +420,18 @@ class Proposer:
     def __init__(self, weights: Weights, segments, *, oversample: int = 10, objective: int = 0,
                  k: int | None = None, widen: int | None = None,
                  threshold: float | None = None, chunk: int = 1024, stream=None):
+        meta = weights.meta
+        self._init_grid(segments, oversample, objective,
+                        int(widen if widen is not None else meta.get("widen", 1)))
         self.net = ProposalNet(weights, Ops(stream))
         self.stream = stream
+        self.k = int(k if k is not None else meta.get("k", 16))
+        self.threshold = float(threshold if threshold is not None else meta.get("threshold", 0.0))
+        self.chunk = int(chunk)
+
+    def _init_grid(self, segments, oversample: int, objective: int, widen: int) -> None:
+        """The host-side grid state (no device work): the full grid, its class
+        edges and segment bounds."""
         self.segments = [(np.ascontiguousarray(p, dtype=np.float64),
                           np.ascontiguousarray(d, dtype=np.float64)) for p, d in segments]
         self.periods = np.concatenate([p for p, _ in self.segments])
@@ -430,12 +440,7 @@ class Proposer:
                              f"{N_CLASSES} periods")
         self.seg_bounds = np.concatenate([[0], np.cumsum([p.size for p, _ in self.segments])])
         self.edges = class_edges(self.periods.size)
-        self.oversample, self.objective = int(oversample), int(objective)
-        meta = weights.meta
-        self.k = int(k if k is not None else meta.get("k", 16))
-        self.widen = int(widen if widen is not None else meta.get("widen", 1))
-        self.threshold = float(threshold if threshold is not None else meta.get("threshold", 0.0))
-        self.chunk = int(chunk)
+        self.oversample, self.objective, self.widen = int(oversample), int(objective), int(widen)
         self.full = _lib.PackedGrid.from_segments(self.segments, self.oversample, self.objective)
 
     def propose_packed(self, t, y, offsets):
@@ -482,26 +487,69 @@ class Proposer:
         pc = _lib.PackedCurves.from_arrays(curves)
         return self.search_packed(pc, engine)
 
+    def window_grids(self, classes: np.ndarray):
+        """Every row's window grid at once: ``(grids, index)`` with one
+        ``_lib.PackedGrid`` per row of ``classes`` (its periods a view into one
+        array, its segments the full grid's, empty where no window reaches) and
+        the full-grid index of every period, concatenated row after row."""
+        n = classes.shape[0]
+        if n == 0:
+            return [], np.empty(0, dtype=np.int64)
+        if not hasattr(self, "_pieces"):
+            # the grid's index runs cut at every class edge and segment bound:
+            # piece p is [cut[p], cut[p + 1]), of one class and one segment
+            cut = np.unique(np.concatenate([self.edges, self.seg_bounds]))
+            lo = cut[:-1]
+            self._pieces = (lo, np.diff(cut),
+                            np.searchsorted(self.edges, lo, side="right") - 1,
+                            np.searchsorted(self.seg_bounds, lo, side="right") - 1)
+        lo, ln, pcls, pseg = self._pieces
+        sel = np.zeros((n, N_CLASSES), dtype=bool)
+        rows = np.arange(n)[:, None]
+        for off in range(-self.widen, self.widen + 1):
+            sel[rows, np.clip(classes.astype(np.int64) + off, 0, N_CLASSES - 1)] = True
+        ci, pi = np.nonzero(sel[:, pcls])              # row-major: each row's pieces ascending
+        lens = ln[pi]
+        # the index runs as one cumulative sum: steps of 1, a jump at each piece
+        ends = np.cumsum(lens)
+        index = np.ones(int(ends[-1]), dtype=np.int64)
+        index[0] = lo[pi[0]]
+        index[ends[:-1]] = lo[pi[1:]] - (lo[pi[:-1]] + lens[:-1] - 1)
+        np.cumsum(index, out=index)
+        n_seg = len(self.segments)
+        counts = np.zeros((n, n_seg), dtype=np.int64)
+        np.add.at(counts, (ci, pseg[pi]), lens)
+        seg_off = np.zeros((n, n_seg + 1), dtype=np.int64)
+        seg_off[:, 1:] = np.cumsum(counts, axis=1)
+        row_off = np.concatenate([[0], np.cumsum(seg_off[:, -1])])
+        periods = self.periods[index]
+        grids = [_lib.PackedGrid(seg_off[i], periods[row_off[i]:row_off[i + 1]],
+                                 self.full.dur_offsets, self.full.durations, self.oversample,
+                                 self.objective) for i in range(n)]
+        return grids, index
+
     def search_packed(self, packed, engine) -> PrunedResult:
         """A packed batch (``_lib.PackedCurves``): the network, then one engine
         launch over every curve's windows or full grid."""
         idx, mass = self.propose_packed(packed.t, packed.y, packed.offsets)
         confident = mass >= self.threshold
-        grids = [self.full]
+        conf = np.flatnonzero(confident)
+        wgrids, windex = self.window_grids(idx[conf])
+        grids = [self.full] + wgrids
         gid = np.zeros(packed.n_curves, dtype=np.int32)
-        maps = [None]
-        for i in np.flatnonzero(confident):
-            segs = self.window_segments(idx[i])
-            grids.append(_lib.PackedGrid.from_segments(segs, self.oversample, self.objective))
-            maps.append(np.searchsorted(self.periods, np.concatenate([p for p, _ in segs])))
-            gid[i] = len(grids) - 1
+        gid[conf] = np.arange(1, conf.size + 1, dtype=np.int32)
         engine.prepare_grids(grids, gid, packed)
         engine.launch()
         bi, bp, _, _ = engine.download_best()
-        full_index = np.array([int(b) if g == 0 else int(maps[g][b]) for b, g in zip(bi, gid)],
-                              dtype=np.int64)
-        return PrunedResult(self.periods[full_index], full_index, bp, confident, mass,
-                            int(sum(grids[g].n_periods for g in gid)))
+        bi = np.asarray(bi, dtype=np.int64)
+        full_index = bi.copy()
+        if conf.size:
+            # a window grid's index k is the k-th period of its row in windex
+            sizes = np.array([g.n_periods for g in wgrids], dtype=np.int64)
+            base = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+            full_index[conf] = windex[base + bi[conf]]
+        searched = int((packed.n_curves - conf.size) * self.full.n_periods + windex.size)
+        return PrunedResult(self.periods[full_index], full_index, bp, confident, mass, searched)
 
 
 __all__ = ["N_BINS", "N_CLASSES", "Ops", "PrunedResult", "ProposalNet", "Proposer", "Weights",
