@@ -205,3 +205,40 @@ def test_box_holding_every_point_is_not_admissible(engine, objective, weights):
     got = _run(engine, t, y, dy, periods, durations, 10, objective)
     diag = compare(ref, got, rtol=1e-6, box_agree=0.98)
     assert diag["same_argmax"]
+
+
+
+@pytest.mark.parametrize("objective", ["snr", "likelihood"])
+@pytest.mark.parametrize("cadence,p_lo,dur_lo", [(2.0 / 1440, 0.3, 0.01),    # ~1 point a bin a cycle
+                                                 (0.5 / 1440, 0.36, 0.0139)])  # ~300 a bin
+def test_regular_cadence_spectra_are_identical(engine, objective, cadence, p_lo, dur_lo):
+    # One weight, a regular cadence with dropouts, FP32 fluxes: the reference's
+    # FP64 sums are exact, and so are the engine's fixed-point sums, so every
+    # field of every period is identical.  The second case puts ~300 points in
+    # one phase bin (a 0.5-minute cadence folded over 75 cycles).
+    t, y, dy = transit_curve(int(27.0 / cadence), span=27.0, period=3.3, depth=2e-3, seed=5,
+                             cadence=cadence)
+    keep = np.random.default_rng(1).uniform(size=t.size) < 0.9          # gaps
+    t, y = t[keep], y[keep].astype(np.float32).astype(np.float64)
+    dy = np.ones_like(y)            # unit weights: the reference's FP64 sums are exact
+    periods = np.geomspace(p_lo, 2.0 * p_lo, 400)
+    durations = np.geomspace(dur_lo, 4.0 * dur_lo, 6)
+    ref = oracle.bls_power(t, y, dy, periods, durations, 10, objective=objective)
+    got = _run(engine, t, y, dy, periods, durations, 10, objective)
+    for f in FIELDS:
+        np.testing.assert_array_equal(got[f], ref[f], err_msg=f)
+
+
+def test_four_year_regular_cadence_spectra_are_identical(engine):
+    # four years at 1.5-hour cadence: a bin of a 0.5 d period gathers points
+    # from ~2900 cycles
+    t, y, dy = transit_curve(int(1461.0 * 48), span=1461.0, period=3.3, depth=2e-3, seed=6,
+                             cadence=30.0 / 1440)
+    t, y = t[::3], y[::3].astype(np.float32).astype(np.float64)
+    dy = np.ones_like(y)
+    periods = np.geomspace(0.5, 1.0, 300)
+    durations = np.geomspace(0.04, 0.16, 6)
+    ref = oracle.bls_power(t, y, dy, periods, durations, 10)
+    got = _run(engine, t, y, dy, periods, durations, 10, "snr")
+    for f in FIELDS:
+        np.testing.assert_array_equal(got[f], ref[f], err_msg=f)
