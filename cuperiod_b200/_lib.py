@@ -237,6 +237,48 @@ def default_grid_sizes(spec: DefaultGridSpec, baselines) -> np.ndarray:
     return out
 
 
+_PACK_THREADS = max(1, min(16, os.cpu_count() or 1))
+_pack_pool = None
+_pack_pool_lock = threading.Lock()
+
+
+def _concat(parts, off: np.ndarray, fill: float | None = None) -> np.ndarray:
+    """The arrays of ``parts`` (``None``: ``fill``) end to end at ``off``; large
+    batches are copied by several host threads (numpy's copies release the GIL),
+    each writing, and so first touching, its own share of the output."""
+    global _pack_pool
+    total = int(off[-1])
+    out = np.empty(total, dtype=np.float64)
+    if total == 0:
+        return out
+
+    def copy(lo: int, hi: int) -> None:
+        for i in range(lo, hi):
+            dst = out[off[i]:off[i + 1]]
+            if parts[i] is None:
+                dst.fill(fill)
+            else:
+                dst[...] = parts[i]
+
+    n = len(parts)
+    k = min(_PACK_THREADS, n, max(1, total // (1 << 20)))      # >= 1M points a thread
+    if k <= 1:
+        copy(0, n)
+        return out
+    with _pack_pool_lock:
+        if _pack_pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+            _pack_pool = ThreadPoolExecutor(max_workers=_PACK_THREADS,
+                                            thread_name_prefix="bls-pack")
+        pool = _pack_pool
+    # split by points, not curves, so the threads' shares are even
+    cuts = np.searchsorted(off, np.linspace(0, total, k + 1)).tolist()
+    cuts[0], cuts[-1] = 0, n
+    for f in [pool.submit(copy, a, b) for a, b in zip(cuts[:-1], cuts[1:]) if b > a]:
+        f.result()
+    return out
+
+
 @dataclass
 class PackedCurves:
     """Light curves concatenated in the C ABI's layout (keeps its arrays alive)."""
@@ -256,11 +298,11 @@ class PackedCurves:
             ts.append(t)
             ys.append(y)
             if any_dy:
-                dys.append(np.ones_like(t) if dy is None else _f64(dy).ravel())
+                dys.append(None if dy is None else _f64(dy).ravel())
         off = np.zeros(len(curves) + 1, dtype=np.int64)
         off[1:] = np.cumsum([t.size for t in ts])
-        cat = lambda xs: _f64(np.concatenate(xs)) if xs else np.empty(0)
-        return cls(off, cat(ts), cat(ys), cat(dys) if any_dy else None)
+        return cls(off, _concat(ts, off), _concat(ys, off),
+                   _concat(dys, off, fill=1.0) if any_dy else None)
 
     @property
     def n_curves(self) -> int:

@@ -174,15 +174,16 @@ def _assemble(fields: dict[str, np.ndarray], n: int, baseline: float, meta: Any)
 
 
 def _prepared_curve(lc: LightCurve, settings: BLSSettings):
-    """``finite()``, the reference's guards and unit errors (bls.py:369-380)."""
+    """``finite()`` and the reference's guards (bls.py:369-380).  A curve without
+    errors keeps ``None``: the engine then takes every point's ivar as 1, the
+    reference's unit errors, without an array of ones being built and packed."""
     finite = lc.finite()
     if finite.n < settings.min_detections:
         raise InsufficientDataError(
             f"BLS: {finite.n} finite points < min_detections {settings.min_detections}")
     if finite.baseline <= 0.0:
         raise InsufficientDataError("BLS: no usable time baseline")
-    err = finite.error if finite.error is not None else np.ones_like(finite.value)
-    return finite, err
+    return finite, finite.error
 
 
 class BLSMethod:
