@@ -365,7 +365,10 @@ def pruned_check(engine, curves, segments, grid, packed, plain_best, steps: int,
     if not os.path.exists(weights_path):
         return {"unavailable": "no trained proposal weights at " + os.path.relpath(weights_path, ROOT)}
     w = Weights.load(weights_path)
-    prop = Proposer(w, segments)
+    # the threshold calibrated on held-out curves of this workload's generator
+    # (another seed), else the training distribution's
+    thr_key = "threshold_batch" if "threshold_batch" in w.meta else "threshold"
+    prop = Proposer(w, segments, threshold=w.meta.get(thr_key))
     host = [(c.t, c.y, c.dy) for c in curves]
     prop.search(host[:256], engine)                        # warm-up
     times, res = [], None
@@ -398,7 +401,10 @@ def pruned_check(engine, curves, segments, grid, packed, plain_best, steps: int,
             "confident_agreement": float(agree[conf].mean()) if conf.any() else None,
             "periods_searched_frac": res.periods_searched / float(n * grid.n_periods),
             "plain_best_e2e": plain, "speedup_vs_plain": value / plain,
-            "threshold": prop.threshold, "k": prop.k, "widen": prop.widen,
+            "threshold": prop.threshold, "threshold_source": thr_key,
+            "calibration": w.meta.get("batch_calibration") if thr_key == "threshold_batch"
+            else None,
+            "k": prop.k, "widen": prop.widen,
             "all_pruned": {"value": len(curves) / t_all,
                            "agreement": float(np.mean(res_all.best_index ==
                                                       np.asarray(plain_best))),

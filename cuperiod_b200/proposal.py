@@ -375,6 +375,14 @@ def window_mask(classes, edges: np.ndarray, widen: int) -> list[tuple[int, int]]
     return out
 
 
+def windows_hold(classes: np.ndarray, index: np.ndarray, edges: np.ndarray,
+                 widen: int) -> np.ndarray:
+    """Per row: whether the windows of ``classes[i]`` (``window_mask``) hold grid
+    index ``index[i]`` -- a chosen class within ``widen`` of the index's class."""
+    cls = np.searchsorted(edges, np.asarray(index, dtype=np.int64), side="right") - 1
+    return (np.abs(np.asarray(classes, dtype=np.int64) - cls[:, None]) <= widen).any(axis=1)
+
+
 def device_packed(t, y, offsets):
     """Packed FP64 times and fluxes and their int64 offsets (host arrays,
     offsets from 0) on the device, copied on the current stream (asynchronously
@@ -553,4 +561,5 @@ class Proposer:
 
 
 __all__ = ["N_BINS", "N_CLASSES", "Ops", "PrunedResult", "ProposalNet", "Proposer", "Weights",
-           "class_edges", "device_curves", "device_packed", "kp", "labels_of", "window_mask"]
+           "class_edges", "device_curves", "device_packed", "kp", "labels_of", "window_mask",
+           "windows_hold"]

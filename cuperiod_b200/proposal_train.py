@@ -37,7 +37,7 @@ from . import _lib
 from .bls import _grid_segments
 from .grid import GridSpec
 from .proposal import (IN_CHANNELS, N_BINS, ProposalNet, Weights, class_edges, device_curves,
-                       labels_of, window_mask)
+                       labels_of, window_mask, windows_hold)
 from .settings import BLSSettings
 from .synthetic import batched_periods, proposal_curves
 
@@ -168,6 +168,47 @@ def train(args) -> dict:
     return meta
 
 
+def calibrate_batch(weights_path: str, n_curves: int, seed: int, agreement: float) -> dict:
+    """The confidence threshold for the batched workload: ``n_curves`` curves of
+    its generator (``synthetic.batched_curves``, a seed apart from any benchmark
+    batch) searched over the full grid, then ranked by the network; the
+    threshold is the smallest at which the confident curves whose full-grid best
+    period falls outside their windows stay within ``1 - agreement`` of all
+    curves.  Written to the weights' meta as ``threshold_batch`` with a record;
+    the training-distribution threshold (``threshold``) is kept."""
+    from .proposal import Proposer
+    from .synthetic import batched_curves
+    segments = grid_segments()
+    w = Weights.load(weights_path)
+    engine = _lib.Engine()
+    curves = [(c.t, c.y, c.dy) for c in batched_curves(n_curves, seed=seed)]
+    packed = _lib.PackedCurves.from_arrays(curves)
+    grid = _lib.PackedGrid.from_segments(segments, 10, 0)
+    engine.prepare(grid, packed)
+    engine.launch()
+    best = np.asarray(engine.download_best()[0], dtype=np.int64)
+    prop = Proposer(w, segments, threshold=0.0)
+    idx, mass = prop.propose_packed(packed.t, packed.y, packed.offsets)
+    hit = windows_hold(idx, best, prop.edges, prop.widen)
+    window = float(np.mean([sum(hi - lo for lo, hi in window_mask(r, prop.edges, prop.widen))
+                            for r in idx[:256]]) / prop.edges[-1])
+
+    def at(thr: float) -> dict:
+        conf = mass >= thr
+        return {"threshold": float(thr), "confident_frac": float(conf.mean()),
+                "agreement_bound": float(1.0 - np.mean(conf & ~hit)),
+                "periods_searched_frac": float(1.0 - conf.mean() * (1.0 - window))}
+    thr = calibrate(mass, hit, 1.0 - agreement)
+    record = {"curves": n_curves, "seed": seed, "target_agreement": agreement, **at(thr),
+              "window_hit_frac": float(hit.mean()),
+              "table": [at(calibrate(mass, hit, 1.0 - a)) for a in (0.999, 0.998, 0.995, 0.99)]}
+    w.meta["threshold_batch"] = float(thr)
+    w.meta["batch_calibration"] = record
+    w.save(weights_path, compact=True)
+    engine.close()
+    return record
+
+
 def main(argv=None) -> None:
     p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     p.add_argument("--curves", type=int, default=65536, help="training curves")
@@ -184,7 +225,16 @@ def main(argv=None) -> None:
     p.add_argument("--seed", type=int, default=1000003)
     p.add_argument("--flip", type=int, default=1, help="time-reversal augmentation (0: off)")
     p.add_argument("--out", default=DEFAULT_OUT)
+    p.add_argument("--calibrate-batch", type=int, default=0, metavar="N",
+                   help="instead of training: set the batched workload's threshold on N "
+                        "curves of its generator (weights at --out)")
+    p.add_argument("--calib-seed", type=int, default=424242)
+    p.add_argument("--agreement", type=float, default=0.995)
     args = p.parse_args(argv)
+    if args.calibrate_batch > 0:
+        rec = calibrate_batch(args.out, args.calibrate_batch, args.calib_seed, args.agreement)
+        print(json.dumps(rec), flush=True)
+        return
     meta = train(args)
     print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}), flush=True)
 

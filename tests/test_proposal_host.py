@@ -71,3 +71,17 @@ def test_window_grids_match_the_per_curve_windows():
 def test_window_grids_of_no_curves():
     grids, index = _proposer().window_grids(np.empty((0, 16), dtype=np.int64))
     assert grids == [] and index.size == 0
+
+
+def test_windows_hold_is_the_window_test():
+    from cuperiod_b200.proposal import windows_hold
+    e = class_edges(50_000)
+    rng = np.random.default_rng(3)
+    idx = rng.integers(0, N_CLASSES, (500, 16))
+    best = rng.integers(0, 50_000, 500)
+    best[:16] = e[idx[:16, 0]]                 # on a class's first index
+    best[16:32] = e[idx[16:32, 0] + 1] - 1     # on its last
+    got = windows_hold(idx, best, e, 1)
+    want = [any(lo <= b < hi for lo, hi in window_mask(r, e, 1)) for r, b in zip(idx, best)]
+    np.testing.assert_array_equal(got, want)
+    assert got[:32].all()
