@@ -323,11 +323,13 @@ class BLSMethod:
                                   [(prepared[i][0].time, prepared[i][0].value, prepared[i][1])
                                    for i in dev]))
             eng.launch()
-            order, sep, tol = _peak_params([prepared[i][0].baseline for i in dev], settings)
+            base = [prepared[i][0].baseline for i in dev]
+            order, sep, tol = _peak_params(base, settings)
             n_peaks, _, fields = eng.rows(count, order, sep, tol)
+            made = self._rows([items[i][0] for i in dev], [prepared[i][0].n for i in dev], base,
+                              n_peaks, fields, n_best, extra_keys)
             for j, i in enumerate(dev):
-                rows[i] = self._row(items[i][0], prepared[i][0], int(n_peaks[j]), fields[j],
-                                    n_best, extra_keys)
+                rows[i] = made[j]
         return rows  # type: ignore[return-value]
 
     def split_default(self, keyed: Sequence[tuple[str, LightCurve]], settings: BLSSettings
@@ -388,29 +390,55 @@ class BLSMethod:
         eng.launch()
         order, sep, tol = _peak_params(baselines, settings)
         n_peaks, _, fields = eng.rows(count, order, sep, tol)
-        return [self._row(key, f, int(n_peaks[j]), fields[j], n_best, extra_keys)
-                for j, ((key, _), (f, _)) in enumerate(zip(keyed, prepared))]
+        return self._rows([key for key, _ in keyed], [f.n for f, _ in prepared], baselines,
+                          n_peaks, fields, n_best, extra_keys)
 
-    def _row(self, key: str, f: LightCurve, k_have: int, fields: np.ndarray, n_best: int,
-             extra_keys: Sequence[str]) -> dict:
-        """One result row from the device's ranked peaks (period, frequency,
-        power, depth, depth_snr, duration, t0, sde per rank)."""
+    def _rows(self, keys: Sequence[str], n_samples: Sequence[int], baselines: Sequence[float],
+              n_peaks: np.ndarray, fields: np.ndarray, n_best: int,
+              extra_keys: Sequence[str]) -> list[dict]:
+        """The result rows from the device's ranked peaks (fields per rank:
+        period, frequency, power, depth, depth_snr, duration, t0, sde): the
+        reference's row layout (batch/io.py:507-571) -- best_period, then per
+        rank period, power, the ``extra_keys`` (NaN where absent) and the other
+        extras -- with the column names built once for all rows."""
         names = ("depth", "depth_snr", "duration", "t0", "sde")
-        row: dict[str, Any] = {"key": key, "method": self.name, "backend": BACKEND_NAME,
-                               "n_samples": f.n, "baseline": f.baseline}
-        row["best_period"] = float(fields[0, 0]) if k_have else float("nan")
-        for rank in range(1, int(n_best) + 1):
-            have = rank <= k_have
-            fr = fields[rank - 1] if rank - 1 < fields.shape[0] else None
-            row[f"period_{rank}"] = float(fr[0]) if have else float("nan")
-            row[f"power_{rank}"] = float(fr[2]) if have else float("nan")
-            extra = {n: float(fr[3 + j]) for j, n in enumerate(names)} if have else {}
-            for ekey in extra_keys:
-                row[f"{ekey}_{rank}"] = extra.get(ekey, float("nan"))
-            for ekey, v in extra.items():
-                if ekey not in extra_keys:
-                    row[f"{ekey}_{rank}"] = v
-        return row
+        nan = float("nan")
+        n_best = int(n_best)
+        # per rank: period key, power key, the extra_keys' (key, field column or
+        # None), the other extras' (key, column); a rank without a peak keeps
+        # only the extra_keys, as NaN
+        layout = []
+        for rank in range(1, n_best + 1):
+            asked = [(f"{e}_{rank}", 3 + names.index(e) if e in names else None)
+                     for e in extra_keys]
+            rest = [(f"{e}_{rank}", 3 + j) for j, e in enumerate(names) if e not in extra_keys]
+            layout.append((f"period_{rank}", f"power_{rank}", asked, rest))
+        counts = np.asarray(n_peaks).tolist()
+        width = fields.shape[1]
+        rows = []
+        for j, key in enumerate(keys):
+            k_have = int(counts[j])
+            fl = fields[j, :min(k_have, width)].tolist()
+            row: dict[str, Any] = {"key": key, "method": self.name, "backend": BACKEND_NAME,
+                                   "n_samples": int(n_samples[j]),
+                                   "baseline": float(baselines[j]),
+                                   "best_period": fl[0][0] if k_have else nan}
+            for r, (pk, wk, asked, rest) in enumerate(layout):
+                if r < k_have:
+                    fr = fl[r]
+                    row[pk] = fr[0]
+                    row[wk] = fr[2]
+                    for ck, c in asked:
+                        row[ck] = fr[c] if c is not None else nan
+                    for ck, c in rest:
+                        row[ck] = fr[c]
+                else:
+                    row[pk] = nan
+                    row[wk] = nan
+                    for ck, _ in asked:
+                        row[ck] = nan
+            rows.append(row)
+        return rows
 
     def _search(self, segments, curves, settings, engine):
         grid = _lib.PackedGrid.from_segments(segments, settings.bins_per_duration,
