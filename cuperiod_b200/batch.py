@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import hashlib
 import os
+import threading
 from dataclasses import dataclass, field
 from typing import Any, Iterable, Sequence
 
@@ -71,6 +72,25 @@ class BatchSummary:
     @property
     def n_failed(self) -> int:
         return len(self.errors)
+
+
+_pools: dict[int, Any] = {}
+_pools_lock = threading.Lock()
+
+
+def _worker_pool(n: int):
+    """The process's pool of ``n`` batch worker threads, created once: each
+    thread keeps its engine (``_lib.default_engine``: device buffers, pinned
+    staging, graph cache) from one call to the next, so a batch does not pay
+    for creating engines.  Jobs of concurrent calls share the threads; each job
+    runs on one thread and its engine."""
+    with _pools_lock:
+        pool = _pools.get(n)
+        if pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+            pool = ThreadPoolExecutor(max_workers=n, thread_name_prefix=f"bls-batch-{n}")
+            _pools[n] = pool
+        return pool
 
 
 def _grid_key(grid: GridSpec) -> str:
@@ -176,9 +196,9 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
     ``workers``: host threads that run the launches (default 4; each thread its
     own engine and CUDA stream, so the small launches of curves with distinct
     default grids, and of multi-band stars, overlap each other and the host
-    work); with an explicit
-    ``engine`` every launch runs on that engine in this thread.  Rows keep the
-    order of a single-threaded run.
+    work; the threads and their engines persist from call to call); with an
+    explicit ``engine`` every launch runs on that engine in this thread.  Rows
+    keep the order of a single-threaded run.
     """
     m = get_method(method)
     s = _settings(settings, m.settings_cls)
@@ -280,13 +300,11 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
 
     n_workers = 1 if engine is not None else max(1, int(workers if workers is not None else 4))
     # engine None: each launch runs on its thread's own engine (default_engine),
-    # created at the first launch
+    # created at the thread's first launch and kept by the persistent pool
     if n_workers == 1 or len(jobs) <= 1:
         results = [run(job, engine) for job in jobs]
     else:
-        from concurrent.futures import ThreadPoolExecutor
-        with ThreadPoolExecutor(max_workers=min(n_workers, len(jobs))) as pool:
-            results = list(pool.map(lambda job: run(job, None), jobs))
+        results = list(_worker_pool(n_workers).map(lambda job: run(job, None), jobs))
     for rows, errors in results:
         summary.rows.extend(rows)
         summary.errors.update(errors)
