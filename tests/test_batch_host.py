@@ -68,3 +68,25 @@ def test_an_explicit_grid_takes_the_grid_path(fake_rows):
                              workers=1)
     assert [kind for kind, _ in fake_rows] == ["grid", "grid", "grid"]
     assert res.launches == 3 and len(res.rows) == 5
+
+
+def test_worker_threads_persist_between_calls(monkeypatch):
+    # each worker thread keeps its engine from one call to the next: the pool's
+    # threads are the same ones in a second call
+    import threading
+
+    from cuperiod_b200.batch import batch_periodograms
+    from cuperiod_b200.bls import BLSMethod
+    seen = []
+
+    def rows_default(self, keyed, settings, *, n_best=10, extra_keys=(), engine=None):
+        seen.append(threading.get_ident())
+        return [{"key": k} for k, _ in keyed]
+
+    monkeypatch.setattr(BLSMethod, "rows_default", rows_default)
+    inputs = _curves(8)
+    batch_periodograms(inputs, "BLS", domain="flux", chunk_size=2, workers=2)
+    first = set(seen)
+    seen.clear()
+    batch_periodograms(inputs, "BLS", domain="flux", chunk_size=2, workers=2)
+    assert set(seen) <= first and threading.get_ident() not in first
