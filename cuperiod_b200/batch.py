@@ -233,7 +233,9 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
         groups.setdefault(gk, (g, []))[1].append((str(key), lc))
         entries.append((str(key), lc, gk))
 
-    def searchable(key: str, lc: Any) -> bool:
+    def searchable(key: str, lc: Any) -> Any:
+        """The curve's finite points when they can be searched, else None (the
+        failure recorded); the searches take these and do not filter again."""
         finite = lc.finite()
         if finite.n < s.min_detections or finite.baseline <= 0.0:
             summary.errors[key] = (f"InsufficientDataError: {m.name}: {finite.n} "
@@ -241,28 +243,31 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                                    if finite.n < s.min_detections
                                    else f"InsufficientDataError: {m.name}: no usable "
                                         "time baseline")
-            return False
-        return True
+            return None
+        return finite
 
     jobs: list[Any] = [("star", job) for job in star_jobs]
     if native_default:
         # one launch per chunk of curves in input order, each over its default grid
-        ok_all, failed = m.split_default([(key, lc) for key, lc, _ in entries
-                                          if searchable(key, lc)], s)
+        usable = ((key, searchable(key, lc)) for key, lc, _ in entries)
+        ok_all, failed = m.split_default([(key, f) for key, f in usable if f is not None], s,
+                                         prefiltered=True)
         summary.errors.update(failed)
         for start in range(0, len(ok_all), chunk_size):
             jobs.append(("default", ok_all[start:start + chunk_size]))
     elif hasattr(m, "rows_by_grid"):
         # one launch per chunk of curves in input order, each curve over its own
         # grid (equal grids shared)
-        ok_all = [(key, lc, groups[gk][0]) for key, lc, gk in entries if searchable(key, lc)]
+        usable = ((key, searchable(key, lc), gk) for key, lc, gk in entries)
+        ok_all = [(key, f, groups[gk][0]) for key, f, gk in usable if f is not None]
         for start in range(0, len(ok_all), chunk_size):
             jobs.append(("mixed", ok_all[start:start + chunk_size]))
     else:
         for g, members in groups.values():
             for start in range(0, len(members), chunk_size):
-                ok = [(key, lc) for key, lc in members[start:start + chunk_size]
-                      if searchable(key, lc)]
+                usable = ((key, searchable(key, lc))
+                          for key, lc in members[start:start + chunk_size])
+                ok = [(key, f) for key, f in usable if f is not None]
                 if ok:
                     jobs.append(("curves", (g, ok)))
     extras = METHOD_PEAK_EXTRAS.get(m.name, ())
@@ -280,11 +285,11 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
                                        extra_keys=PEAK_EXTRA_COLUMNS, alias_diverse=True)], {}
         if kind == "default":
             return m.rows_default(body, s, n_best=n_best, extra_keys=extras,
-                                  engine=job_engine), {}
+                                  engine=job_engine, prefiltered=True), {}
         if kind == "mixed":
             # peaks ranked on the device: only the rows leave the GPU
             return m.rows_by_grid(body, s, n_best=n_best, extra_keys=extras,
-                                  engine=job_engine), {}
+                                  engine=job_engine, prefiltered=True), {}
         return run_curves(body, job_engine), {}
 
     def run_curves(body, job_engine):

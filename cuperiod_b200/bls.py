@@ -271,12 +271,16 @@ class BLSMethod:
     def rows_by_grid(self, items: Sequence[tuple[str, LightCurve, GridSpec]],
                      settings: BLSSettings, *, n_best: int = 10,
                      extra_keys: Sequence[str] = (),
-                     engine: _lib.Engine | None = None) -> list[dict]:
+                     engine: _lib.Engine | None = None,
+                     prefiltered: bool = False) -> list[dict]:
         """``rows_many`` for curves that each bring their own grid (the
         reference's batch searches every curve over its own default grid,
         batch/runner.py:187-250): every curve of ``items`` -- ``(key, curve,
         grid)``, equal grids passed as the same object -- in one launch, each
-        over its grid, peaks ranked on the device.  Rows in ``items`` order."""
+        over its grid, peaks ranked on the device.  Rows in ``items`` order.
+        ``prefiltered``: the curves are ``finite()`` results that already passed
+        the minimum-detection and baseline guards (the batch runner's check), so
+        they are not filtered again."""
         count = max(int(n_best), 1)
         slot: dict[int, int] = {}
         grids: list[GridSpec] = []
@@ -289,7 +293,8 @@ class BLSMethod:
         segments = [_grid_segments(g, settings) for g in grids]
         if any(not sg for sg in segments):
             raise InsufficientDataError("BLS: empty trial grid")
-        prepared = [_prepared_curve(lc, settings) for _, lc, _ in items]
+        prepared = ([(lc, lc.error) for _, lc, _ in items] if prefiltered
+                    else [_prepared_curve(lc, settings) for _, lc, _ in items])
         eng = engine or _lib.default_engine()
         periods = [np.concatenate([np.asarray(p, dtype=np.float64) for p, _ in sg])
                    for sg in segments]
@@ -332,18 +337,19 @@ class BLSMethod:
                 rows[i] = made[j]
         return rows  # type: ignore[return-value]
 
-    def split_default(self, keyed: Sequence[tuple[str, LightCurve]], settings: BLSSettings
+    def split_default(self, keyed: Sequence[tuple[str, LightCurve]], settings: BLSSettings,
+                      prefiltered: bool = False
                       ) -> tuple[list[tuple[str, LightCurve]], dict[str, str]]:
         """The curves whose default grid can be searched, and the failure of each
         other curve as ``default_grid`` would raise it (the grid-size guard,
         GridTooLargeError, or an empty grid, InsufficientDataError), without
-        building the grids in Python."""
+        building the grids in Python (``prefiltered`` as in ``rows_by_grid``)."""
         from .errors import CuPeriodError
         good: list[tuple[str, LightCurve]] = []
         errors: dict[str, str] = {}
         base: list[float] = []
         for key, lc in keyed:
-            finite = lc.finite()
+            finite = lc if prefiltered else lc.finite()
             b = finite.baseline
             try:
                 check_grid_size(_default_total(b, settings), automatic=True, time=finite.time,
@@ -368,18 +374,21 @@ class BLSMethod:
 
     def rows_default(self, keyed: Sequence[tuple[str, LightCurve]], settings: BLSSettings, *,
                      n_best: int = 10, extra_keys: Sequence[str] = (),
-                     engine: _lib.Engine | None = None) -> list[dict]:
+                     engine: _lib.Engine | None = None,
+                     prefiltered: bool = False) -> list[dict]:
         """``rows_by_grid`` with every curve over its own default grid
         (``default_grid``), the grids built by the engine library on the host
         cores (``bls_prepare_default``) instead of as one GridSpec per curve:
         the same trial periods bit for bit, the same rows.  The curves must pass
-        ``split_default``."""
+        ``split_default`` (``prefiltered`` as in ``rows_by_grid``)."""
         count = max(int(n_best), 1)
         if count > 1024:
             return self.rows_by_grid([(key, lc, self.default_grid(lc, settings))
                                       for key, lc in keyed], settings, n_best=n_best,
-                                     extra_keys=extra_keys, engine=engine)
-        prepared = [_prepared_curve(lc, settings) for _, lc in keyed]
+                                     extra_keys=extra_keys, engine=engine,
+                                     prefiltered=prefiltered)
+        prepared = ([(lc, lc.error) for _, lc in keyed] if prefiltered
+                    else [_prepared_curve(lc, settings) for _, lc in keyed])
         if not prepared:
             return []
         baselines = np.array([f.baseline for f, _ in prepared], dtype=np.float64)

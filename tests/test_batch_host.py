@@ -22,11 +22,13 @@ def fake_rows(monkeypatch):
     from cuperiod_b200.bls import BLSMethod
     calls = []
 
-    def rows_default(self, keyed, settings, *, n_best=10, extra_keys=(), engine=None):
+    def rows_default(self, keyed, settings, *, n_best=10, extra_keys=(), engine=None,
+                     prefiltered=False):
         calls.append(("default", [k for k, _ in keyed]))
         return [{"key": k, "n": lc.n} for k, lc in keyed]
 
-    def rows_by_grid(self, items, settings, *, n_best=10, extra_keys=(), engine=None):
+    def rows_by_grid(self, items, settings, *, n_best=10, extra_keys=(), engine=None,
+                     prefiltered=False):
         calls.append(("grid", [k for k, _, _ in items]))
         return [{"key": k, "n": lc.n} for k, lc, _ in items]
 
@@ -79,7 +81,8 @@ def test_worker_threads_persist_between_calls(monkeypatch):
     from cuperiod_b200.bls import BLSMethod
     seen = []
 
-    def rows_default(self, keyed, settings, *, n_best=10, extra_keys=(), engine=None):
+    def rows_default(self, keyed, settings, *, n_best=10, extra_keys=(), engine=None,
+                     prefiltered=False):
         seen.append(threading.get_ident())
         return [{"key": k} for k, _ in keyed]
 
