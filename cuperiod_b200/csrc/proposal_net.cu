@@ -5,15 +5,16 @@
 //   * pn_gemm_kernel<BN>: D[M, N] = A[M, K] . B[N, K]^T, bf16 operands (both
 //     K-major), fp32 accumulation in tensor memory.  One CTA per 128 x BN output
 //     tile (grid.z splits K): thread 0 streams 128 x 64 and BN x 64 tiles of A
-//     and B into a four-stage shared-memory ring with TMA (128-byte swizzle, no
-//     multicast), thread 32 issues tcgen05.mma (M = 128, N = BN, K = 16 per
-//     instruction) as each stage lands and returns the stage to the producer
-//     with tcgen05.commit, and the four warps read the accumulator back with
-//     tcgen05.ld (warp w owns rows 32w..32w+31) for a fused epilogue: bias,
-//     ReLU, a ReLU-derivative mask, bf16 or fp32 store (optionally transposed),
-//     or fp32 atomic accumulation for split-K.  Every wait on an mbarrier is
-//     bounded by the global timer; a wait that runs out sets the error flag, the
-//     CTA skips its stores, frees its tensor memory and returns.
+//     and B into a four-stage shared-memory ring with TMA (128-byte swizzle,
+//     each CTA loading its own tiles), thread 32 issues tcgen05.mma (M = 128,
+//     N = BN, K = 16 per instruction) as each stage lands and returns the stage
+//     to the producer with tcgen05.commit, and the four warps read the
+//     accumulator back with tcgen05.ld (warp w owns rows 32w..32w+31) for a
+//     fused epilogue: bias, ReLU, a ReLU-derivative mask, bf16 or fp32 store
+//     (optionally transposed), or fp32 atomic accumulation for split-K.  Every
+//     wait on an mbarrier is bounded by the global timer; a wait that runs out
+//     sets the error flag, the CTA skips its stores, frees its tensor memory and
+//     returns.
 //   * the network's data movers and small steps: time binning of the curves,
 //     im2col / col2im for the stride-2 convolutions, transposes, bias
 //     gradients, softmax cross-entropy, Adam, and the top-k window selection.
