@@ -8,6 +8,7 @@
 // from clock64() against %globaltimer inside the same kernel.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <math.h>
 #include <stdio.h>
 
 namespace {
@@ -95,6 +96,113 @@ __global__ void arith_probe(double* sink, Stamp* st, double seed) {
     sink[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// Fold probe: the search kernel's fast fold path alone, on one synthetic
+// one-weight curve (10,240 points at a 2-minute cadence with 5% dropouts) and
+// eight periods of 0.3-0.6 d with 0.001 d bins (611-bin histograms, 12-byte
+// records, the kernel's layout), each CTA folding it kFoldItems times.
+// Variant 0: the phase, the edge tests and the record address only; 1: plus
+// three atomics per point; 2: plus the merging of runs of equal bins before
+// the atomics, as the kernel does.  Every record address stays inside its
+// period's histogram: S <= 600.1 * 2^22, so (S - 1) >> 22 + 1 <= 601 < 611.
+constexpr int kFoldThreads = 256, kFoldPts = 8, kFoldPeriods = 8, kFoldBins = 611;
+constexpr int kFoldItems = 64, kFoldN = 10240;
+constexpr int kFoldRec = 12;
+constexpr uint32_t kFoldPeriodBytes = ((kFoldBins * kFoldRec + 15) / 16) * 16;
+
+template <int OFF>
+__device__ __forceinline__ void probe_red(uint32_t a, uint32_t v) {
+    asm volatile("red.shared.add.u32 [%0+%2], %1;" ::"r"(a), "r"(v), "n"(OFF) : "memory");
+}
+
+template <int V>
+__global__ void __launch_bounds__(kFoldThreads, 3)
+    fold_probe(const double* __restrict__ tau, const uint32_t* __restrict__ pay,
+               const double* __restrict__ fq, const uint32_t* __restrict__ sq,
+               uint32_t* sink) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double s_f[kFoldPeriods];
+    __shared__ uint32_t s_S[kFoldPeriods];
+    const int tid = threadIdx.x;
+    if (tid < kFoldPeriods) {
+        s_f[tid] = fq[tid];
+        s_S[tid] = sq[tid];
+    }
+    const uint32_t hist_s = (uint32_t)__cvta_generic_to_shared(smem);
+    const int fb = 22;
+    const uint32_t fmask = (1u << fb) - 1u, mu = 5u, fr_span = (1u << fb) - 10u;
+    const uint32_t mphi = 3u, phi_span = 0u - 6u;
+    constexpr uint32_t kB = kFoldRec;
+    uint32_t acc = 0;
+    for (int it = 0; it < kFoldItems; ++it) {
+        for (int i = tid; i < (int)(kFoldPeriods * kFoldPeriodBytes / 16); i += kFoldThreads)
+            reinterpret_cast<uint4*>(smem)[i] = make_uint4(0u, 0u, 0u, 0u);
+        __syncthreads();
+        for (int base = 0; base < kFoldN; base += kFoldThreads * kFoldPts) {
+            double x[kFoldPts];
+            uint32_t lo[kFoldPts], hi[kFoldPts];
+#pragma unroll
+            for (int r = 0; r < kFoldPts; ++r) {
+                const int j = base + r * kFoldThreads + tid;
+                x[r] = __ldg(tau + j);
+                const uint32_t w = __ldg(pay + j);
+                lo[r] = w & 0xffffu;
+                hi[r] = (uint32_t)((int32_t)w >> 16);
+            }
+            for (int q = 0; q < kFoldPeriods; ++q) {
+                const double f = s_f[q];
+                const uint32_t S = s_S[q];
+                const uint32_t hq = hist_s + (uint32_t)q * kFoldPeriodBytes;
+                uint32_t rec[kFoldPts];
+                bool all_ok = true;
+#pragma unroll
+                for (int r = 0; r < kFoldPts; ++r) {
+                    const double qm = __fma_rn(x[r], f, 1572864.0);
+                    const uint32_t phi = (uint32_t)__double2loint(qm);
+                    const uint32_t v = __umulhi(phi, S);
+                    all_ok &= ((phi - mphi) < phi_span) & (((v & fmask) - mu) < fr_span);
+                    rec[r] = hq + kB + (v >> fb) * kB;
+                }
+                if (V == 0) {
+#pragma unroll
+                    for (int r = 0; r < kFoldPts; ++r) acc += all_ok ? rec[r] : 1u;
+                } else if (!all_ok) {
+                    continue;
+                } else if (V == 1) {
+#pragma unroll
+                    for (int r = 0; r < kFoldPts; ++r) {
+                        probe_red<0>(rec[r], lo[r]);
+                        probe_red<4>(rec[r], hi[r]);
+                        probe_red<8>(rec[r], 1u);
+                    }
+                } else {
+                    uint32_t s_lo = lo[0], s_hi = hi[0], s_c = 1u;
+#pragma unroll
+                    for (int r = 1; r < kFoldPts; ++r) {
+                        if (rec[r] != rec[r - 1]) {
+                            probe_red<0>(rec[r - 1], s_lo);
+                            probe_red<4>(rec[r - 1], s_hi);
+                            probe_red<8>(rec[r - 1], s_c);
+                            s_lo = 0u;
+                            s_hi = 0u;
+                            s_c = 0u;
+                        }
+                        s_lo += lo[r];
+                        s_hi += hi[r];
+                        s_c += 1u;
+                    }
+                    probe_red<0>(rec[kFoldPts - 1], s_lo);
+                    probe_red<4>(rec[kFoldPts - 1], s_hi);
+                    probe_red<8>(rec[kFoldPts - 1], s_c);
+                }
+            }
+        }
+        __syncthreads();
+        acc += reinterpret_cast<const uint32_t*>(smem)[tid];
+        __syncthreads();
+    }
+    sink[blockIdx.x * kFoldThreads + tid] = acc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -164,6 +272,85 @@ int bls_probe_pipes(char* report, int report_len) {
     cudaFree(sink);
     cudaFree(st);
     return rc;
+}
+
+
+// Runs the fold probe's three variants (three CTAs per SM), each once to warm up
+// and once timed with CUDA events, and writes one line per variant: name,
+// milliseconds, point-folds per second (1e9).  Returns 0 or a CUDA error code.
+int bls_probe_fold(char* report, int report_len) {
+    int dev = 0, n_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = 3 * n_sm;
+    // the curve: a 2-minute cadence with a seeded 5% of dropouts, and one-weight
+    // payload words (13-bit low part, small signed high part)
+    double* h_tau = new double[kFoldN];
+    uint32_t* h_pay = new uint32_t[kFoldN];
+    uint32_t rnd = 12345u;
+    int n = 0;
+    for (int k = 0; n < kFoldN; ++k) {
+        rnd = rnd * 1664525u + 1013904223u;
+        if ((rnd >> 8) % 100u < 5u) continue;
+        h_tau[n] = k * (2.0 / 1440.0);
+        rnd = rnd * 1664525u + 1013904223u;
+        const uint32_t lo = (rnd >> 9) & 8191u;
+        const int32_t hi = (int32_t)((rnd >> 3) % 601u) - 300;
+        h_pay[n] = lo | ((uint32_t)(uint16_t)(int16_t)hi << 16);
+        ++n;
+    }
+    double h_f[kFoldPeriods];
+    uint32_t h_S[kFoldPeriods];
+    for (int q = 0; q < kFoldPeriods; ++q) {
+        const double P = 0.3 * pow(2.0, q / 7.0);          // 0.3 .. 0.6 d
+        h_f[q] = 1.0 / P;
+        h_S[q] = (uint32_t)llrint(P / 0.001 * 4194304.0);
+    }
+    double *tau = nullptr, *fq = nullptr;
+    uint32_t *pay = nullptr, *sq = nullptr, *sink = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMalloc(&tau, sizeof(double) * kFoldN);
+    if (e == cudaSuccess) e = cudaMalloc(&pay, sizeof(uint32_t) * kFoldN);
+    if (e == cudaSuccess) e = cudaMalloc(&fq, sizeof(h_f));
+    if (e == cudaSuccess) e = cudaMalloc(&sq, sizeof(h_S));
+    if (e == cudaSuccess) e = cudaMalloc(&sink, sizeof(uint32_t) * blocks * kFoldThreads);
+    if (e == cudaSuccess) e = cudaMemcpy(tau, h_tau, sizeof(double) * kFoldN, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(pay, h_pay, sizeof(uint32_t) * kFoldN, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(fq, h_f, sizeof(h_f), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(sq, h_S, sizeof(h_S), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    const size_t smem = (size_t)kFoldPeriods * kFoldPeriodBytes;
+    const double folds = (double)blocks * kFoldItems * kFoldN * kFoldPeriods;
+    int pos = 0;
+    auto run = [&](const char* name, auto kernel) {
+        if (e != cudaSuccess) return;
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return;
+        kernel<<<blocks, kFoldThreads, smem>>>(tau, pay, fq, sq, sink);
+        cudaEventRecord(e0);
+        kernel<<<blocks, kFoldThreads, smem>>>(tau, pay, fq, sq, sink);
+        cudaEventRecord(e1);
+        e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        float ms = 0.0f;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        pos += snprintf(report + pos, report_len - pos, "%s %.3f %.1f\n", name, ms,
+                        folds / (ms * 1e-3) / 1e9);
+    };
+    run("fold_phase_tests_address", fold_probe<0>);
+    run("fold_plus_three_atomics", fold_probe<1>);
+    run("fold_plus_run_merging", fold_probe<2>);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(tau);
+    cudaFree(pay);
+    cudaFree(fq);
+    cudaFree(sq);
+    cudaFree(sink);
+    delete[] h_tau;
+    delete[] h_pay;
+    return (int)e;
 }
 
 }  // extern "C"
