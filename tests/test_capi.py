@@ -50,3 +50,26 @@ def test_engine_creation_without_a_device_raises():
         pytest.skip("a device is present")
     with pytest.raises((_lib.EngineError, RuntimeError)):
         _lib.Engine()
+
+
+def test_packed_curves_concatenate_in_order():
+    # large batches are copied by several host threads; the layout is the plain
+    # concatenation, missing errors filled with ones, and no error array at all
+    # when no curve has one
+    import numpy as np
+
+    from cuperiod_b200 import _lib
+    rng = np.random.default_rng(4)
+    sizes = rng.integers(1, 40000, 120)
+    curves = [(rng.uniform(size=n), rng.normal(size=n), None if i % 4 else rng.uniform(size=n))
+              for i, n in enumerate(sizes)]
+    pc = _lib.PackedCurves.from_arrays(curves)
+    assert pc.t.size == sizes.sum() > (1 << 21)
+    np.testing.assert_array_equal(pc.offsets, np.concatenate([[0], np.cumsum(sizes)]))
+    np.testing.assert_array_equal(pc.t, np.concatenate([c[0] for c in curves]))
+    np.testing.assert_array_equal(pc.y, np.concatenate([c[1] for c in curves]))
+    np.testing.assert_array_equal(
+        pc.dy, np.concatenate([np.ones(c[0].size) if c[2] is None else c[2] for c in curves]))
+    assert _lib.PackedCurves.from_arrays([(c[0], c[1], None) for c in curves]).dy is None
+    empty = _lib.PackedCurves.from_arrays([(np.zeros(0), np.zeros(0), None)])
+    assert empty.t.size == 0 and empty.n_curves == 1
