@@ -93,6 +93,17 @@ def _worker_pool(n: int):
         return pool
 
 
+def release_workers() -> None:
+    """Shut the batch worker pools down: their threads exit, and with them each
+    thread's engine (device buffers, pinned staging) is freed.  A later call
+    with ``workers > 1`` starts a new pool."""
+    with _pools_lock:
+        pools = list(_pools.values())
+        _pools.clear()
+    for pool in pools:
+        pool.shutdown(wait=True)
+
+
 def _grid_key(grid: GridSpec) -> str:
     h = hashlib.sha1(np.ascontiguousarray(grid.period).tobytes())
     h.update(repr(sorted(grid.meta.items())).encode())
@@ -321,5 +332,4 @@ def batch_periodograms(inputs: Any, method: str = "BLS", *,
 
 
 __all__ = ["BatchSummary", "METHOD_PEAK_EXTRAS", "PEAK_EXTRA_COLUMNS", "batch_periodograms",
-           "periodogram_to_row",
-           "resolve_inputs"]
+           "periodogram_to_row", "release_workers", "resolve_inputs"]

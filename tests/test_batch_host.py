@@ -93,3 +93,23 @@ def test_worker_threads_persist_between_calls(monkeypatch):
     seen.clear()
     batch_periodograms(inputs, "BLS", domain="flux", chunk_size=2, workers=2)
     assert set(seen) <= first and threading.get_ident() not in first
+
+
+def test_release_workers_ends_the_pool_threads(monkeypatch):
+    import threading
+
+    from cuperiod_b200.batch import batch_periodograms, release_workers
+    from cuperiod_b200.bls import BLSMethod
+
+    def rows_default(self, keyed, settings, *, n_best=10, extra_keys=(), engine=None,
+                     prefiltered=False):
+        return [{"key": k} for k, _ in keyed]
+
+    monkeypatch.setattr(BLSMethod, "rows_default", rows_default)
+    batch_periodograms(_curves(6), "BLS", domain="flux", chunk_size=2, workers=3)
+    assert any(t.name.startswith("bls-batch-3") for t in threading.enumerate())
+    release_workers()
+    assert not any(t.name.startswith("bls-batch-") for t in threading.enumerate())
+    res = batch_periodograms(_curves(6), "BLS", domain="flux", chunk_size=2, workers=3)
+    assert len(res.rows) == 6
+    release_workers()
