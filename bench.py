@@ -583,6 +583,8 @@ def run_ours(args) -> None:
         summary_o = batch_periodograms(keyed, "BLS", grid=gspec, chunk_size=1024, workers=4)
         ovl_ms.append(1000.0 * (time.perf_counter() - t0))
     ovl_value = world * n_curves / (max_over_ranks(statistics.mean(ovl_ms)) / 1000.0)
+    from cuperiod_b200.batch import release_workers
+    release_workers()                       # the worker engines' memory back
     ovl_same = sum(int(a["best_period"] == b["best_period"])
                    for a, b in zip(summary.rows, summary_o.rows))
     rows = summary.rows
