@@ -246,11 +246,45 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         const int m = m0 + warp * 32 + lane;
         const bool add = g.out_mode == PN_OUT_F32_ADD;
         const bool use_bias = g.bias != nullptr && (!add || blockIdx.z == 0);
+        const bool bf16_out = g.out_mode == PN_OUT_BF16;
+        // row-major stores of 16 whole columns go out as 16-byte vectors when the
+        // row's first element is 16-byte aligned
+        const bool vec = !add && !g.transpose_out &&
+                         ((reinterpret_cast<uintptr_t>(g.out) & 15u) == 0u) &&
+                         (g.ldo % (bf16_out ? 8 : 4)) == 0;
 #pragma unroll 1
         for (int c = 0; c < BN; c += 16) {
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
             if (m >= g.M) continue;
+            if (vec && n0 + c + 16 <= g.N) {
+                const long long o = (long long)m * g.ldo + n0 + c;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    float x = v[j];
+                    if (use_bias) x += g.bias[n0 + c + j];
+                    if (g.relu) x = fmaxf(x, 0.0f);
+                    if (g.mask != nullptr && !(__bfloat162float(g.mask[o + j]) > 0.0f)) x = 0.0f;
+                    v[j] = x;
+                }
+                if (bf16_out) {
+                    uint32_t w[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                        w[j] = *reinterpret_cast<const uint32_t*>(&h);
+                    }
+                    uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(g.out) + o);
+                    dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                    dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                } else {
+                    float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(g.out) + o);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+                }
+                continue;
+            }
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 const int n = n0 + c + j;
